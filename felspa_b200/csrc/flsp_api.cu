@@ -1,0 +1,912 @@
+// flsp_api.cu — C ABI of the B200 level-set hot path (include/flsp_dg.h).
+//
+// Host side of the drop-in: one handle per level-set problem, resident on
+// one GPU, driven through one CUDA stream.  The host mirrors the control
+// flow of the reference simulators (AdvectSimulator::advance_time,
+// ReinitSimulatorLDG::run_iteration*, LevelSetSurface::advance_time); all
+// arithmetic on the state runs in the kernels of flsp_k_*.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "flsp_dg.h"
+#include "flsp_launch.h"
+#include "flsp_tables.h"
+
+using namespace flsp;
+
+namespace {
+thread_local std::string g_err;
+}
+
+namespace flsp {
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace flsp
+
+namespace {
+
+int fail(int code, const std::string& msg) { return set_error(code, msg); }
+
+#define CU(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(e_ == cudaErrorMemoryAllocation ? FLSP_ERR_OOM : FLSP_ERR_CUDA,        \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define ST(call)                  \
+  do {                            \
+    int s_ = (call);              \
+    if (s_ != FLSP_OK) return s_; \
+  } while (0)
+
+double host_factor(const flsp_factor& f, double x) {
+  const double kPi = 3.14159265358979323846;
+  switch (f.kind) {
+    case FLSP_F_ONE: return 1.0;
+    case FLSP_F_LIN: return f.a * x + f.b;
+    case FLSP_F_SIN: return std::sin(f.a * x + f.b);
+    case FLSP_F_COS: return std::cos(f.a * x + f.b);
+    case FLSP_F_SINSQ: { double s = std::sin(f.a * x + f.b); return s * s; }
+    case FLSP_F_SINPI: return std::sin(kPi * (f.a * x + f.b));
+    case FLSP_F_COSPI: return std::cos(kPi * (f.a * x + f.b));
+    case FLSP_F_SINPISQ: { double s = std::sin(kPi * (f.a * x + f.b)); return s * s; }
+  }
+  return 0.0;
+}
+
+double host_time_factor(const flsp_velocity_desc& v, double t) {
+  const double kPi = 3.14159265358979323846;
+  switch (v.time_kind) {
+    case FLSP_T_COS: return std::cos(v.ta * t + v.tb);
+    case FLSP_T_COSPI: return std::cos(kPi * (v.ta * t + v.tb));
+    case FLSP_T_ONE_MINUS_EXP: return 1.0 - std::exp(-v.ta * t);
+    default: return 1.0;
+  }
+}
+
+double adv_cfl_scaling(int p) {  // AdvectSimulator::cfl_scaling (advection.cc:487-496)
+  const double pp = p;
+  double c = 4.0 / (2.0 + pp) / (2.0 + pp) + 1.0;
+  c *= (2.0 * pp + 1.0);
+  return c;
+}
+
+bool g_tables_ready[64] = {false};
+
+int upload_tables(int dev) {
+  if (dev >= 0 && dev < 64 && g_tables_ready[dev]) return FLSP_OK;
+  ST(upload_tables_adv());
+  ST(upload_tables_hj());
+  ST(upload_tables_misc());
+  if (dev >= 0 && dev < 64) g_tables_ready[dev] = true;
+  return FLSP_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------
+// handle
+// ------------------------------------------------------------------
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  int cur_after = 0;
+};
+
+struct flsp_handle {
+  int dim = 2, p = 1, basis = 1, prec = 0, rk = 3;
+  double cfl_max = 0.9;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  MeshArgs m;
+  long long ndofs = 0;
+  size_t tsize = 8;
+  void* buf[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  void* snap = nullptr;
+  bool has_snap = false;
+  void* vtab = nullptr;
+  double* vtab64 = nullptr;
+  bool has_vel = false;
+  flsp_velocity_desc vel;
+  int nmax = 1, npt = 1;
+  DevClock* clk = nullptr;
+  DevClock* clk_host = nullptr;   // pinned mirror
+  int64_t* perm = nullptr;
+  double* stage64 = nullptr;      // FP64 device staging (2 * dim * ndofs)
+  double* partial = nullptr;
+  int partial_n = 0;
+  double* red_out = nullptr;
+  flsp_ic_desc* ic_dev = nullptr;
+  unsigned int* flag_dev = nullptr;
+  int n_since_reinit = 0;
+  int adv_tile[3] = {0, 0, 0};
+  int hj_tile[3] = {0, 0, 0};
+  std::map<long long, GraphEntry> graphs;
+
+  Ctx ctx() const {
+    Ctx c;
+    c.dim = dim;
+    c.p = p;
+    c.prec = prec;
+    c.m = m;
+    c.stream = stream;
+    return c;
+  }
+  VelDev veldev() const {
+    VelDev v;
+    std::memset(&v, 0, sizeof(v));
+    v.vtab = vtab;
+    v.n_terms = vel.n_terms;
+    v.nmax = nmax;
+    v.npt = npt;
+    for (int k = 0; k < vel.n_terms; ++k) v.comp[k] = vel.terms[k].comp;
+    return v;
+  }
+};
+
+namespace {
+
+void clear_graphs(flsp_handle* h) {
+  for (auto& kv : h->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  h->graphs.clear();
+}
+
+int ensure_partial(flsp_handle* h, int n) {
+  if (h->partial_n >= n) return FLSP_OK;
+  if (h->partial) cudaFree(h->partial);
+  h->partial = nullptr;
+  CU(cudaMalloc(&h->partial, sizeof(double) * 2 * (size_t)n));
+  h->partial_n = n;
+  return FLSP_OK;
+}
+
+int sync_clock(flsp_handle* h) {
+  CU(cudaMemcpyAsync(h->clk_host, h->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+// kernel configuration of this handle (tiles, shared-memory attributes);
+// done outside any stream capture
+int prepare_kernels(flsp_handle* h) {
+  Ctx c = h->ctx();
+  ST(adv_default_tile(c, h->vel.n_terms, h->adv_tile));
+  ST(adv_prepare(c, h->vel.n_terms, h->adv_tile));
+  ST(hj_default_tile(c, h->hj_tile));
+  ST(hj_prepare(c, h->hj_tile));
+  if (h->dim == 2) ST(weno_prepare(c));
+  return FLSP_OK;
+}
+
+int other(int a, int b) {  // the buffer index that is neither a nor b
+  for (int i = 0; i < 3; ++i)
+    if (i != a && i != b) return i;
+  return -1;
+}
+
+int stage(flsp_handle* h, const void* in, const void* phin, void* out, int st, int combine) {
+  return launch_adv_stage(h->ctx(), h->veldev(), in, phin, out, h->clk, st, combine, 0.0, h->adv_tile);
+}
+
+// one SSP-RK substep on the device clock (no host synchronisation)
+int enqueue_adv_step(flsp_handle* h) {
+  AdvClockArgs ca;
+  ca.cfl_max = h->cfl_max;
+  ca.scale = adv_cfl_scaling(h->p);
+  ca.tkind = h->vel.time_kind;
+  ca.ta = h->vel.ta;
+  ca.tb = h->vel.tb;
+  ca.rk = h->rk;
+  ST(launch_adv_clock_begin(h->stream, h->clk, ca));
+  const int x = h->cur, y = (h->cur + 1) % 3, z = (h->cur + 2) % 3;
+  void* X = h->buf[x];
+  void* Y = h->buf[y];
+  void* Z = h->buf[z];
+  if (h->rk == 1) {
+    ST(stage(h, X, X, Y, 0, kRK1));
+    h->cur = y;
+  } else if (h->rk == 2) {
+    ST(stage(h, X, X, Y, 0, kRK2a));
+    ST(stage(h, Y, X, Z, 1, kRK2b));
+    h->cur = z;
+  } else {
+    ST(stage(h, X, X, Y, 0, kRK3a));
+    ST(stage(h, Y, X, Z, 1, kRK3b));
+    ST(stage(h, Z, X, Y, 2, kRK3c));
+    h->cur = y;
+  }
+  return launch_adv_clock_end(h->stream, h->clk);
+}
+
+bool reinit_limiter(const flsp_handle* h, const flsp_reinit_opts* o) {
+  if (h->dim != 2) return false;
+  return o->limiter < 0 ? true : o->limiter != 0;
+}
+
+// one reinitialisation pseudo-step: reads cur and phi0, writes a free buffer
+int enqueue_hj_step(flsp_handle* h, const flsp_reinit_opts* o, int phi0_idx, bool limiter) {
+  ST(launch_hj_clock_begin(h->stream, h->clk, o->cfl_max, h->p, o->viscosity, h->m.min_diam,
+                           adv_cfl_scaling(h->p)));
+  const int src = h->cur;
+  const int dst = (src == phi0_idx) ? (phi0_idx + 1) % 3 : other(src, phi0_idx);
+  ST(launch_hj(h->ctx(), h->buf[src], h->buf[phi0_idx], h->buf[dst], h->clk, kHJStep, o->rk_order, 0.0,
+               h->ndofs, h->hj_tile));
+  int res = dst;
+  if (limiter) {
+    const int lim = other(dst, phi0_idx);
+    ST(launch_weno(h->ctx(), h->buf[dst], h->buf[lim], nullptr));
+    res = lim;
+  }
+  h->cur = res;
+  return launch_hj_clock_end(h->stream, h->clk);
+}
+
+int reduce_dev(flsp_handle* h, int which, const void* phi, const void* ref, bool with_ic, double* out2) {
+  Ctx c = h->ctx();
+  ST(ensure_partial(h, reduce_blocks(c)));
+  ST(launch_reduce(c, which, phi, ref, with_ic ? h->ic_dev : nullptr, h->partial, h->red_out));
+  CU(cudaMemcpyAsync(out2, h->red_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int check_finite(flsp_handle* h, const void* x) {
+  CU(cudaMemsetAsync(h->flag_dev, 0, sizeof(unsigned int), h->stream));
+  ST(launch_nonfinite(h->ctx(), x, h->ndofs, h->flag_dev));
+  unsigned int cnt = 0;
+  CU(cudaMemcpyAsync(&cnt, h->flag_dev, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  if (cnt) return fail(FLSP_ERR_NONFINITE, std::to_string(cnt) + " non-finite coefficients");
+  return FLSP_OK;
+}
+
+void fill_reinit_defaults(flsp_reinit_opts* o) {
+  o->mode = FLSP_REINIT_BAND;
+  o->n_pseudo_steps = 5;
+  o->band_width_coeff = 4.0;
+  o->max_iter = 1000;
+  o->cfl_max = 0.2;
+  o->viscosity = 0.0;
+  o->rk_order = 1;
+  o->limiter = -1;
+  o->narrow_band = 0;
+  o->band_cells = 6.0;
+}
+
+int validate_reinit(const flsp_handle* h, const flsp_reinit_opts* o) {
+  if (!o) return fail(FLSP_ERR_BAD_ARG, "null reinit options");
+  if (o->mode < 0 || o->mode > 2) return fail(FLSP_ERR_BAD_ARG, "bad reinit mode");
+  if (!(o->cfl_max > 0.0)) return fail(FLSP_ERR_BAD_ARG, "reinit cfl_max must be positive");
+  if (o->mode == FLSP_REINIT_BAND && !(o->band_width_coeff > 1.0))
+    return fail(FLSP_ERR_BAD_ARG, "band_width_coeff must be greater than 1 (reinit.cc:597-598)");
+  if (o->mode == FLSP_REINIT_FIXED && (o->n_pseudo_steps < 0 || o->n_pseudo_steps > 100000))
+    return fail(FLSP_ERR_BAD_ARG, "bad n_pseudo_steps");
+  if (o->max_iter < 0) return fail(FLSP_ERR_BAD_ARG, "negative max_iter");
+  if (o->viscosity < 0.0) return fail(FLSP_ERR_BAD_ARG, "negative viscosity");
+  if (o->viscosity > 0.0) return fail(FLSP_ERR_UNSUPPORTED, "LDG artificial viscosity not built yet");
+  if (o->rk_order < 1 || o->rk_order > 3) return fail(FLSP_ERR_BAD_ARG, "reinit rk_order must be 1..3");
+  (void)h;
+  return FLSP_OK;
+}
+
+// ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637)
+int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
+  ST(validate_reinit(h, o));
+  const bool limiter = reinit_limiter(h, o);
+  const int phi0 = h->cur;
+  ST(launch_hj_clock_reset(h->stream, h->clk));
+  // CFL estimate of the first pseudo-step: gradients of the initial state
+  ST(launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, o->rk_order, 0.0,
+               h->ndofs, h->hj_tile));
+  int it = 0;
+  if (o->mode == FLSP_REINIT_FIXED) {
+    for (it = 0; it < o->n_pseudo_steps; ++it) ST(enqueue_hj_step(h, o, phi0, limiter));
+  } else {
+    double horizon;
+    if (o->mode == FLSP_REINIT_GLOBAL) {
+      double r[2];
+      ST(reduce_dev(h, FLSP_RED_MAX_ABS, h->buf[phi0], nullptr, false, r));
+      horizon = 1.2 * r[0];
+    } else {
+      horizon = o->band_width_coeff * h->m.min_diam;
+    }
+    double cum = 0.0;
+    while (cum < horizon && it <= o->max_iter) {
+      ST(enqueue_hj_step(h, o, phi0, limiter));
+      ++it;
+      ST(sync_clock(h));
+      cum = h->clk_host->hj_cum;
+      if (!std::isfinite(cum) || !(h->clk_host->hj_dt > 0.0))
+        return fail(FLSP_ERR_NONFINITE, "reinit pseudo-time step is not positive/finite");
+    }
+  }
+  if (n_iter) *n_iter = it;
+  if (o->mode == FLSP_REINIT_BAND && it == o->max_iter)
+    return fail(FLSP_ERR_BAND_NOT_REACHED, "reinit reached max_iter before the band width");
+  return FLSP_OK;
+}
+
+int build_vtab(flsp_handle* h) {
+  const int dim = h->dim;
+  const int nq = h->p + 2;
+  h->npt = nq + 2;
+  h->nmax = std::max(h->m.n[0], std::max(h->m.n[1], h->m.n[2]));
+  const int nt = std::max(h->vel.n_terms, 1);
+  const size_t n = (size_t)nt * 3 * h->nmax * h->npt;
+  std::vector<double> tabd(n, 0.0);
+  double x[8], w[8];
+  gauss_rule(nq, x, w);
+  for (int k = 0; k < h->vel.n_terms; ++k) {
+    const flsp_vel_term& tm = h->vel.terms[k];
+    for (int ax = 0; ax < 3; ++ax)
+      for (int i = 0; i < h->nmax; ++i)
+        for (int j = 0; j < h->npt; ++j) {
+          double v = 1.0;
+          if (ax < dim && i < h->m.n[ax]) {
+            const double xi = j < nq ? x[j] : (double)(j - nq);
+            const double X0 = h->m.lo[ax] + i * h->m.h[ax];
+            const double xx = X0 + h->m.h[ax] * xi;
+            // coefficient folded into the x factor: ((coeff f0) f1) f2
+            v = (ax == 0) ? tm.coeff * host_factor(tm.f[0], xx) : host_factor(tm.f[ax], xx);
+          }
+          tabd[(((size_t)k * 3 + ax) * h->nmax + i) * h->npt + j] = v;
+        }
+  }
+  if (h->vtab) cudaFree(h->vtab);
+  if (h->vtab64) cudaFree(h->vtab64);
+  h->vtab = nullptr;
+  h->vtab64 = nullptr;
+  CU(cudaMalloc(&h->vtab64, n * sizeof(double)));
+  CU(cudaMemcpy(h->vtab64, tabd.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  if (h->prec == FLSP_FP64) {
+    CU(cudaMalloc(&h->vtab, n * sizeof(double)));
+    CU(cudaMemcpy(h->vtab, tabd.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> tf(n);
+    for (size_t i = 0; i < n; ++i) tf[i] = (float)tabd[i];
+    CU(cudaMalloc(&h->vtab, n * sizeof(float)));
+    CU(cudaMemcpy(h->vtab, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  // static CFL part: max over vertices of |u_spatial| / diam
+  int comp[kMaxTerms];
+  for (int k = 0; k < h->vel.n_terms; ++k) comp[k] = h->vel.terms[k].comp;
+  CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
+  ST(launch_static_cfl(h->ctx(), h->vtab64, h->vel.n_terms, comp, h->nmax, h->npt, h->clk));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+}  // namespace
+
+// ==================================================================
+// C ABI
+// ==================================================================
+extern "C" {
+
+const char* flsp_last_error(void) { return g_err.c_str(); }
+int flsp_version(void) { return 1; }
+
+void flsp_default_dg_opts(flsp_dg_opts* o) {
+  if (!o) return;
+  o->degree = 1;
+  o->basis = FLSP_BASIS_P;
+  o->precision = FLSP_FP64;
+  o->rk_order = 3;
+  o->cfl_max = 0.9;   // AdvectControl: TempoControl(rktvd3, exp, 0.5, 0.9)
+  o->device = 0;
+}
+void flsp_default_reinit_opts(flsp_reinit_opts* o) {
+  if (o) fill_reinit_defaults(o);
+}
+void flsp_default_ls_opts(flsp_ls_opts* o) {
+  if (!o) return;
+  o->reinit_frequency = 10;
+  o->execute_reinit = 1;
+  fill_reinit_defaults(&o->reinit);
+}
+
+int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts, flsp_handle** out) {
+  if (!mesh || !opts || !out) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->dim < 2 || mesh->dim > 3) return fail(FLSP_ERR_BAD_ARG, "dim must be 2 or 3");
+  if (!supported_config(mesh->dim, opts->degree))
+    return fail(FLSP_ERR_UNSUPPORTED, "degree " + std::to_string(opts->degree) + " not built for dim " +
+                                          std::to_string(mesh->dim));
+  if (opts->basis != FLSP_BASIS_P && opts->basis != FLSP_BASIS_Q) return fail(FLSP_ERR_BAD_ARG, "bad basis");
+  if (opts->precision != FLSP_FP64 && opts->precision != FLSP_FP32) return fail(FLSP_ERR_BAD_ARG, "bad precision");
+  if (opts->rk_order < 1 || opts->rk_order > 3) return fail(FLSP_ERR_BAD_ARG, "rk_order must be 1..3");
+  if (!(opts->cfl_max > 0.0)) return fail(FLSP_ERR_BAD_ARG, "cfl_max must be positive");
+  long long ncell = 1;
+  for (int d = 0; d < mesh->dim; ++d) {
+    if (mesh->n[d] < 1 || mesh->n[d] > (1 << 20)) return fail(FLSP_ERR_BAD_MESH, "bad cell count");
+    if (!(mesh->hi[d] > mesh->lo[d])) return fail(FLSP_ERR_BAD_MESH, "empty box");
+    ncell *= mesh->n[d];
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(FLSP_ERR_NO_DEVICE, "no CUDA device visible");
+  if (opts->device < 0 || opts->device >= ndev) return fail(FLSP_ERR_BAD_ARG, "bad device ordinal");
+  CU(cudaSetDevice(opts->device));
+  ST(upload_tables(opts->device));
+
+  flsp_handle* h = new flsp_handle();
+  h->dim = mesh->dim;
+  h->p = opts->degree;
+  h->basis = opts->basis;
+  h->prec = opts->precision;
+  h->rk = opts->rk_order;
+  h->cfl_max = opts->cfl_max;
+  h->dev = opts->device;
+  h->tsize = h->prec == FLSP_FP64 ? 8 : 4;
+  std::memset(&h->m, 0, sizeof(h->m));
+  double d2 = 0.0, vol = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    h->m.n[d] = d < h->dim ? mesh->n[d] : 1;
+    h->m.lo[d] = d < h->dim ? mesh->lo[d] : 0.0;
+    h->m.h[d] = d < h->dim ? (mesh->hi[d] - mesh->lo[d]) / mesh->n[d] : 1.0;
+    if (d < h->dim) { d2 += h->m.h[d] * h->m.h[d]; vol *= h->m.h[d]; }
+  }
+  h->m.ncell = ncell;
+  h->m.vol = vol;
+  h->m.diam = std::sqrt(d2);   // cell diagonal (mesh.implement.h:60-71)
+  h->m.min_diam = h->m.diam;
+  // DoF order inside a cell and its Q-layout map
+  const int n1 = h->p + 1, cz = h->dim > 2 ? h->p : 0;
+  std::memset(h->m.q2g, -1, sizeof(h->m.q2g));
+  std::memset(h->m.g2q, 0, sizeof(h->m.g2q));
+  int nb = 0;
+  if (h->basis == FLSP_BASIS_Q) {
+    for (int c = 0; c <= cz; ++c)
+      for (int b = 0; b <= h->p; ++b)
+        for (int a = 0; a <= h->p; ++a) {
+          const int q = a + n1 * (b + n1 * c);
+          h->m.q2g[q] = (signed char)nb;
+          h->m.g2q[nb++] = (signed char)q;
+        }
+  } else {
+    for (int c = 0; c <= cz; ++c)
+      for (int b = 0; b <= h->p - c; ++b)
+        for (int a = 0; a <= h->p - b - c; ++a) {
+          const int q = a + n1 * (b + n1 * c);
+          h->m.q2g[q] = (signed char)nb;
+          h->m.g2q[nb++] = (signed char)q;
+        }
+  }
+  h->m.nb = nb;
+  h->ndofs = ncell * nb;
+
+  auto cleanup_fail = [&](int code) {
+    flsp_destroy(h);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup_fail(fail(FLSP_ERR_CUDA, "stream creation failed"));
+  for (int i = 0; i < 3; ++i)
+    if (cudaMalloc(&h->buf[i], h->ndofs * h->tsize) != cudaSuccess)
+      return cleanup_fail(fail(FLSP_ERR_OOM, "state allocation failed"));
+  if (cudaMalloc(&h->clk, sizeof(DevClock)) != cudaSuccess ||
+      cudaMallocHost(&h->clk_host, sizeof(DevClock)) != cudaSuccess ||
+      cudaMalloc(&h->stage64, sizeof(double) * (size_t)h->ndofs * 2 * h->dim) != cudaSuccess ||
+      cudaMalloc(&h->red_out, 2 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->ic_dev, sizeof(flsp_ic_desc)) != cudaSuccess ||
+      cudaMalloc(&h->flag_dev, sizeof(unsigned int)) != cudaSuccess)
+    return cleanup_fail(fail(FLSP_ERR_OOM, "allocation failed"));
+  cudaMemset(h->clk, 0, sizeof(DevClock));
+  cudaMemset(h->buf[0], 0, h->ndofs * h->tsize);
+  if (mesh->host_cell_order) {
+    std::vector<char> seen(ncell, 0);
+    for (long long k = 0; k < ncell; ++k) {
+      const int64_t v = mesh->host_cell_order[k];
+      if (v < 0 || v >= ncell || seen[v]) return cleanup_fail(fail(FLSP_ERR_BAD_MESH, "host_cell_order is not a permutation"));
+      seen[v] = 1;
+    }
+    if (cudaMalloc(&h->perm, sizeof(int64_t) * ncell) != cudaSuccess)
+      return cleanup_fail(fail(FLSP_ERR_OOM, "allocation failed"));
+    cudaMemcpy(h->perm, mesh->host_cell_order, sizeof(int64_t) * ncell, cudaMemcpyHostToDevice);
+  }
+  std::memset(&h->vel, 0, sizeof(h->vel));
+  {
+    int st = prepare_kernels(h);
+    if (st) return cleanup_fail(st);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return cleanup_fail(fail(FLSP_ERR_CUDA, "device sync failed"));
+  *out = h;
+  return FLSP_OK;
+}
+
+void flsp_destroy(flsp_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  clear_graphs(h);
+  for (int i = 0; i < 3; ++i) if (h->buf[i]) cudaFree(h->buf[i]);
+  if (h->snap) cudaFree(h->snap);
+  if (h->vtab) cudaFree(h->vtab);
+  if (h->vtab64) cudaFree(h->vtab64);
+  if (h->clk) cudaFree(h->clk);
+  if (h->clk_host) cudaFreeHost(h->clk_host);
+  if (h->perm) cudaFree(h->perm);
+  if (h->stage64) cudaFree(h->stage64);
+  if (h->partial) cudaFree(h->partial);
+  if (h->red_out) cudaFree(h->red_out);
+  if (h->ic_dev) cudaFree(h->ic_dev);
+  if (h->flag_dev) cudaFree(h->flag_dev);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int flsp_n_dofs(const flsp_handle* h, int64_t* n) {
+  if (!h || !n) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *n = h->ndofs;
+  return FLSP_OK;
+}
+
+int flsp_dofs_per_cell(const flsp_handle* h, int* n) {
+  if (!h || !n) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *n = h->m.nb;
+  return FLSP_OK;
+}
+
+int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v) {
+  if (!h || !v) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (v->n_terms < 0 || v->n_terms > FLSP_MAX_VEL_TERMS) return fail(FLSP_ERR_BAD_ARG, "bad n_terms");
+  for (int k = 0; k < v->n_terms; ++k) {
+    if (v->terms[k].comp < 0 || v->terms[k].comp >= h->dim) return fail(FLSP_ERR_BAD_ARG, "bad velocity component");
+    for (int a = 0; a < 3; ++a)
+      if (v->terms[k].f[a].kind < 0 || v->terms[k].f[a].kind > FLSP_F_SINPISQ)
+        return fail(FLSP_ERR_BAD_ARG, "bad factor kind");
+  }
+  if (v->time_kind < 0 || v->time_kind > FLSP_T_ONE_MINUS_EXP) return fail(FLSP_ERR_BAD_ARG, "bad time kind");
+  CU(cudaSetDevice(h->dev));
+  h->vel = *v;
+  ST(build_vtab(h));
+  h->has_vel = true;
+  clear_graphs(h);
+  return prepare_kernels(h);
+}
+
+int flsp_set_state(flsp_handle* h, const double* coeffs, int64_t n) {
+  if (!h || !coeffs) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n != h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
+  CU(cudaSetDevice(h->dev));
+  CU(cudaMemcpyAsync(h->stage64, coeffs, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+  ST(launch_scatter(h->ctx(), h->stage64, h->buf[h->cur], h->perm));
+  CU(cudaStreamSynchronize(h->stream));
+  return check_finite(h, h->buf[h->cur]);
+}
+
+int flsp_get_state(flsp_handle* h, double* coeffs, int64_t n) {
+  if (!h || !coeffs) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n != h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
+  CU(cudaSetDevice(h->dev));
+  ST(launch_gather(h->ctx(), h->buf[h->cur], h->stage64, h->perm));
+  CU(cudaMemcpyAsync(coeffs, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int flsp_set_time(flsp_handle* h, double t) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  ST(sync_clock(h));
+  h->clk_host->t = t;
+  CU(cudaMemcpyAsync(h->clk, h->clk_host, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int flsp_get_time(const flsp_handle* hc, double* t) {
+  flsp_handle* h = const_cast<flsp_handle*>(hc);
+  if (!h || !t) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  CU(cudaSetDevice(h->dev));
+  ST(sync_clock(h));
+  *t = h->clk_host->t;
+  return FLSP_OK;
+}
+
+int flsp_project_ic(flsp_handle* h, const flsp_ic_desc* ic) {
+  if (!h || !ic) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (ic->n_nodes < 1 || ic->n_nodes > FLSP_MAX_IC_NODES || ic->root < 0 || ic->root >= ic->n_nodes ||
+      ic->n_waves < 0 || ic->n_waves > FLSP_MAX_IC_WAVES)
+    return fail(FLSP_ERR_BAD_ARG, "bad IC description");
+  for (int k = 0; k < ic->n_nodes; ++k) {
+    const flsp_ic_node& nd = ic->nodes[k];
+    if (nd.kind < 0 || nd.kind > FLSP_IC_INTERSECT) return fail(FLSP_ERR_BAD_ARG, "bad IC node kind");
+    if (nd.kind >= FLSP_IC_UNION && (nd.a < 0 || nd.a >= k || nd.b < 0 || nd.b >= k))
+      return fail(FLSP_ERR_BAD_ARG, "IC operands must precede their node");
+    if (nd.kind == FLSP_IC_HEIGHT && ((int)nd.p[0] < 0 || (int)nd.p[0] >= h->dim))
+      return fail(FLSP_ERR_BAD_ARG, "bad height-function axis");
+  }
+  CU(cudaSetDevice(h->dev));
+  CU(cudaMemcpyAsync(h->ic_dev, ic, sizeof(flsp_ic_desc), cudaMemcpyHostToDevice, h->stream));
+  ST(launch_project_ic(h->ctx(), h->ic_dev, h->buf[h->cur]));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int flsp_snapshot(flsp_handle* h) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  if (!h->snap) CU(cudaMalloc(&h->snap, h->ndofs * h->tsize));
+  CU(cudaMemcpyAsync(h->snap, h->buf[h->cur], h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  h->has_snap = true;
+  return FLSP_OK;
+}
+
+int flsp_advect_rhs(flsp_handle* h, double t, double* phidot, int64_t n) {
+  if (!h || !phidot) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n != h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  CU(cudaSetDevice(h->dev));
+  const int tmp = (h->cur + 1) % 3;
+  ST(launch_adv_stage(h->ctx(), h->veldev(), h->buf[h->cur], h->buf[h->cur], h->buf[tmp], nullptr, 0,
+                      kRhsOnly, host_time_factor(h->vel, t), h->adv_tile));
+  ST(launch_gather(h->ctx(), h->buf[tmp], h->stage64, h->perm));
+  CU(cudaMemcpyAsync(phidot, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+// AdvectSimulator::advance_time(time_step, compute_single_cycle)
+int flsp_advance(flsp_handle* h, double time_step, int single_cycle, double* advanced) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  if (!(time_step >= 0.0) || !std::isfinite(time_step)) return fail(FLSP_ERR_BAD_ARG, "bad time step");
+  CU(cudaSetDevice(h->dev));
+  ST(launch_adv_clock_horizon(h->stream, h->clk, time_step));
+  double cum = 0.0;
+  long long guard = 0;
+  do {
+    ST(enqueue_adv_step(h));
+    ST(sync_clock(h));
+    cum = h->clk_host->scratch[1];
+    if (!std::isfinite(h->clk_host->dt)) return fail(FLSP_ERR_NONFINITE, "non-finite time step");
+    if (single_cycle) break;
+    if (++guard > 100000000LL) return fail(FLSP_ERR_TIMEOUT, "substep loop did not terminate");
+  } while (!(std::fabs(cum - time_step) <= 2.220446049250313e-16));
+  if (advanced) *advanced = cum;
+  return FLSP_OK;
+}
+
+int flsp_advance_steps(flsp_handle* h, int n_steps, double t_end) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  if (n_steps < 0) return fail(FLSP_ERR_BAD_ARG, "negative step count");
+  CU(cudaSetDevice(h->dev));
+  ST(sync_clock(h));
+  const double horizon = std::isfinite(t_end) ? t_end - h->clk_host->t : INFINITY;
+  ST(launch_adv_clock_horizon(h->stream, h->clk, horizon));
+  for (int i = 0; i < n_steps; ++i) ST(enqueue_adv_step(h));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int flsp_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  int st = run_reinit(h, o, n_iter);
+  cudaStreamSynchronize(h->stream);
+  return st;
+}
+
+int flsp_hj_gradients(flsp_handle* h, double* grads, int64_t n) {
+  if (!h || !grads) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n != 2 * h->dim * h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch (2*dim*n_dofs)");
+  CU(cudaSetDevice(h->dev));
+  void* tmp = nullptr;
+  CU(cudaMalloc(&tmp, (size_t)n * h->tsize));
+  int st = launch_hj(h->ctx(), h->buf[h->cur], h->buf[h->cur], tmp, nullptr, kHJGradients, 1, 0.0,
+                     h->ndofs, h->hj_tile);
+  for (int b = 0; b < 2 * h->dim && st == FLSP_OK; ++b)
+    st = launch_gather(h->ctx(), (const char*)tmp + (size_t)b * h->ndofs * h->tsize,
+                       h->stage64 + b * h->ndofs, h->perm);
+  if (st == FLSP_OK) {
+    cudaMemcpyAsync(grads, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) st = fail(FLSP_ERR_CUDA, "sync failed");
+  }
+  cudaFree(tmp);
+  return st;
+}
+
+int flsp_weno_limit(flsp_handle* h, int* n_troubled) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  CU(cudaMemsetAsync(h->flag_dev, 0, sizeof(unsigned int), h->stream));
+  const int dst = (h->cur + 1) % 3;
+  ST(launch_weno(h->ctx(), h->buf[h->cur], h->buf[dst], h->flag_dev));
+  unsigned int cnt = 0;
+  CU(cudaMemcpyAsync(&cnt, h->flag_dev, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  h->cur = dst;
+  if (n_troubled) *n_troubled = (int)cnt;
+  return FLSP_OK;
+}
+
+// LevelSetSurface::advance_time(time_step, compute_single_step)
+int flsp_ls_advance(flsp_handle* h, const flsp_ls_opts* o, double time_step, int single_step,
+                    double* advanced) {
+  if (!h || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (o->reinit_frequency < 1) return fail(FLSP_ERR_BAD_ARG, "reinit_frequency must be >= 1");
+  double cum = 0.0;
+  long long guard = 0;
+  do {
+    double sub = 0.0;
+    ST(flsp_advance(h, time_step, 1, &sub));
+    h->n_since_reinit++;
+    if (o->execute_reinit && h->n_since_reinit == o->reinit_frequency) {
+      int nit = 0;
+      ST(flsp_reinit(h, &o->reinit, &nit));
+      if (nit) h->n_since_reinit = 0;
+    }
+    cum += sub;
+    time_step -= sub;
+    if (++guard > 100000000LL) return fail(FLSP_ERR_TIMEOUT, "level-set loop did not terminate");
+  } while (!(std::fabs(time_step) <= 2.220446049250313e-16) && !single_step);
+  if (advanced) *advanced = cum;
+  return FLSP_OK;
+}
+
+// n_steps advection substeps, fixed-count reinit every reinit_frequency
+// steps; one reinit period is captured into a CUDA graph and replayed
+int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
+  if (!h || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  if (n_steps < 0 || o->reinit_frequency < 1) return fail(FLSP_ERR_BAD_ARG, "bad step counts");
+  flsp_reinit_opts ro = o->reinit;
+  if (o->execute_reinit) {
+    if (ro.mode != FLSP_REINIT_FIXED)
+      return fail(FLSP_ERR_BAD_ARG, "flsp_ls_run_steps needs a fixed-count reinit (FLSP_REINIT_FIXED)");
+    ST(validate_reinit(h, &ro));
+  }
+  CU(cudaSetDevice(h->dev));
+  ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
+  int done = 0;
+  while (done < n_steps) {
+    const int to_reinit = o->execute_reinit ? o->reinit_frequency - h->n_since_reinit : n_steps - done;
+    if (to_reinit <= 0) { h->n_since_reinit = 0; continue; }
+    if (done + to_reinit <= n_steps && o->execute_reinit) {
+      // a full period: replay (or capture) the graph for this buffer role
+      const long long key = ((long long)h->cur << 40) ^ ((long long)to_reinit << 20) ^
+                            ((long long)ro.n_pseudo_steps << 4) ^ (reinit_limiter(h, &ro) ? 1 : 0);
+      auto it = h->graphs.find(key);
+      if (it == h->graphs.end()) {
+        const int cur0 = h->cur;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int st = FLSP_OK;
+        for (int s = 0; s < to_reinit && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
+        if (st == FLSP_OK) {
+          const bool limiter = reinit_limiter(h, &ro);
+          const int phi0 = h->cur;
+          st = launch_hj_clock_reset(h->stream, h->clk);
+          if (st == FLSP_OK)
+            st = launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, ro.rk_order, 0.0,
+                           h->ndofs, h->hj_tile);
+          for (int k = 0; k < ro.n_pseudo_steps && st == FLSP_OK; ++k) st = enqueue_hj_step(h, &ro, phi0, limiter);
+        }
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+        if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); h->cur = cur0; return st; }
+        if (ce != cudaSuccess) return fail(FLSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        GraphEntry ge;
+        ge.cur_after = h->cur;
+        h->cur = cur0;
+        CU(cudaGraphInstantiate(&ge.exec, g, 0));
+        cudaGraphDestroy(g);
+        it = h->graphs.emplace(key, ge).first;
+      }
+      CU(cudaGraphLaunch(it->second.exec, h->stream));
+      h->cur = it->second.cur_after;
+      done += to_reinit;
+      h->n_since_reinit = 0;
+    } else {
+      const int k = std::min(to_reinit, n_steps - done);
+      for (int s = 0; s < k; ++s) ST(enqueue_adv_step(h));
+      done += k;
+      h->n_since_reinit += k;
+    }
+  }
+  return FLSP_OK;
+}
+
+int flsp_sync(flsp_handle* h) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
+}
+
+int flsp_stream(const flsp_handle* h, void** stream) {
+  if (!h || !stream) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *stream = (void*)h->stream;
+  return FLSP_OK;
+}
+
+int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch) {
+  if (!h || !ms_per_launch || reps < 1) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  if (which == 0 && !h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  CU(cudaSetDevice(h->dev));
+  CU(cudaStreamSynchronize(h->stream));
+  const int x = h->cur, y = (h->cur + 1) % 3, z = (h->cur + 2) % 3;
+  if (which == 0) {
+    // a valid substep on the clock (idempotent: the CFL maximum is a max)
+    AdvClockArgs ca;
+    ca.cfl_max = h->cfl_max;
+    ca.scale = adv_cfl_scaling(h->p);
+    ca.tkind = h->vel.time_kind;
+    ca.ta = h->vel.ta;
+    ca.tb = h->vel.tb;
+    ca.rk = h->rk;
+    ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
+    ST(launch_adv_clock_begin(h->stream, h->clk, ca));
+  } else {
+    ST(launch_hj_clock_reset(h->stream, h->clk));
+  }
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  int st = FLSP_OK;
+  // one untimed round, then the timed repetitions
+  for (int pass = 0; pass < 2 && st == FLSP_OK; ++pass) {
+    if (pass == 1) cudaEventRecord(e0, h->stream);
+    const int n = pass == 0 ? 1 : reps;
+    for (int r = 0; r < n && st == FLSP_OK; ++r) {
+      if (which == 0) {
+        st = stage(h, h->buf[x], h->buf[x], h->buf[y], 0, kRK3a);
+        if (st == FLSP_OK) st = stage(h, h->buf[y], h->buf[x], h->buf[z], 1, kRK3b);
+        if (st == FLSP_OK) st = stage(h, h->buf[z], h->buf[x], h->buf[y], 2, kRK3c);
+      } else {
+        st = launch_hj(h->ctx(), h->buf[x], h->buf[x], h->buf[y], h->clk, kHJStep, 1, 0.0, h->ndofs,
+                       h->hj_tile);
+      }
+    }
+  }
+  cudaEventRecord(e1, h->stream);
+  cudaError_t ce = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (st == FLSP_OK && ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  if (ce != cudaSuccess) return fail(FLSP_ERR_CUDA, cudaGetErrorString(ce));
+  *ms_per_launch = (double)ms / (double)(reps * (which == 0 ? 3 : 1));
+  return FLSP_OK;
+}
+
+int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic, double* out) {
+  if (!h || !out) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  CU(cudaSetDevice(h->dev));
+  const bool need_ic = which == FLSP_RED_MASS_ERROR || which == FLSP_RED_L2_ERROR_IC ||
+                       which == FLSP_RED_L1_INTERFACE_IC;
+  const bool need_ref = which == FLSP_RED_L1_INTERFACE || which == FLSP_RED_MEAN_ABS_DIFF;
+  if (which < 0 || which > FLSP_RED_MASS_SHARP) return fail(FLSP_ERR_BAD_ARG, "bad reduction kind");
+  if (need_ic) {
+    if (!ic) return fail(FLSP_ERR_BAD_ARG, "reduction needs an IC");
+    CU(cudaMemcpyAsync(h->ic_dev, ic, sizeof(flsp_ic_desc), cudaMemcpyHostToDevice, h->stream));
+  }
+  if (need_ref && !h->has_snap) return fail(FLSP_ERR_BAD_ARG, "reduction needs flsp_snapshot first");
+  double r[2];
+  ST(reduce_dev(h, which, h->buf[h->cur], need_ref ? h->snap : nullptr, need_ic, r));
+  switch (which) {
+    case FLSP_RED_MASS_ERROR: *out = (r[0] - r[1]) / r[1]; break;
+    case FLSP_RED_MEAN_ABS_DIFF: *out = r[0] / (double)h->ndofs; break;
+    case FLSP_RED_GRAD_DEVIATION: *out = r[0] / r[1]; break;
+    case FLSP_RED_L2_ERROR_IC: *out = std::sqrt(r[0]); break;
+    default: *out = r[0];
+  }
+  return FLSP_OK;
+}
+
+}  // extern "C"

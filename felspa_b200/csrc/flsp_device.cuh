@@ -1,0 +1,250 @@
+// flsp_device.cuh — device-side building blocks shared by every kernel of
+// libflsp_dg.so: 1D Legendre/Gauss tables in constant memory, the device
+// clock, parameter blocks, small reduction helpers.
+//
+// Data layout in HBM: one array of n_cells * nb coefficients per state
+// vector, cells lexicographic (x fastest), nb DoFs of a cell contiguous in
+// deal.II order (FE_DGQLegendre lexicographic, FE_DGP total-degree order).
+// Inside a CTA every cell is expanded to the Q layout of (p+1)^dim modes
+// (zero where the P space has no mode), so one code path serves both bases.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace flsp {
+
+constexpr int kMaxP = 3;
+constexpr int kMaxN1 = kMaxP + 1;   // modes per axis
+constexpr int kMaxNQ = kMaxP + 2;   // Gauss points per axis (p+2 rule)
+constexpr int kMaxTerms = 24;
+
+__host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+// 1D tables for one polynomial degree p (entries beyond p unused)
+template <typename T>
+struct Tab1D {
+  T xq[kMaxNQ], wq[kMaxNQ];            // Gauss (p+2) points/weights on [0,1]
+  T Lq[kMaxN1][kMaxNQ];                 // L_a(xq)
+  T Dq[kMaxN1][kMaxNQ];                 // L_a'(xq)
+  T Hq[kMaxN1][kMaxNQ];                 // L_a''(xq)
+  T L0[kMaxN1], L1[kMaxN1];             // L_a(0), L_a(1)
+  T D0[kMaxN1], D1[kMaxN1];             // L_a'(0), L_a'(1)
+  T H0[kMaxN1], H1[kMaxN1];             // L_a''(0), L_a''(1)
+  T A[kMaxN1][kMaxN1];                  // int_0^1 L_a' L_b
+  T xl[kMaxN1], wl[kMaxN1];             // Gauss (p+1) points/weights
+  T Ll[kMaxN1][kMaxN1];                 // L_a(xl)
+  T Dl[kMaxN1][kMaxN1];                 // L_a'(xl)
+};
+
+// Every translation unit of the library holds its own copy of the tables
+// (no relocatable device code); flsp_upload_tables_<unit>() fills it.
+static __constant__ Tab1D<double> c_tab_d[kMaxP + 1];
+static __constant__ Tab1D<float> c_tab_f[kMaxP + 1];
+
+template <typename T> __device__ __forceinline__ const Tab1D<T>& tab(int p);
+template <> __device__ __forceinline__ const Tab1D<double>& tab<double>(int p) { return c_tab_d[p]; }
+template <> __device__ __forceinline__ const Tab1D<float>& tab<float>(int p) { return c_tab_f[p]; }
+
+// ---------------------------------------------------------------------
+// device clock: simulation time and CFL state live on the GPU so that a
+// whole reinit period can be replayed from a CUDA graph without host
+// synchronisation.  All fields in double (clocks are FP64 in both modes).
+// ---------------------------------------------------------------------
+struct DevClock {
+  double t;          // time at the start of the current substep
+  double dt;         // current substep
+  double vd_run;     // running max of (max vertex |u|)/diam (never reset:
+                     // the reference CFLEstimator keeps its maximum)
+  double t_end;      // clamp for the substep (time_step - cumulative)
+  double ct[3];      // velocity time factor at the RK stage times
+  double vd_static;  // max over vertices of |u_spatial| / diam
+  int active;        // current substep is non-zero
+  int pending;       // dt still to be added to t
+  int n_substeps;    // executed substeps
+  int err;           // device error word (0 = ok)
+  // reinitialisation
+  double hj_vd_run;  // running max of characteristic speed / diam
+  double hj_dt;      // current pseudo-step
+  double hj_cum;     // accumulated pseudo-time (before the current step)
+  unsigned long long hj_vd_bits;  // atomicMax slot for the next CFL estimate
+  int hj_iter;
+  int hj_pending;
+  double band_ratio; // accumulated pseudo-time / horizon (host convenience)
+  double scratch[4];
+};
+
+// stage combinations of the SSP-RK schemes (time_integration.implement.h:141-234)
+enum CombineMode : int {
+  kRhsOnly = 0,     // out = phidot
+  kRK1 = 1,         // out = phidot*dt + phi
+  kRK2a = 2,        // out = phi + dt*phidot
+  kRK2b = 3,        // out = (phi1 + dt*phidot + phin) * 0.5
+  kRK3a = 4,        // out = phi + dt*phidot
+  kRK3b = 5,        // out = (phi1 + dt*phidot + 3 phin) * 0.25
+  kRK3c = 6         // out = ((phi2 + dt*phidot) * 2 + phin) * (1/3)
+};
+
+// modes of the reinitialisation kernel
+enum HJMode : int { kHJCflOnly = 0, kHJStep = 1, kHJGradients = 2 };
+
+// advection clock parameters (scale = AdvectSimulator::cfl_scaling(p))
+struct AdvClockArgs {
+  double cfl_max, scale;
+  int tkind;
+  double ta, tb;
+  int rk;
+};
+
+// time factor kinds (flsp_time_kind)
+__device__ __forceinline__ double time_factor(int kind, double a, double b, double t) {
+  switch (kind) {
+    case 1: return cos(a * t + b);
+    case 2: return cospi(a * t + b);
+    case 3: return 1.0 - exp(-a * t);
+    default: return 1.0;
+  }
+}
+
+// positive doubles compare like their bit patterns
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* slot, double v) {
+  if (!(v > 0.0)) return;
+  atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block-wide max of a non-negative double, result valid in thread 0
+__device__ __forceinline__ double block_max(double v, double* red) {
+  v = warp_max(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double x = l < nw ? red[l] : 0.0;
+    x = warp_max(x);
+    if (l == 0) red[0] = x;
+  }
+  __syncthreads();
+  return red[0];
+}
+
+// ---------------------------------------------------------------------
+// mesh / tile description passed by value to every stencil kernel
+// ---------------------------------------------------------------------
+struct MeshArgs {
+  int n[3];          // cells per axis (1 for unused axes)
+  long long ncell;
+  double lo[3], h[3];
+  double vol, diam, min_diam;
+  int nb;            // DoFs per cell in HBM
+  signed char q2g[64];  // Q-layout mode -> in-cell DoF index (-1: absent)
+  signed char g2q[64];  // in-cell DoF index -> Q-layout mode
+  int tile[3];       // CTA tile in cells
+  int ntile[3];      // tiles per axis
+};
+
+// separable velocity: vtab[((k*3 + axis) * nmax + i) * npt + j]
+// j < NQ: Gauss (p+2) point j of cell i; j == NQ: xi = 0; j == NQ+1: xi = 1
+template <typename T>
+struct VelArgs {
+  const T* vtab;
+  int n_terms;
+  int nmax;
+  int npt;
+  int comp[kMaxTerms];
+};
+
+// local (tile) coordinates of the thread's cell
+struct TileCoord {
+  int lx, ly, lz;     // in [0, tile)
+  int gx, gy, gz;     // global lattice coordinates
+  bool valid;
+  int ox, oy, oz;     // tile origin
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim) {
+  TileCoord c;
+  int b = blockIdx.x;
+  const int bx = b % m.ntile[0];
+  b /= m.ntile[0];
+  const int by = dim > 1 ? b % m.ntile[1] : 0;
+  const int bz = dim > 2 ? b / m.ntile[1] : 0;
+  c.ox = bx * m.tile[0];
+  c.oy = by * m.tile[1];
+  c.oz = bz * m.tile[2];
+  int t = threadIdx.x;
+  c.lx = t % m.tile[0];
+  t /= m.tile[0];
+  c.ly = dim > 1 ? t % m.tile[1] : 0;
+  c.lz = dim > 2 ? t / m.tile[1] : 0;
+  c.gx = c.ox + c.lx;
+  c.gy = c.oy + c.ly;
+  c.gz = c.oz + c.lz;
+  c.valid = (int)threadIdx.x < m.tile[0] * m.tile[1] * m.tile[2] && c.gx < m.n[0] &&
+            c.gy < m.n[1] && c.gz < m.n[2];
+  return c;
+}
+
+// padded smem box (tile + 1 halo layer per axis, edge/corner slots unused)
+__device__ __forceinline__ int box_index(const MeshArgs& m, int dim, int lx, int ly, int lz) {
+  const int bx = m.tile[0] + 2, by = dim > 1 ? m.tile[1] + 2 : 1;
+  return (lx + 1) + bx * ((dim > 1 ? ly + 1 : 0) + by * (dim > 2 ? lz + 1 : 0));
+}
+
+__device__ __forceinline__ int box_cells(const MeshArgs& m, int dim) {
+  return (m.tile[0] + 2) * (dim > 1 ? m.tile[1] + 2 : 1) * (dim > 2 ? m.tile[2] + 2 : 1);
+}
+
+// Cooperative load of the tile and its face halo (no edges/corners) from a
+// cell-major vector into the smem box, expanded to the Q layout.  Rows of
+// cells along x are contiguous in HBM, so consecutive threads read
+// consecutive addresses.  Slots of cells outside the domain are not
+// written (boundary faces never read them).
+template <int DIM, int NM, typename T>
+__device__ __forceinline__ void load_box(const MeshArgs& m, const T* __restrict__ g,
+                                         T* __restrict__ sm, int ox, int oy, int oz,
+                                         bool with_halo) {
+  const int tx = m.tile[0], ty = DIM > 1 ? m.tile[1] : 1, tz = DIM > 2 ? m.tile[2] : 1;
+  const int h = with_halo ? 1 : 0;
+  // rows: (ly, lz) in [-h, ty+h) x [-h, tz+h), excluding corners
+  const int nry = ty + 2 * (DIM > 1 ? h : 0), nrz = tz + 2 * (DIM > 2 ? h : 0);
+  const int ly0 = DIM > 1 ? -h : 0, lz0 = DIM > 2 ? -h : 0;
+  for (int r = 0; r < nry * nrz; ++r) {
+    const int ly = ly0 + r % nry, lz = lz0 + r / nry;
+    const bool yout = ly < 0 || ly >= ty, zout = lz < 0 || lz >= tz;
+    if (yout && zout) continue;
+    const int gy = oy + ly, gz = oz + lz;
+    if (gy < 0 || gy >= m.n[1] || gz < 0 || gz >= m.n[2]) continue;
+    // interior rows get the x halo too; halo rows only the tile span
+    const int lx0 = (!yout && !zout) ? -h : 0;
+    const int lx1 = (!yout && !zout) ? tx + h : tx;
+    const int gx0 = max(ox + lx0, 0), gx1 = min(ox + lx1, m.n[0]);
+    if (gx1 <= gx0) continue;
+    const long long rowcell = (long long)m.n[0] * (gy + (long long)m.n[1] * gz);
+    const int count = (gx1 - gx0) * NM;
+    for (int e = threadIdx.x; e < count; e += blockDim.x) {
+      const int cx = e / NM, q = e - cx * NM;
+      const int gx = gx0 + cx;
+      const int gi = m.q2g[q];
+      T v = T(0);
+      if (gi >= 0) v = g[(rowcell + gx) * m.nb + gi];
+      sm[box_index(m, DIM, gx - ox, ly, lz) * NM + q] = v;
+    }
+  }
+}
+
+}  // namespace flsp

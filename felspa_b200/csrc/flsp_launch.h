@@ -1,0 +1,106 @@
+// flsp_launch.h — host launchers exported by the kernel units
+// (flsp_k_adv.cu, flsp_k_hj.cu, flsp_k_misc.cu) to the C-ABI unit.
+// Launchers return a flsp_status and leave a message through set_error().
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <type_traits>
+
+#include "flsp_device.cuh"
+#include "flsp_dg.h"
+
+namespace flsp {
+
+int set_error(int code, const std::string& msg);
+
+struct Ctx {
+  int dim, p, prec;
+  MeshArgs m;          // tile fields are filled by the launchers
+  cudaStream_t stream;
+};
+
+inline bool supported_config(int dim, int p) {
+  return (dim == 2 && p >= 1 && p <= 3) || (dim == 3 && p >= 1 && p <= 2);
+}
+
+// compile-time dispatch over the built (dim, degree, precision) variants
+template <typename F>
+int dispatch(const Ctx& c, F&& f) {
+#define FLSP_CASE(D, PP)                                                                      \
+  if (c.dim == D && c.p == PP) {                                                              \
+    if (c.prec == FLSP_FP64)                                                                  \
+      return f(std::integral_constant<int, D>(), std::integral_constant<int, PP>(), (double)0); \
+    return f(std::integral_constant<int, D>(), std::integral_constant<int, PP>(), (float)0);  \
+  }
+  FLSP_CASE(2, 1)
+  FLSP_CASE(2, 2)
+  FLSP_CASE(2, 3)
+  FLSP_CASE(3, 1)
+  FLSP_CASE(3, 2)
+#undef FLSP_CASE
+  return set_error(FLSP_ERR_UNSUPPORTED, "unsupported (dim, degree)");
+}
+
+inline void set_tile(MeshArgs& m, int dim, const int* t) {
+  for (int d = 0; d < 3; ++d) {
+    m.tile[d] = d < dim ? t[d] : 1;
+    m.ntile[d] = (m.n[d] + m.tile[d] - 1) / m.tile[d];
+  }
+}
+inline long long nblocks(const MeshArgs& m) { return (long long)m.ntile[0] * m.ntile[1] * m.ntile[2]; }
+
+inline int launch_status(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return FLSP_OK;
+}
+
+// ---------------- tables (one per unit) ----------------
+int upload_tables_adv();
+int upload_tables_hj();
+int upload_tables_misc();
+
+// ---------------- advection (flsp_k_adv.cu) ----------------
+struct VelDev {
+  const void* vtab;    // T-precision table
+  int n_terms, nmax, npt;
+  int comp[kMaxTerms];
+};
+// tile: cells per CTA (nullptr = default); smem attribute is set on first use
+int adv_default_tile(const Ctx& c, int n_terms, int* tile);
+int adv_prepare(const Ctx& c, int n_terms, const int* tile);
+int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* phin, void* out,
+                     const DevClock* clk, int stage, int combine, double ct_explicit,
+                     const int* tile);
+
+// ---------------- reinitialisation (flsp_k_hj.cu) ----------------
+int hj_default_tile(const Ctx& c, int* tile);
+int hj_prepare(const Ctx& c, const int* tile);
+int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClock* clk, int mode,
+              int rk, double dt_explicit, long long block, const int* tile);
+
+// ---------------- misc (flsp_k_misc.cu) ----------------
+int weno_prepare(const Ctx& c);
+int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count);
+int launch_project_ic(const Ctx& c, const flsp_ic_desc* ic_dev, void* out);
+int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int* comp, int nmax,
+                      int npt, DevClock* clk);
+// two-level FP64 reduction; partial holds 2 * reduce_blocks(c) doubles,
+// out_dev receives two doubles (sum pair, or max)
+int launch_reduce(const Ctx& c, int which, const void* phi, const void* ref,
+                  const flsp_ic_desc* ic_dev, double* partial, double* out_dev);
+int reduce_blocks(const Ctx& c);
+int launch_scatter(const Ctx& c, const double* src, void* dst, const int64_t* perm);
+int launch_gather(const Ctx& c, const void* src, double* dst, const int64_t* perm);
+int launch_nonfinite(const Ctx& c, const void* x, long long n, unsigned int* count);
+
+int launch_adv_clock_begin(cudaStream_t s, DevClock* clk, const AdvClockArgs& a);
+int launch_adv_clock_end(cudaStream_t s, DevClock* clk);
+int launch_adv_clock_horizon(cudaStream_t s, DevClock* clk, double time_step);
+int launch_hj_clock_reset(cudaStream_t s, DevClock* clk);
+int launch_hj_clock_begin(cudaStream_t s, DevClock* clk, double cfl_max, int p, double nu,
+                          double min_diam, double adv_scale);
+int launch_hj_clock_end(cudaStream_t s, DevClock* clk);
+
+}  // namespace flsp

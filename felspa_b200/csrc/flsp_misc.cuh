@@ -1,0 +1,422 @@
+// flsp_misc.cuh — small kernels around the two stencil kernels: device
+// clocks, host<->device DoF order, initial-condition projection, FP64
+// diagnostics reductions, the static part of the advection CFL.
+#pragma once
+#include "flsp_device.cuh"
+#include "flsp_dg.h"
+
+namespace flsp {
+
+constexpr double kPiD = 3.14159265358979323846;
+constexpr double kEpsD = 2.220446049250313e-16;
+
+// ---------------------------------------------------------------------
+// clocks
+// ---------------------------------------------------------------------
+
+// AdvectSimulator::advance_time substep set-up (advection.cc:396-404):
+// CFL estimate at the current time (running maximum, the estimator never
+// resets), substep = min(cfl_max / estimate, remaining), stage time factors.
+__global__ void adv_clock_begin(DevClock* c, const AdvClockArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double ctn = time_factor(a.tkind, a.ta, a.tb, c->t);
+  const double vd = fabs(ctn) * c->vd_static;
+  c->vd_run = fmax(c->vd_run, vd);
+  const double suggest = a.cfl_max / (c->vd_run * a.scale);
+  const double remaining = c->scratch[0] - c->scratch[1];   // time_step - cumulative
+  const double dt = fmin(suggest, remaining);
+  c->dt = dt;
+  c->active = fabs(dt) <= kEpsD ? 0 : 1;   // TempoIntegrator skips zero steps
+  c->ct[0] = ctn;
+  c->ct[1] = time_factor(a.tkind, a.ta, a.tb, c->t + dt);
+  c->ct[2] = time_factor(a.tkind, a.ta, a.tb, c->t + 0.5 * dt);
+}
+
+__global__ void adv_clock_end(DevClock* c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (c->active) {
+    c->t += c->dt;
+    c->n_substeps += 1;
+  }
+  c->scratch[1] += c->dt;   // cumulative time of this advance call
+}
+
+// start an advance call of length time_step (scratch[0]); +inf = unclamped
+__global__ void adv_clock_horizon(DevClock* c, double time_step) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  c->scratch[0] = time_step;
+  c->scratch[1] = 0.0;
+}
+
+__global__ void hj_clock_reset(DevClock* c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  c->hj_vd_run = 0.0;
+  c->hj_dt = 0.0;
+  c->hj_cum = 0.0;
+  c->hj_vd_bits = 0ull;
+  c->hj_iter = 0;
+}
+
+// ReinitSimulatorLDG::advance_time step size (reinit.cc:396-408) with
+// HJSimulator::cfl_scaling (hamilton_jacobi.cc:554-580)
+__global__ void hj_clock_begin(DevClock* c, double cfl_max, int p, double nu, double min_diam,
+                               double adv_scale) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double vd = __longlong_as_double((long long)c->hj_vd_bits);
+  c->hj_vd_bits = 0ull;
+  c->hj_vd_run = fmax(c->hj_vd_run, vd);
+  double scale;
+  if (nu > 0.0)
+    scale = pow((double)(p + 1), 2.0) * c->hj_vd_run + nu * pow((double)(p + 1), 4.0) / pow(min_diam, 2.0);
+  else
+    scale = adv_scale * c->hj_vd_run;
+  c->hj_dt = cfl_max / scale;
+}
+
+__global__ void hj_clock_end(DevClock* c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  c->hj_cum += c->hj_dt;
+  c->hj_iter += 1;
+}
+
+// ---------------------------------------------------------------------
+// host DoF order <-> device layout (optional cell permutation)
+// ---------------------------------------------------------------------
+template <typename T>
+__global__ void scatter_state(const double* __restrict__ src, T* __restrict__ dst,
+                              const int64_t* __restrict__ perm, long long ncell, int nb) {
+  const long long n = ncell * nb;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / nb, j = i - k * nb;
+    const long long cell = perm ? perm[k] : k;
+    dst[cell * nb + j] = T(src[i]);
+  }
+}
+
+template <typename T>
+__global__ void gather_state(const T* __restrict__ src, double* __restrict__ dst,
+                             const int64_t* __restrict__ perm, long long ncell, int nb) {
+  const long long n = ncell * nb;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long k = i / nb, j = i - k * nb;
+    const long long cell = perm ? perm[k] : k;
+    dst[i] = double(src[cell * nb + j]);
+  }
+}
+
+// ---------------------------------------------------------------------
+// initial conditions (src/level_set/geometry.cc:17-235, geometry.h:80-160)
+// nodes are evaluated in index order; children precede their parents
+// ---------------------------------------------------------------------
+__device__ inline double ic_eval(const flsp_ic_desc* ic, int dim, const double* x) {
+  double val[FLSP_MAX_IC_NODES];
+  for (int k = 0; k < ic->n_nodes; ++k) {
+    const flsp_ic_node& nd = ic->nodes[k];
+    double r = 0.0;
+    switch (nd.kind) {
+      case FLSP_IC_SPHERE: {
+        double s = 0.0;
+        for (int d = 0; d < dim; ++d) { const double e = x[d] - nd.p[d]; s += e * e; }
+        r = sqrt(s) - nd.p[3];
+        break;
+      }
+      case FLSP_IC_RECT: {
+        double out2 = 0.0;
+        bool inside = true;
+        for (int d = 0; d < dim; ++d) {
+          double e = 0.0;
+          if (x[d] < nd.p[d]) { e = x[d] - nd.p[d]; inside = false; }
+          else if (x[d] > nd.p[3 + d]) { e = x[d] - nd.p[3 + d]; inside = false; }
+          out2 += e * e;
+        }
+        if (!inside) { r = sqrt(out2); break; }
+        double mm = -1e300;
+        for (int d = 0; d < dim; ++d) {
+          mm = fmax(mm, nd.p[d] - x[d]);
+          mm = fmax(mm, x[d] - nd.p[3 + d]);
+        }
+        r = mm;
+        break;
+      }
+      case FLSP_IC_HEIGHT: {
+        const int ax = (int)nd.p[0];
+        int u = -1, v = -1;
+        for (int d = 0; d < dim; ++d)
+          if (d != ax) { if (u < 0) u = d; else v = d; }
+        double hgt = nd.p[1];
+        for (int w = 0; w < ic->n_waves; ++w) {
+          double arg = ic->waves[w][1] * x[u];
+          if (v >= 0) arg += ic->waves[w][2] * x[v];
+          hgt += ic->waves[w][0] * cos(2.0 * kPiD * arg + ic->waves[w][3]);
+        }
+        r = x[ax] - hgt;
+        break;
+      }
+      case FLSP_IC_UNION: r = fmin(val[nd.a], val[nd.b]); break;
+      case FLSP_IC_DIFF: r = fmax(val[nd.a], -val[nd.b]); break;
+      case FLSP_IC_INTERSECT: r = fmax(val[nd.a], val[nd.b]); break;
+    }
+    val[k] = r;
+  }
+  return val[ic->root];
+}
+
+// evaluate the DG function of one cell at reference point (table columns)
+template <int DIM, int P>
+__device__ __forceinline__ double eval_modal(const double* c, const double* bx, const double* by,
+                                             const double* bz) {
+  constexpr int N1 = P + 1;
+  double s = 0.0;
+  if constexpr (DIM == 2) {
+#pragma unroll
+    for (int b = 0; b < N1; ++b) {
+      double r = 0.0;
+#pragma unroll
+      for (int a = 0; a < N1; ++a) r += c[a + N1 * b] * bx[a];
+      s += r * by[b];
+    }
+  } else {
+#pragma unroll
+    for (int cc = 0; cc < N1; ++cc)
+#pragma unroll
+      for (int b = 0; b < N1; ++b) {
+        double r = 0.0;
+#pragma unroll
+        for (int a = 0; a < N1; ++a) r += c[a + N1 * (b + N1 * cc)] * bx[a];
+        s += r * by[b] * bz[cc];
+      }
+  }
+  return s;
+}
+
+// L2 projection with QGauss(p+2) (advection.cc:145-161); always in FP64
+template <int DIM, int P, typename T>
+__global__ void project_ic_kernel(const MeshArgs m, const flsp_ic_desc* __restrict__ ic,
+                                  T* __restrict__ out) {
+  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM);
+  const Tab1D<double>& tb = c_tab_d[P];
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= m.ncell) return;
+  const int gx = (int)(cell % m.n[0]);
+  const int gy = (int)((cell / m.n[0]) % m.n[1]);
+  const int gz = DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0;
+  const double x0[3] = {m.lo[0] + gx * m.h[0], m.lo[1] + gy * m.h[1], DIM > 2 ? m.lo[2] + gz * m.h[2] : 0.0};
+  double R[NM];
+#pragma unroll
+  for (int q = 0; q < NM; ++q) R[q] = 0.0;
+  const int nqz = DIM > 2 ? NQ : 1;
+  for (int qz = 0; qz < nqz; ++qz)
+    for (int qy = 0; qy < NQ; ++qy)
+      for (int qx = 0; qx < NQ; ++qx) {
+        double x[3] = {x0[0] + m.h[0] * tb.xq[qx], x0[1] + m.h[1] * tb.xq[qy],
+                       DIM > 2 ? x0[2] + m.h[2] * tb.xq[qz] : 0.0};
+        double f = ic_eval(ic, DIM, x);
+        double w = tb.wq[qx] * tb.wq[qy];
+        if (DIM > 2) w *= tb.wq[qz];
+        const double fw = f * w;
+#pragma unroll
+        for (int q = 0; q < NM; ++q) {
+          const int i0 = q % N1, i1 = (q / N1) % N1, i2 = q / (N1 * N1);
+          double bw = tb.Lq[i0][qx] * tb.Lq[i1][qy];
+          if (DIM > 2) bw *= tb.Lq[i2][qz];
+          R[q] += fw * bw;
+        }
+      }
+  for (int k = 0; k < m.nb; ++k) out[cell * m.nb + k] = T(R[m.g2q[k]]);
+}
+
+// ---------------------------------------------------------------------
+// static CFL part: max over cells and vertices of |u_spatial| / diam
+// (CFLEstimator::local_estimate, pde_tools.implement.h:44-57)
+// ---------------------------------------------------------------------
+template <int DIM>
+__global__ void static_cfl_kernel(const MeshArgs m, const VelArgs<double> v, DevClock* clk) {
+  __shared__ double red[32];
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double best = 0.0;
+  if (cell < m.ncell) {
+    const int g[3] = {(int)(cell % m.n[0]), (int)((cell / m.n[0]) % m.n[1]),
+                      DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0};
+    const int NQ = v.npt - 2;
+    for (int vv = 0; vv < (1 << DIM); ++vv) {
+      double u[3] = {0.0, 0.0, 0.0};
+      for (int k = 0; k < v.n_terms; ++k) {
+        double tv = 1.0;
+        for (int d = 0; d < DIM; ++d) {
+          const int j = NQ + ((vv >> d) & 1);
+          tv *= v.vtab[((size_t)(k * 3 + d) * v.nmax + g[d]) * v.npt + j];
+        }
+        u[v.comp[k]] += tv;
+      }
+      double s = 0.0;
+      for (int d = 0; d < DIM; ++d) s += u[d] * u[d];
+      best = fmax(best, sqrt(s));
+    }
+    best /= m.diam;
+  }
+  const double bm = block_max(best, red);
+  if (threadIdx.x == 0) {
+    unsigned long long* slot = reinterpret_cast<unsigned long long*>(&clk->vd_static);
+    atomic_max_pos(slot, bm);
+  }
+}
+
+// ---------------------------------------------------------------------
+// FP64 reductions (level_set.implement.h:215-295, 356-380, 957-993;
+// advection.cc:452-484; reinit.cc:491-526).  Two levels, fixed order.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ double heaviside_sine(double x, double eps) {
+  if (x > eps) return 1.0;
+  if (x < -eps) return 0.0;
+  const double val = 0.5 * (1.0 + x / eps + sin(x * kPiD / eps) / kPiD);
+  if (fabs(val) < kEpsD) return 0.0;
+  if (fabs(val - 1.0) < kEpsD) return 1.0;
+  return val;
+}
+__device__ __forceinline__ double heaviside_sharp(double x) {
+  return x > 0.0 ? 1.0 : (x < 0.0 ? 0.0 : 0.5);
+}
+
+template <typename T>
+struct RedArgs {
+  MeshArgs m;
+  const T* phi;
+  const T* ref;
+  const flsp_ic_desc* ic;
+  int which;
+  double* partial;   // [gridDim.x][2]
+};
+
+template <int DIM, int P, typename T>
+__global__ void reduce_kernel(const RedArgs<T> a) {
+  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM);
+  __shared__ double red[2][32];
+  const MeshArgs& m = a.m;
+  const Tab1D<double>& tb = c_tab_d[P];
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double s0 = 0.0, s1 = 0.0;
+  if (cell < m.ncell) {
+    double c[NM], r[NM];
+#pragma unroll
+    for (int q = 0; q < NM; ++q) {
+      const int gi = m.q2g[q];
+      c[q] = gi >= 0 ? double(a.phi[cell * m.nb + gi]) : 0.0;
+      r[q] = (gi >= 0 && a.ref) ? double(a.ref[cell * m.nb + gi]) : 0.0;
+    }
+    const int g[3] = {(int)(cell % m.n[0]), (int)((cell / m.n[0]) % m.n[1]),
+                      DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0};
+    const double eps = 1.5 * m.min_diam;
+    const int w = a.which;
+    if (w == FLSP_RED_MEAN_ABS_DIFF) {
+      for (int k = 0; k < m.nb; ++k) s0 += fabs(double(a.phi[cell * m.nb + k]) - double(a.ref[cell * m.nb + k]));
+    } else if (w == FLSP_RED_MAX_ABS) {
+      for (int k = 0; k < m.nb; ++k) s0 = fmax(s0, fabs(double(a.phi[cell * m.nb + k])));
+    } else {
+      const bool gauss_p1 = (w == FLSP_RED_MASS || w == FLSP_RED_MASS_ERROR ||
+                             w == FLSP_RED_GRAD_DEVIATION || w == FLSP_RED_L2_ERROR_IC);
+      const int nq = gauss_p1 ? N1 : NQ;
+      const int nqz = DIM > 2 ? nq : 1;
+      double cellacc = 0.0;
+      for (int qz = 0; qz < nqz; ++qz)
+        for (int qy = 0; qy < nq; ++qy)
+          for (int qx = 0; qx < nq; ++qx) {
+            const int qq[3] = {qx, qy, qz};
+            double bx[N1], by[N1], bz[N1], dx[N1], dy[N1], dz[N1], xx[3], wgt = 1.0;
+            for (int d = 0; d < 3; ++d) xx[d] = 0.0;
+            for (int i = 0; i < N1; ++i) {
+              bx[i] = gauss_p1 ? tb.Ll[i][qx] : tb.Lq[i][qx];
+              by[i] = gauss_p1 ? tb.Ll[i][qy] : tb.Lq[i][qy];
+              bz[i] = DIM > 2 ? (gauss_p1 ? tb.Ll[i][qz] : tb.Lq[i][qz]) : 1.0;
+              dx[i] = gauss_p1 ? tb.Dl[i][qx] : tb.Dq[i][qx];
+              dy[i] = gauss_p1 ? tb.Dl[i][qy] : tb.Dq[i][qy];
+              dz[i] = DIM > 2 ? (gauss_p1 ? tb.Dl[i][qz] : tb.Dq[i][qz]) : 1.0;
+            }
+            for (int d = 0; d < DIM; ++d) {
+              const double xi = gauss_p1 ? tb.xl[qq[d]] : tb.xq[qq[d]];
+              xx[d] = (m.lo[d] + g[d] * m.h[d]) + m.h[d] * xi;
+              wgt *= gauss_p1 ? tb.wl[qq[d]] : tb.wq[qq[d]];
+            }
+            const double jxw = wgt * m.vol;
+            const double val = eval_modal<DIM, P>(c, bx, by, bz);
+            if (w == FLSP_RED_MASS || w == FLSP_RED_MASS_ERROR) {
+              s0 += heaviside_sine(-val, eps) * jxw;
+              if (w == FLSP_RED_MASS_ERROR) s1 += heaviside_sine(-ic_eval(a.ic, DIM, xx), eps) * jxw;
+            } else if (w == FLSP_RED_MASS_SHARP) {
+              s0 += heaviside_sharp(-val) * jxw;
+            } else if (w == FLSP_RED_L1_INTERFACE) {
+              s0 += fabs(heaviside_sharp(-val) - heaviside_sharp(-eval_modal<DIM, P>(r, bx, by, bz))) * jxw;
+            } else if (w == FLSP_RED_L1_INTERFACE_IC) {
+              s0 += fabs(heaviside_sharp(-val) - heaviside_sharp(-ic_eval(a.ic, DIM, xx))) * jxw;
+            } else if (w == FLSP_RED_L2_ERROR_IC) {
+              const double diff = val - ic_eval(a.ic, DIM, xx);
+              cellacc += diff * diff * jxw;
+            } else if (w == FLSP_RED_GRAD_DEVIATION) {
+              const double gxv = eval_modal<DIM, P>(c, dx, by, bz) / m.h[0];
+              const double gyv = eval_modal<DIM, P>(c, bx, dy, bz) / m.h[1];
+              const double gzv = DIM > 2 ? eval_modal<DIM, P>(c, bx, by, dz) / m.h[2] : 0.0;
+              const double g2 = gxv * gxv + gyv * gyv + gzv * gzv;
+              s0 += fabs(sqrt(g2) - 1.0) * jxw;
+            }
+          }
+      if (w == FLSP_RED_L2_ERROR_IC) s0 += cellacc;
+      if (w == FLSP_RED_GRAD_DEVIATION) s1 += m.vol;
+    }
+  }
+  if (a.which == FLSP_RED_MAX_ABS) {
+    const double bm = block_max(s0, red[0]);
+    if (threadIdx.x == 0) { a.partial[2 * blockIdx.x] = bm; a.partial[2 * blockIdx.x + 1] = 0.0; }
+    return;
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  const int wi = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { red[0][wi] = s0; red[1][wi] = s1; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < nw; ++i) { t0 += red[0][i]; t1 += red[1][i]; }
+    a.partial[2 * blockIdx.x] = t0;
+    a.partial[2 * blockIdx.x + 1] = t1;
+  }
+}
+
+__global__ void reduce_final(const double* __restrict__ partial, int n, int is_max, double* out) {
+  __shared__ double red[2][32];
+  double s0 = 0.0, s1 = 0.0;
+  // fixed assignment of partials to threads -> deterministic
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (is_max) s0 = fmax(s0, partial[2 * i]);
+    else { s0 += partial[2 * i]; s1 += partial[2 * i + 1]; }
+  }
+  if (is_max) {
+    const double bm = block_max(s0, red[0]);
+    if (threadIdx.x == 0) { out[0] = bm; out[1] = 0.0; }
+    return;
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  const int wi = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { red[0][wi] = s0; red[1][wi] = s1; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) { t0 += red[0][i]; t1 += red[1][i]; }
+    out[0] = t0;
+    out[1] = t1;
+  }
+}
+
+// finite check of a state vector: counts non-finite entries
+template <typename T>
+__global__ void nonfinite_kernel(const T* __restrict__ x, long long n, unsigned int* count) {
+  unsigned int local = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    if (!isfinite((double)x[i])) ++local;
+  if (local) atomicAdd(count, local);
+}
+
+}  // namespace flsp

@@ -1,0 +1,299 @@
+"""Host-side mirror of FELSPA's level-set simulator interface, on top of the
+C ABI of libflsp_dg.so.
+
+Class and method names follow the reference so that a driver written
+against it reads the same:
+
+* ``AdvectSimulator``   — dg::AdvectSimulator (include/felspa/pde/advection.h:91-381)
+* ``ReinitSimulatorLDG`` — dg::ReinitSimulatorLDG (include/felspa/level_set/reinit.h:154-268)
+* ``LevelSetSurface``   — ls::LevelSetSurface (include/felspa/level_set/level_set.h:176-413)
+
+All three drive one device-resident problem (``Problem``): the reference's
+reinit simulator shares the advection solution vector, and so do these.
+Errors from the library surface as ``FlspError`` (the reference throws
+EXCEPT_MSG exceptions, base/exceptions.h:227-245).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .lib import check, dp, load
+
+# ----------------------------------------------------------------------
+# mesh helpers
+# ----------------------------------------------------------------------
+
+
+def dealii_hypercube_order(dim, n_subdiv, n_refine):
+    """Active-cell order of deal.II's subdivided_hyper_cube(n_subdiv) refined
+    n_refine times globally: coarse cells lexicographic, the children of
+    every cell in lexicographic (x fastest) order, depth first.  Returns, for
+    each cell of that order, its lexicographic lattice index (the
+    permutation flsp_create takes as host_cell_order)."""
+    N = n_subdiv * 2 ** n_refine
+    order = []
+
+    def rec(ix, iy, iz, level):
+        if level == n_refine:
+            order.append(ix + N * (iy + N * iz))
+            return
+        for cz in range(2 if dim == 3 else 1):
+            for cy in range(2):
+                for cx in range(2):
+                    rec(2 * ix + cx, 2 * iy + cy, 2 * iz + cz, level + 1)
+
+    for kz in range(n_subdiv if dim == 3 else 1):
+        for ky in range(n_subdiv):
+            for kx in range(n_subdiv):
+                rec(kx, ky, kz, 0)
+    return np.asarray(order, dtype=np.int64)
+
+
+class Mesh:
+    """Uniform Cartesian mesh of a box (the part of dealii::Triangulation the
+    hot path needs): cells per axis, corners, optional host cell order."""
+
+    def __init__(self, dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=None):
+        self.dim = dim
+        self.n = tuple(int(v) for v in n[:dim])
+        self.lo = tuple(float(v) for v in lo[:dim])
+        self.hi = tuple(float(v) for v in hi[:dim])
+        self.host_cell_order = None if host_cell_order is None else np.ascontiguousarray(
+            host_cell_order, dtype=np.int64)
+
+    @property
+    def n_cells(self):
+        return int(np.prod(self.n))
+
+    @property
+    def min_diameter(self):
+        h = [(self.hi[d] - self.lo[d]) / self.n[d] for d in range(self.dim)]
+        return float(np.sqrt(sum(x * x for x in h)))
+
+    def desc(self):
+        order = None
+        if self.host_cell_order is not None:
+            order = self.host_cell_order.ctypes.data_as(C.POINTER(C.c_int64))
+        return abi.mesh_desc(self.dim, self.n, self.lo, self.hi, order)
+
+
+# ----------------------------------------------------------------------
+# one device-resident problem
+# ----------------------------------------------------------------------
+class Problem:
+    def __init__(self, mesh, fe_degree, basis=abi.BASIS_Q, precision=abi.FP64, rk_order=3,
+                 cfl_max=0.9, device=0):
+        L = load()
+        self.mesh = mesh
+        self.fe_degree = fe_degree
+        self.basis = basis
+        self.precision = precision
+        self._mdesc = mesh.desc()
+        o = abi.DGOpts()
+        L.flsp_default_dg_opts(C.byref(o))
+        o.degree = fe_degree
+        o.basis = basis
+        o.precision = precision
+        o.rk_order = rk_order
+        o.cfl_max = cfl_max
+        o.device = device
+        h = C.c_void_p()
+        check(L.flsp_create(C.byref(self._mdesc), C.byref(o), C.byref(h)))
+        self.h = h
+        n = C.c_int64(0)
+        check(L.flsp_n_dofs(h, C.byref(n)))
+        self.n_dofs = n.value
+        nb = C.c_int(0)
+        check(L.flsp_dofs_per_cell(h, C.byref(nb)))
+        self.dofs_per_cell = nb.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().flsp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # state ------------------------------------------------------------
+    def set_velocity(self, field):
+        self._vdesc = field.desc()
+        check(load().flsp_set_velocity(self.h, C.byref(self._vdesc)))
+
+    def project(self, ic):
+        self._icdesc = ic.desc()
+        check(load().flsp_project_ic(self.h, C.byref(self._icdesc)))
+
+    def set_state(self, coeffs):
+        a = np.ascontiguousarray(coeffs, dtype=np.float64)
+        check(load().flsp_set_state(self.h, dp(a), a.size))
+
+    def get_state(self):
+        out = np.empty(self.n_dofs)
+        check(load().flsp_get_state(self.h, dp(out), out.size))
+        return out
+
+    def get_time(self):
+        t = C.c_double(0.0)
+        check(load().flsp_get_time(self.h, C.byref(t)))
+        return t.value
+
+    def set_time(self, t):
+        check(load().flsp_set_time(self.h, float(t)))
+
+    def snapshot(self):
+        check(load().flsp_snapshot(self.h))
+
+    def sync(self):
+        check(load().flsp_sync(self.h))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(load().flsp_stream(self.h, C.byref(s)))
+        return s.value
+
+    def time_kernel(self, which, reps=20):
+        """average ms per launch of a hot kernel (0: advection stage, 1: reinit step)."""
+        ms = C.c_double(0.0)
+        check(load().flsp_time_kernel(self.h, int(which), int(reps), C.byref(ms)))
+        return ms.value
+
+    def reduce(self, which, ic=None):
+        out = C.c_double(0.0)
+        icd = C.byref(ic.desc()) if ic is not None else None
+        check(load().flsp_reduce(self.h, which, icd, C.byref(out)))
+        return out.value
+
+
+# ----------------------------------------------------------------------
+# reference-named simulators
+# ----------------------------------------------------------------------
+class AdvectSimulator:
+    """dg::AdvectSimulator: DG advection with CFL-limited SSP-RK substeps."""
+
+    def __init__(self, mesh, fe_degree, basis=abi.BASIS_Q, precision=abi.FP64, rk_order=3,
+                 cfl_max=0.9, device=0, problem=None):
+        self.problem = problem or Problem(mesh, fe_degree, basis, precision, rk_order, cfl_max, device)
+
+    @property
+    def n_dofs(self):
+        return self.problem.n_dofs
+
+    def initialize(self, initial_condition, velocity_field):
+        """AdvectSimulator::initialize(ScalarFunction | vector, ptr_velocity_field)."""
+        self.problem.set_velocity(velocity_field)
+        if isinstance(initial_condition, np.ndarray):
+            self.problem.set_state(initial_condition)
+        else:
+            self.problem.project(initial_condition)
+
+    def explicit_time_derivative(self, current_time):
+        """phidot = M^-1 R(phi, t) of the current solution (advection.cc:269-296)."""
+        out = np.empty(self.n_dofs)
+        check(load().flsp_advect_rhs(self.problem.h, float(current_time), dp(out), out.size))
+        return out
+
+    def advance_time(self, time_step, compute_single_cycle=False):
+        """AdvectSimulator::advance_time(time_step, compute_single_cycle) (advection.cc:359-426)."""
+        adv = C.c_double(0.0)
+        check(load().flsp_advance(self.problem.h, float(time_step), 1 if compute_single_cycle else 0,
+                                  C.byref(adv)))
+        return adv.value
+
+    def advance_steps(self, n_steps, t_end=float("inf")):
+        """n CFL-limited substeps with the time step kept on the device."""
+        check(load().flsp_advance_steps(self.problem.h, int(n_steps), float(t_end)))
+
+    def get_solution_vector(self):
+        return self.problem.get_state()
+
+    def get_time(self):
+        return self.problem.get_time()
+
+    def compute_error(self, reference):
+        """compute_error(vector): mean |coefficient difference| (advection.cc:471-484);
+        compute_error(ic): L2 error against an analytic IC with QGauss(p+1) (:452-468)."""
+        if isinstance(reference, np.ndarray):
+            return float(np.abs(self.get_solution_vector() - reference).mean())
+        return self.problem.reduce(abi.RED_L2_ERROR_IC, reference)
+
+
+class ReinitSimulatorLDG:
+    """dg::ReinitSimulatorLDG acting on the advection solution in place."""
+
+    def __init__(self, problem, control=None):
+        self.problem = problem
+        self.control = control if control is not None else abi.default_reinit_opts()
+
+    def run_iteration(self, control=None):
+        """initialize(solution) + run_iteration(); returns the iteration count."""
+        o = control if control is not None else self.control
+        nit = C.c_int(0)
+        check(load().flsp_reinit(self.problem.h, C.byref(o), C.byref(nit)))
+        return nit.value
+
+    def local_left_right_gradients(self):
+        """(left, right) LDG gradients, each of shape (dim, n_dofs)."""
+        d = self.problem.mesh.dim
+        out = np.empty(2 * d * self.problem.n_dofs)
+        check(load().flsp_hj_gradients(self.problem.h, dp(out), out.size))
+        g = out.reshape(2 * d, -1)
+        return g[:d], g[d:]
+
+    def apply_weno_limiter(self):
+        n = C.c_int(0)
+        check(load().flsp_weno_limit(self.problem.h, C.byref(n)))
+        return n.value
+
+
+class LevelSetSurface(AdvectSimulator):
+    """ls::LevelSetSurface<AdvectSimulator, ReinitSimulatorLDG>."""
+
+    def __init__(self, mesh, fe_degree, basis=abi.BASIS_Q, precision=abi.FP64, rk_order=3,
+                 cfl_max=0.9, device=0, control=None):
+        super().__init__(mesh, fe_degree, basis, precision, rk_order, cfl_max, device)
+        self.control = control if control is not None else abi.default_ls_opts()
+        self.reinit_simulator = ReinitSimulatorLDG(self.problem, self.control.reinit)
+
+    def initialize(self, initial_condition, velocity_field):
+        """level_set.implement.h:119-142: project the IC; a non-exact IC gets a
+        global reinit."""
+        super().initialize(initial_condition, velocity_field)
+        if not isinstance(initial_condition, np.ndarray) and not initial_condition.exact:
+            o = abi.ReinitOpts.from_buffer_copy(self.control.reinit)
+            o.mode = abi.REINIT_GLOBAL
+            self.reinit_simulator.run_iteration(o)
+
+    def advance_time(self, time_step, compute_single_step=False):
+        """LevelSetSurface::advance_time(time_step, compute_single_step) (level_set.implement.h:180-205)."""
+        adv = C.c_double(0.0)
+        check(load().flsp_ls_advance(self.problem.h, C.byref(self.control), float(time_step),
+                                     1 if compute_single_step else 0, C.byref(adv)))
+        return adv.value
+
+    def run_steps(self, n_steps, sync=True):
+        """n advection substeps with a fixed-count reinit every reinit_frequency
+        steps, replayed from captured CUDA graphs (enqueued asynchronously;
+        sync=True waits for completion)."""
+        check(load().flsp_ls_run_steps(self.problem.h, C.byref(self.control), int(n_steps)))
+        if sync:
+            self.problem.sync()
+
+    # diagnostics (FP64 device reductions)
+    def integrate_mass(self):
+        return self.problem.reduce(abi.RED_MASS)
+
+    def compute_mass_error(self, analytical_soln):
+        return self.problem.reduce(abi.RED_MASS_ERROR, analytical_soln)
+
+    def interface_error_l1(self, analytical_soln=None):
+        if analytical_soln is None:
+            return self.problem.reduce(abi.RED_L1_INTERFACE)
+        return self.problem.reduce(abi.RED_L1_INTERFACE_IC, analytical_soln)
+
+    def gradient_deviation(self):
+        return self.problem.reduce(abi.RED_GRAD_DEVIATION)

@@ -1,0 +1,295 @@
+/*
+ * flsp_dg.h — C ABI of the B200 level-set hot path (DG advection + HJ
+ * reinitialization) of FELSPA.
+ *
+ * One handle = one level-set problem on a uniform Cartesian mesh, resident
+ * on one GPU, driven through one CUDA stream.  Host pointers passed to any
+ * call are borrowed for the duration of that call only.  Every call returns
+ * an int status (FLSP_OK == 0); flsp_last_error() gives a thread-local
+ * message.  No C++ exception crosses this boundary.
+ *
+ * Reference interfaces each entry point replaces (paths inside the FELSPA
+ * source tree):
+ *   flsp_create / flsp_destroy     dg::AdvectSimulator ctor + do_initialize
+ *                                  (include/felspa/pde/src/advection.implement.h:22-83)
+ *   flsp_project_ic                AdvectSimulator::discretize_function_to_solution
+ *                                  (src/pde/advection.cc:145-169)
+ *   flsp_set_state / flsp_get_state  AdvectSimulator::initialize(vector) and
+ *                                  get_solution_vector (advection.implement.h:119-131)
+ *   flsp_set_velocity              AdvectSimulator::initialize(..., ptr_velocity_field)
+ *                                  (advection.implement.h:86-115)
+ *   flsp_advect_rhs                AdvectSimulator::explicit_time_derivative
+ *                                  (src/pde/advection.cc:269-296)
+ *   flsp_advance                   AdvectSimulator::advance_time(dt, single)
+ *                                  (src/pde/advection.cc:359-426)
+ *   flsp_reinit                    ReinitSimulatorLDG::initialize + run_iteration
+ *                                  (src/level_set/reinit.cc:386-393,529-637)
+ *   flsp_ls_advance                LevelSetSurface::advance_time(dt, single)
+ *                                  (include/felspa/level_set/src/level_set.implement.h:180-205)
+ *   flsp_hj_gradients              HJSimulator::local_left_right_gradients
+ *                                  (src/pde/hamilton_jacobi.cc:462-511)
+ *   flsp_weno_limit                dg::apply_weno_limiter
+ *                                  (include/felspa/pde/src/pde_tools.implement.h:977-1004)
+ *   flsp_reduce                    LevelSetSurface::compute_mass_error / integrate_mass
+ *                                  (level_set.implement.h:215-295), AdvectSimulator::
+ *                                  compute_error (advection.cc:452-484),
+ *                                  ReinitSimulatorLDG::gradient_deviation (reinit.cc:491-526)
+ */
+#ifndef FLSP_DG_H
+#define FLSP_DG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+enum flsp_status {
+  FLSP_OK = 0,
+  FLSP_ERR_CUDA = 1,              /* a CUDA runtime call failed          */
+  FLSP_ERR_NONFINITE = 2,         /* NaN/Inf found in state or input     */
+  FLSP_ERR_BAD_ARG = 3,           /* invalid argument / size mismatch    */
+  FLSP_ERR_BAD_MESH = 4,          /* mesh / permutation failed checks    */
+  FLSP_ERR_TIMEOUT = 5,           /* bounded device loop gave up         */
+  FLSP_ERR_BAND_NOT_REACHED = 6,  /* reinit hit max_iter (ExcNotEnoughStepsForWidth) */
+  FLSP_ERR_UNSUPPORTED = 7,       /* (dim, degree, basis) not compiled   */
+  FLSP_ERR_NO_DEVICE = 8,         /* no CUDA device visible              */
+  FLSP_ERR_OOM = 9                /* device allocation failed            */
+};
+
+enum flsp_basis {
+  FLSP_BASIS_P = 0, /* FE_DGP: Legendre, total degree <= p (reference)  */
+  FLSP_BASIS_Q = 1  /* FE_DGQLegendre: Legendre tensor product          */
+};
+
+enum flsp_precision {
+  FLSP_FP64 = 0, /* parity mode: every operation in double             */
+  FLSP_FP32 = 1  /* production: stencil arithmetic in float; clocks,
+                    CFL and all reductions in double                    */
+};
+
+/* ------------------------------------------------------------------ */
+/* mesh: uniform Cartesian box, cells numbered lexicographically       */
+/* (x fastest) on the device.                                          */
+/* ------------------------------------------------------------------ */
+typedef struct flsp_mesh_desc {
+  int dim;          /* 2 or 3                                            */
+  int n[3];         /* cells per axis                                    */
+  double lo[3];     /* lower corner                                      */
+  double hi[3];     /* upper corner                                      */
+  /* Optional host cell order: host_cell_order[k] = lexicographic lattice
+     index of the k-th cell of the host DoF vector (for example the active
+     cell order of a refined deal.II hyper cube).  NULL = lexicographic.
+     Must be a permutation of 0..n_cells-1 (checked at create).          */
+  const int64_t* host_cell_order;
+} flsp_mesh_desc;
+
+typedef struct flsp_dg_opts {
+  int degree;      /* 1..3 (3D: 1..2)                                    */
+  int basis;       /* flsp_basis                                         */
+  int precision;   /* flsp_precision                                     */
+  int rk_order;    /* advection SSP-RK order 1..3, reference default 3   */
+  double cfl_max;  /* advection CFL upper bound, reference default 0.9   */
+  int device;      /* CUDA device ordinal                                */
+} flsp_dg_opts;
+
+/* ------------------------------------------------------------------ */
+/* prescribed velocity: a sum of separable terms                       */
+/*   u_comp(x,t) += coeff * f_0(x_0) f_1(x_1) f_2(x_2) * c(t)           */
+/* every field the reference and the benchmark configurations use      */
+/* (rigid rotation, single vortex, 3D deformation, Fourier stream      */
+/* function, plume rolls, constant) is such a sum.                     */
+/* ------------------------------------------------------------------ */
+enum flsp_factor_kind {
+  FLSP_F_ONE = 0,      /* 1                          */
+  FLSP_F_LIN = 1,      /* a*x + b                    */
+  FLSP_F_SIN = 2,      /* sin(a*x + b)               */
+  FLSP_F_COS = 3,      /* cos(a*x + b)               */
+  FLSP_F_SINSQ = 4,    /* sin(a*x + b)^2             */
+  FLSP_F_SINPI = 5,    /* sin(pi*(a*x + b))          */
+  FLSP_F_COSPI = 6,    /* cos(pi*(a*x + b))          */
+  FLSP_F_SINPISQ = 7   /* sin(pi*(a*x + b))^2        */
+};
+
+enum flsp_time_kind {
+  FLSP_T_ONE = 0,           /* 1                     */
+  FLSP_T_COS = 1,           /* cos(a*t + b)          */
+  FLSP_T_COSPI = 2,         /* cos(pi*(a*t + b))     */
+  FLSP_T_ONE_MINUS_EXP = 3  /* 1 - exp(-a*t)         */
+};
+
+typedef struct flsp_factor {
+  int kind;
+  double a, b;
+} flsp_factor;
+
+#define FLSP_MAX_VEL_TERMS 24
+typedef struct flsp_vel_term {
+  int comp;            /* velocity component 0..dim-1 */
+  double coeff;
+  flsp_factor f[3];    /* factor per axis (axis 2 ignored in 2D) */
+} flsp_vel_term;
+
+typedef struct flsp_velocity_desc {
+  int n_terms;
+  flsp_vel_term terms[FLSP_MAX_VEL_TERMS];
+  int time_kind;       /* flsp_time_kind, one factor for all components */
+  double ta, tb;
+} flsp_velocity_desc;
+
+/* ------------------------------------------------------------------ */
+/* initial condition: small CSG tree of signed-distance primitives     */
+/* (reference: include/felspa/level_set/geometry.h:80-160)             */
+/* ------------------------------------------------------------------ */
+enum flsp_ic_kind {
+  FLSP_IC_SPHERE = 0,     /* p[0..2] centre, p[3] radius: |x-c| - r            */
+  FLSP_IC_RECT = 1,       /* p[0..2] lower, p[3..5] upper corner: box SDF      */
+  FLSP_IC_HEIGHT = 2,     /* x_axis - (p[1] + sum_m w0 cos(2 pi (w1 x_u + w2 x_v) + w3)),
+                             axis = (int)p[0]; u,v = the other axes           */
+  FLSP_IC_UNION = 3,      /* min(a, b)                                         */
+  FLSP_IC_DIFF = 4,       /* max(a, -b)                                        */
+  FLSP_IC_INTERSECT = 5   /* max(a, b)                                         */
+};
+
+#define FLSP_MAX_IC_NODES 32
+#define FLSP_MAX_IC_WAVES 32
+typedef struct flsp_ic_node {
+  int kind;
+  int a, b;            /* child node indices (CSG ops) */
+  double p[6];
+} flsp_ic_node;
+
+typedef struct flsp_ic_desc {
+  int n_nodes;
+  int root;
+  int exact;           /* reference ICBase::exact; non-exact ICs get a
+                          global reinit at initialisation              */
+  flsp_ic_node nodes[FLSP_MAX_IC_NODES];
+  int n_waves;         /* shared by FLSP_IC_HEIGHT nodes */
+  double waves[FLSP_MAX_IC_WAVES][4];
+} flsp_ic_desc;
+
+/* ------------------------------------------------------------------ */
+/* reinitialization options (reference: src/level_set/reinit.h:276-341) */
+/* ------------------------------------------------------------------ */
+enum flsp_reinit_mode {
+  FLSP_REINIT_BAND = 0,   /* iterate while pseudo-time < band_width_coeff * min_diam */
+  FLSP_REINIT_GLOBAL = 1, /* iterate while pseudo-time < 1.2 * max|coeff|            */
+  FLSP_REINIT_FIXED = 2   /* exactly n_pseudo_steps pseudo-steps (device resident)   */
+};
+
+typedef struct flsp_reinit_opts {
+  int mode;                /* flsp_reinit_mode, reference default BAND   */
+  int n_pseudo_steps;      /* FIXED mode                                 */
+  double band_width_coeff; /* reference default 4.0                      */
+  int max_iter;            /* reference default 1000                     */
+  double cfl_max;          /* reference ReinitControl default 0.2        */
+  double viscosity;        /* LDG artificial viscosity, default 0        */
+  int rk_order;            /* reference default 1                        */
+  int limiter;             /* 2D WENO limiter: -1 = reference (on in 2D) */
+  int narrow_band;         /* 1 = only cells within band_cells of the
+                              interface are updated (not in reference)   */
+  double band_cells;       /* compute band half-width, in cell diameters */
+} flsp_reinit_opts;
+
+/* level-set driver options (reference: level_set.h:108-166) */
+typedef struct flsp_ls_opts {
+  int reinit_frequency;    /* reference default 10 */
+  int execute_reinit;      /* reference default 1  */
+  flsp_reinit_opts reinit;
+} flsp_ls_opts;
+
+/* reductions (flsp_reduce `which`) */
+enum flsp_reduce_kind {
+  FLSP_RED_MASS = 0,          /* sum H_eps(-phi) JxW, QGauss(p+1), sine Heaviside,
+                                 eps = 1.5 min_diam (integrate_mass)               */
+  FLSP_RED_MASS_ERROR = 1,    /* (mass(phi) - mass(ic)) / mass(ic) vs flsp_ic_desc  */
+  FLSP_RED_L1_INTERFACE = 2,  /* int |H(-phi) - H(-phi_ref)| dx, sharp H, QGauss(p+2);
+                                 reference = the saved snapshot                     */
+  FLSP_RED_MEAN_ABS_DIFF = 3, /* mean |coeff - coeff_ref| (compute_error(vector))    */
+  FLSP_RED_GRAD_DEVIATION = 4,/* mean over domain of ||grad phi| - 1|, QGauss(p+1)   */
+  FLSP_RED_MAX_ABS = 5,       /* max |coeff|                                         */
+  FLSP_RED_L2_ERROR_IC = 6,   /* L2 norm of phi - ic, QGauss(p+1)                    */
+  FLSP_RED_L1_INTERFACE_IC = 7,/* int |H(-phi) - H(-ic)| dx, sharp H, QGauss(p+2)    */
+  FLSP_RED_MASS_SHARP = 8     /* sum H(-phi) JxW with the sharp Heaviside, QGauss(p+2) */
+};
+
+typedef struct flsp_handle flsp_handle;
+
+/* lifetime ----------------------------------------------------------- */
+int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts,
+                flsp_handle** out);
+void flsp_destroy(flsp_handle* h);
+const char* flsp_last_error(void);
+int flsp_version(void);
+
+/* sizes -------------------------------------------------------------- */
+int flsp_n_dofs(const flsp_handle* h, int64_t* n_dofs);
+int flsp_dofs_per_cell(const flsp_handle* h, int* n);
+
+/* state -------------------------------------------------------------- */
+int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v);
+int flsp_project_ic(flsp_handle* h, const flsp_ic_desc* ic);
+int flsp_set_state(flsp_handle* h, const double* coeffs, int64_t n);
+int flsp_get_state(flsp_handle* h, double* coeffs, int64_t n);
+int flsp_set_time(flsp_handle* h, double t);
+int flsp_get_time(const flsp_handle* h, double* t);
+/* save the current state as the comparison snapshot of the reductions */
+int flsp_snapshot(flsp_handle* h);
+
+/* advection ---------------------------------------------------------- */
+/* phidot = M^-1 R(phi, t) of the current state, in host DoF order */
+int flsp_advect_rhs(flsp_handle* h, double t, double* phidot, int64_t n);
+/* AdvectSimulator::advance_time(time_step, single_cycle): CFL-limited
+   SSP-RK substeps until time_step is consumed (or one substep).        */
+int flsp_advance(flsp_handle* h, double time_step, int single_cycle,
+                 double* advanced);
+/* n_steps CFL-limited substeps with no host synchronisation in between
+   (dt is computed on the device), optionally clamped at t_end.        */
+int flsp_advance_steps(flsp_handle* h, int n_steps, double t_end);
+
+/* reinitialization ---------------------------------------------------- */
+int flsp_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter);
+/* left/right LDG gradients of the current state: 2*dim blocks of n dofs,
+   left blocks first, host DoF order                                    */
+int flsp_hj_gradients(flsp_handle* h, double* grads, int64_t n);
+/* one application of the 2D minmod detector + WENO limiter             */
+int flsp_weno_limit(flsp_handle* h, int* n_troubled);
+
+/* level-set driver ---------------------------------------------------- */
+int flsp_ls_advance(flsp_handle* h, const flsp_ls_opts* o, double time_step,
+                    int single_step, double* advanced);
+/* n_steps advection substeps with a reinit every reinit_frequency steps
+   (fixed-count reinit), replayed from a captured CUDA graph.  Returns once
+   the work is enqueued on the handle's stream; flsp_sync() waits for it
+   (flsp_get_state and the reductions synchronise by themselves).        */
+int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps);
+int flsp_sync(flsp_handle* h);
+/* the handle's cudaStream_t (for callers that order their own work or
+   record CUDA events against the library's work)                       */
+int flsp_stream(const flsp_handle* h, void** stream);
+
+/* measurement helper, no counterpart in the reference: average device
+   time (ms, CUDA events on the handle's stream) of one launch of a
+   hot-path kernel over `reps` back-to-back repetitions; the state is not
+   modified.  which: 0 = advection stage kernel (the three SSP-RK3 stages
+   per repetition), 1 = reinit pseudo-step kernel.                      */
+int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch);
+
+/* reductions ---------------------------------------------------------- */
+int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic,
+                double* out);
+
+/* default option structs (reference defaults) */
+void flsp_default_dg_opts(flsp_dg_opts* o);
+void flsp_default_reinit_opts(flsp_reinit_opts* o);
+void flsp_default_ls_opts(flsp_ls_opts* o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLSP_DG_H */
