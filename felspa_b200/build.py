@@ -25,9 +25,23 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompil
          "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 
 
-def headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    return hs + [os.path.join(ROOT, "include", "flsp_dg.h")]
+def deps(path, seen=None):
+    """the file and every local header it includes, recursively"""
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include \""):
+                name = line.split('"')[1]
+                for d in (CSRC, os.path.join(ROOT, "include")):
+                    cand = os.path.join(d, name)
+                    if os.path.exists(cand):
+                        deps(cand, seen)
+                        break
+    return seen
 
 
 def _stale(target, deps):
@@ -40,7 +54,7 @@ def _stale(target, deps):
 def _compile(unit, verbose):
     src = os.path.join(CSRC, unit)
     obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
-    if not _stale(obj, [src] + headers()):
+    if not _stale(obj, sorted(deps(src))):
         return obj, ""
     cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj + ".tmp"]
     if verbose:

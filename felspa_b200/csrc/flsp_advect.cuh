@@ -12,6 +12,8 @@
 // flux is evaluated at the (p+2)^(dim-1) face points.  phidot = R / |K| is
 // formed in "per volume" units directly (faces scale with 1/h_e).
 #pragma once
+#include <type_traits>
+
 #include "flsp_device.cuh"
 
 namespace flsp {
@@ -54,36 +56,154 @@ __device__ __forceinline__ T term_val(const T* __restrict__ vx, const T* __restr
   return v;
 }
 
-// shared-memory footprint of the stage kernel
+// shared-memory footprint of the stage kernel: tile box with face halo,
+// velocity-table rows of the tile, upper-face fluxes shared with the
+// upper neighbours
 template <int DIM, int P, typename T>
 __host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms) {
-  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2;
+  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
+  const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
   size_t vt = (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
-  return box + vt;
+  size_t fl = (size_t)DIM * NF * nt * sizeof(T);
+  return box + vt + fl;
 }
 
-template <int DIM, int P, typename T>
-__global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
-  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2;
+// Upwind flux through face (E, S) of a cell (S = 1: upper face, outward
+// normal +e_E), projected onto the face modes:
+//   Fm[m] = sum_q w_q v_n(q) phi_hat(q) L_m(q),  v_n = (S ? 1 : -1) u_E,
+//   phi_hat = v_n > 0 ? own trace : neighbour trace (own trace on the
+// boundary: zero-Neumann inflow, advection.implement.h:719-741).
+// vel_e(q0, q1) returns the weighted normal component u_E(q) w_q (w_q > 0,
+// so its sign is the sign of u_E).
+template <int DIM, int P, int E, int S, typename T, typename VelE>
+__device__ __forceinline__ void face_flux(const Tab1D<T>& tb, const T* c, const T* cn, bool has_nb,
+                                          VelE&& vel_e, T* Fm) {
+  constexpr int N1 = P + 1, NQ = P + 2, NF = ipow(N1, DIM - 1);
+  constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  constexpr int st[3] = {1, N1, N1 * N1};
+  T tin[NF], tex[NF];
+#pragma unroll
+  for (int mf = 0; mf < NF; ++mf) {
+    const int m0 = mf % N1, m1 = mf / N1;
+    const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
+    T si = T(0), sx = T(0);
+#pragma unroll
+    for (int a = 0; a < N1; ++a) {
+      si += (S ? tb.L1[a] : tb.L0[a]) * c[base + a * st[E]];
+      if (has_nb) sx += (S ? tb.L0[a] : tb.L1[a]) * cn[base + a * st[E]];
+    }
+    tin[mf] = si;
+    tex[mf] = has_nb ? sx : si;
+  }
+  if constexpr (DIM == 2) {
+#pragma unroll
+    for (int m0 = 0; m0 < N1; ++m0) Fm[m0] = T(0);
+#pragma unroll
+    for (int q0 = 0; q0 < NQ; ++q0) {
+      T pin = T(0), pex = T(0);
+#pragma unroll
+      for (int m0 = 0; m0 < N1; ++m0) {
+        pin += tin[m0] * tb.Lq[m0][q0];
+        pex += tex[m0] * tb.Lq[m0][q0];
+      }
+      const T uw = vel_e(q0, 0);
+      const T vn = S ? uw : -uw;
+      const T up = vn > T(0) ? pin : pex;
+      const T F = vn * up;
+#pragma unroll
+      for (int m0 = 0; m0 < N1; ++m0) Fm[m0] += F * tb.Lq[m0][q0];
+    }
+  } else {
+    T Pi[NQ][N1], Pe[NQ][N1];
+#pragma unroll
+    for (int q0 = 0; q0 < NQ; ++q0)
+#pragma unroll
+      for (int m1 = 0; m1 < N1; ++m1) {
+        T si = T(0), sx = T(0);
+#pragma unroll
+        for (int m0 = 0; m0 < N1; ++m0) {
+          si += tin[m0 + N1 * m1] * tb.Lq[m0][q0];
+          sx += tex[m0 + N1 * m1] * tb.Lq[m0][q0];
+        }
+        Pi[q0][m1] = si;
+        Pe[q0][m1] = sx;
+      }
+    T G[N1][NQ];
+#pragma unroll
+    for (int q1 = 0; q1 < NQ; ++q1) {
+#pragma unroll
+      for (int m0 = 0; m0 < N1; ++m0) G[m0][q1] = T(0);
+#pragma unroll
+      for (int q0 = 0; q0 < NQ; ++q0) {
+        T pin = T(0), pex = T(0);
+#pragma unroll
+        for (int m1 = 0; m1 < N1; ++m1) {
+          pin += Pi[q0][m1] * tb.Lq[m1][q1];
+          pex += Pe[q0][m1] * tb.Lq[m1][q1];
+        }
+        const T uw = vel_e(q0, q1);
+        const T vn = S ? uw : -uw;
+        const T up = vn > T(0) ? pin : pex;
+        const T F = vn * up;
+#pragma unroll
+        for (int m0 = 0; m0 < N1; ++m0) G[m0][q1] += F * tb.Lq[m0][q0];
+      }
+    }
+#pragma unroll
+    for (int m1 = 0; m1 < N1; ++m1)
+#pragma unroll
+      for (int m0 = 0; m0 < N1; ++m0) {
+        T s2 = T(0);
+#pragma unroll
+        for (int q1 = 0; q1 < NQ; ++q1) s2 += G[m0][q1] * tb.Lq[m1][q1];
+        Fm[m0 + N1 * m1] = s2;
+      }
+  }
+}
+
+// R[.. a along E ..] += coef * L_side[a] * Fm
+template <int DIM, int P, int E, typename T>
+__device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T coef) {
+  constexpr int N1 = P + 1, NF = ipow(N1, DIM - 1);
+  constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  constexpr int st[3] = {1, N1, N1 * N1};
+#pragma unroll
+  for (int mf = 0; mf < NF; ++mf) {
+    const int m0 = mf % N1, m1 = mf / N1;
+    const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
+    const T f = coef * Fm[mf];
+#pragma unroll
+    for (int a = 0; a < N1; ++a) R[base + a * st[E]] += Ls[a] * f;
+  }
+}
+
+// SEP1: every velocity component is a single separable term and term k is
+// component k (the host reorders; the fields of the benchmark
+// configurations are of this form); otherwise a runtime sum over terms.
+template <int DIM, int P, bool SEP1, typename T>
+__global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
+  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* box = reinterpret_cast<T*>(smem_raw);
   const MeshArgs& m = a.m;
   const int nboxc = box_cells(m, DIM);
+  const int tx = m.tile[0], ty = m.tile[1], tz = m.tile[2];
+  const int nt = tx * ty * tz;
+  const int nterm = a.v.n_terms;
+  const int span = tx + ty + (DIM > 2 ? tz : 0);
   T* vt = box + (size_t)nboxc * NM;
+  T* fl = vt + (size_t)max(nterm, 1) * span * NPT;   // [DIM][NF][nt]
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM);
-  const int tx = m.tile[0], ty = m.tile[1], tz = m.tile[2];
-  const int nterm = a.v.n_terms;
 
-  // ---- stage velocity-table rows of this tile: vt[(k*3+axis)*span + i]*NPT
+  // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
   {
-    const int span = tx + ty + (DIM > 2 ? tz : 0);
     const int total = nterm * span * NPT;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int j = e % NPT;
-      int r = e / NPT;
+      const int r = e / NPT;
       const int li = r % span;
       const int k = r / span;
       int axis, gi;
@@ -96,61 +216,99 @@ __global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
     }
   }
   load_box<DIM, NM>(m, a.phi_s, box, tc.ox, tc.oy, tc.oz, true);
+  cp_async_wait_all();
   __syncthreads();
 
   const T ct = a.clk ? T(a.clk->ct[a.stage]) : T(a.ct_explicit);
   const T dt = a.clk ? T(a.clk->dt) : T(a.dt_explicit);
   const bool active = a.clk ? (a.clk->active != 0) : true;
+  const int cl = tc.lx + tx * (tc.ly + ty * tc.lz);
+  const int me = box_index(m, DIM, tc.lx, tc.ly, tc.lz);
+  const T ih[3] = {T(1.0 / m.h[0]), T(1.0 / m.h[1]), T(DIM > 2 ? 1.0 / m.h[2] : 1.0)};
+  const int g[3] = {tc.gx, tc.gy, tc.gz};
+  const int l[3] = {tc.lx, tc.ly, tc.lz};
+  const int tl[3] = {tx, ty, tz};
 
   T R[NM];
   T c[NM];
 #pragma unroll
   for (int q = 0; q < NM; ++q) R[q] = T(0);
-  const int span = tx + ty + (DIM > 2 ? tz : 0);
-  const int me = box_index(m, DIM, tc.lx, tc.ly, tc.lz);
-  const T ih0 = T(1.0 / m.h[0]), ih1 = T(1.0 / m.h[1]), ih2 = T(DIM > 2 ? 1.0 / m.h[2] : 1.0);
-
   if (tc.valid) {
 #pragma unroll
     for (int q = 0; q < NM; ++q) c[q] = box[(size_t)me * NM + q];
   }
-  if (tc.valid && active) {
-    auto vrow = [&](int k, int axis) -> const T* {
-      const int li = axis == 0 ? tc.lx : (axis == 1 ? tx + tc.ly : tx + ty + tc.lz);
-      return vt + (size_t)(k * span + li) * NPT;
-    };
+  const bool work = tc.valid && active;
 
+  auto vrow = [&](int k, int axis) -> const T* {
+    const int li = axis == 0 ? tc.lx : (axis == 1 ? tx + tc.ly : tx + ty + tc.lz);
+    return vt + (size_t)(k * span + li) * NPT;
+  };
+  // velocity component `comp` (times the time factor) at table columns
+  auto vel = [&](int comp, int jx, int jy, int jz) -> T {
+    T u = T(0);
+    if constexpr (SEP1) {
+      u = vrow(comp, 0)[jx] * vrow(comp, 1)[jy];
+      if constexpr (DIM == 3) u = u * vrow(comp, 2)[jz];
+    } else {
+      for (int k = 0; k < nterm; ++k) {
+        if (a.v.comp[k] != comp) continue;
+        T v = vrow(k, 0)[jx] * vrow(k, 1)[jy];
+        if constexpr (DIM == 3) v = v * vrow(k, 2)[jz];
+        u += v;
+      }
+    }
+    return u * ct;
+  };
+
+  // SEP1: x-factors of the cell with the x weights folded in
+  T Xw[DIM][NQ];
+  if constexpr (SEP1) {
+    if (work) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const T* xr = vrow(d, 0);
+#pragma unroll
+        for (int qx = 0; qx < NQ; ++qx) Xw[d][qx] = xr[qx] * tb.wq[qx];
+      }
+    }
+  }
+
+  if (work) {
     // ============================ cell term ============================
     if constexpr (DIM == 2) {
-      T Pp[N1][NQ];  // Pp[a][qy] = sum_b c[a,b] L_b(y_qy)
+#pragma unroll 1
+      for (int qy = 0; qy < NQ; ++qy) {
+        T Py[N1];
 #pragma unroll
-      for (int aa = 0; aa < N1; ++aa)
-#pragma unroll
-        for (int qy = 0; qy < NQ; ++qy) {
+        for (int aa = 0; aa < N1; ++aa) {
           T s = T(0);
 #pragma unroll
           for (int b = 0; b < N1; ++b) s += c[aa + N1 * b] * tb.Lq[b][qy];
-          Pp[aa][qy] = s;
+          Py[aa] = s;
         }
-#pragma unroll
-      for (int qy = 0; qy < NQ; ++qy) {
         T X1[N1], X2[N1];
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa) { X1[aa] = T(0); X2[aa] = T(0); }
+        T Yc[2];
+        if constexpr (SEP1) {
+#pragma unroll
+          for (int d = 0; d < 2; ++d) Yc[d] = vrow(d, 1)[qy] * tb.wq[qy] * ct * ih[d];
+        }
 #pragma unroll
         for (int qx = 0; qx < NQ; ++qx) {
           T phi = T(0);
 #pragma unroll
-          for (int aa = 0; aa < N1; ++aa) phi += Pp[aa][qy] * tb.Lq[aa][qx];
-          T u0 = T(0), u1 = T(0);
-          for (int k = 0; k < nterm; ++k) {
-            const T tv = term_val<2>(vrow(k, 0), vrow(k, 1), (const T*)nullptr, qx, qy, 0);
-            if (a.v.comp[k] == 0) u0 += tv; else u1 += tv;
+          for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
+          T fx, fy;
+          if constexpr (SEP1) {
+            fx = phi * Xw[0][qx] * Yc[0];
+            fy = phi * Xw[1][qx] * Yc[1];
+          } else {
+            const T u0 = vel(0, qx, qy, 0), u1 = vel(1, qx, qy, 0);
+            const T w = tb.wq[qx] * tb.wq[qy] * phi;
+            fx = w * u0 * ih[0];
+            fy = w * u1 * ih[1];
           }
-          u0 *= ct;
-          u1 *= ct;
-          const T w = tb.wq[qx] * tb.wq[qy] * phi;
-          const T fx = w * u0 * ih0, fy = w * u1 * ih1;
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) {
             X1[aa] += fx * tb.Dq[aa][qx];
@@ -164,42 +322,43 @@ __global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
             R[aa + N1 * b] += X1[aa] * tb.Lq[b][qy] + X2[aa] * tb.Dq[b][qy];
       }
     } else {
-      // Q1[a][b][qz] = sum_c c[a,b,c] L_c(z); Pp[a][qy][qz] = sum_b Q1 L_b(y)
-      T Pp[N1][NQ][NQ];
-      {
-        T Q1[N1][N1][NQ];
-#pragma unroll
-        for (int aa = 0; aa < N1; ++aa)
-#pragma unroll
-          for (int b = 0; b < N1; ++b)
-#pragma unroll
-            for (int qz = 0; qz < NQ; ++qz) {
-              T s = T(0);
-#pragma unroll
-              for (int cc = 0; cc < N1; ++cc) s += c[aa + N1 * (b + N1 * cc)] * tb.Lq[cc][qz];
-              Q1[aa][b][qz] = s;
-            }
-#pragma unroll
-        for (int aa = 0; aa < N1; ++aa)
-#pragma unroll
-          for (int qy = 0; qy < NQ; ++qy)
-#pragma unroll
-            for (int qz = 0; qz < NQ; ++qz) {
-              T s = T(0);
-#pragma unroll
-              for (int b = 0; b < N1; ++b) s += Q1[aa][b][qz] * tb.Lq[b][qy];
-              Pp[aa][qy][qz] = s;
-            }
-      }
 #pragma unroll 1
       for (int qz = 0; qz < NQ; ++qz) {
+        T Pz[N1][N1];
+#pragma unroll
+        for (int aa = 0; aa < N1; ++aa)
+#pragma unroll
+          for (int b = 0; b < N1; ++b) {
+            T s = T(0);
+#pragma unroll
+            for (int cc = 0; cc < N1; ++cc) s += c[aa + N1 * (b + N1 * cc)] * tb.Lq[cc][qz];
+            Pz[aa][b] = s;
+          }
         T U1[N1][N1], U3[N1][N1];
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa)
 #pragma unroll
           for (int b = 0; b < N1; ++b) { U1[aa][b] = T(0); U3[aa][b] = T(0); }
+        T Zc[3];
+        if constexpr (SEP1) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) Zc[d] = vrow(d, 2)[qz] * tb.wq[qz] * ct * ih[d];
+        }
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
+          T YZ[3];
+          if constexpr (SEP1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) YZ[d] = vrow(d, 1)[qy] * tb.wq[qy] * Zc[d];
+          }
+          T Py[N1];
+#pragma unroll
+          for (int aa = 0; aa < N1; ++aa) {
+            T s = T(0);
+#pragma unroll
+            for (int b = 0; b < N1; ++b) s += Pz[aa][b] * tb.Lq[b][qy];
+            Py[aa] = s;
+          }
           T X1[N1], X2[N1], X3[N1];
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) { X1[aa] = T(0); X2[aa] = T(0); X3[aa] = T(0); }
@@ -207,18 +366,19 @@ __global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
           for (int qx = 0; qx < NQ; ++qx) {
             T phi = T(0);
 #pragma unroll
-            for (int aa = 0; aa < N1; ++aa) phi += Pp[aa][qy][qz] * tb.Lq[aa][qx];
-            T u0 = T(0), u1 = T(0), u2 = T(0);
-            for (int k = 0; k < nterm; ++k) {
-              const T tv = term_val<3>(vrow(k, 0), vrow(k, 1), vrow(k, 2), qx, qy, qz);
-              const int cp = a.v.comp[k];
-              if (cp == 0) u0 += tv; else if (cp == 1) u1 += tv; else u2 += tv;
+            for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
+            T fx, fy, fz;
+            if constexpr (SEP1) {
+              fx = phi * Xw[0][qx] * YZ[0];
+              fy = phi * Xw[1][qx] * YZ[1];
+              fz = phi * Xw[2][qx] * YZ[2];
+            } else {
+              const T u0 = vel(0, qx, qy, qz), u1 = vel(1, qx, qy, qz), u2 = vel(2, qx, qy, qz);
+              const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
+              fx = w * u0 * ih[0];
+              fy = w * u1 * ih[1];
+              fz = w * u2 * ih[2];
             }
-            u0 *= ct;
-            u1 *= ct;
-            u2 *= ct;
-            const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
-            const T fx = w * u0 * ih0, fy = w * u1 * ih1, fz = w * u2 * ih2;
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) {
               X1[aa] += fx * tb.Dq[aa][qx];
@@ -243,117 +403,97 @@ __global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
               R[aa + N1 * (b + N1 * cc)] += U1[aa][b] * tb.Lq[cc][qz] + U3[aa][b] * tb.Dq[cc][qz];
       }
     }
+  }
 
-    // ============================ faces ============================
-    constexpr int NF = ipow(N1, DIM - 1);   // face modes
-    // fully unrolled: face axis and side are compile-time, so every modal
-    // index below is static and c / R stay in registers
+  // weighted normal velocity on face (E, S): u_E(q) w_q0 w_q1 at the face
+  // Gauss point (q0, q1) (tangential axes in increasing order)
+  auto face_vel = [&](auto EC, auto SC) {
+    constexpr int E = decltype(EC)::value, S = decltype(SC)::value;
+    constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+    if constexpr (SEP1) {
+      const T* rows[3] = {vrow(E, 0), vrow(E, 1), DIM > 2 ? vrow(E, 2) : nullptr};
+      const T fe = rows[E][NQ + S] * ct;
+      T a0[NQ], a1[NQ];
 #pragma unroll
-    for (int f = 0; f < 2 * DIM; ++f) {
-      const int e = f >> 1, s = f & 1;
-      int nl[3] = {tc.lx, tc.ly, tc.lz};
-      int ng[3] = {tc.gx, tc.gy, tc.gz};
-      nl[e] += s ? 1 : -1;
-      ng[e] += s ? 1 : -1;
-      const bool has_nb = ng[e] >= 0 && ng[e] < m.n[e];
-      const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
-      // traces on the face (modes of the tangential axes, t0 < t1)
-      const int t0 = e == 0 ? 1 : 0;
-      const int t1 = e == 2 ? 1 : 2;
-      const int st[3] = {1, N1, N1 * N1};
-      T tin[NF], tex[NF];
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) {
-        const int m0 = mf % N1, m1 = DIM > 2 ? mf / N1 : 0;
-        const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
-        T si = T(0), sx = T(0);
-#pragma unroll
-        for (int aa = 0; aa < N1; ++aa) {
-          const T li = s ? tb.L1[aa] : tb.L0[aa];
-          const T lx = s ? tb.L0[aa] : tb.L1[aa];
-          si += li * c[base + aa * st[e]];
-          if (has_nb) sx += lx * cn[base + aa * st[e]];
-        }
-        tin[mf] = si;
-        tex[mf] = has_nb ? sx : si;
+      for (int q = 0; q < NQ; ++q) {
+        a0[q] = rows[t0][q] * tb.wq[q];
+        a1[q] = DIM > 2 ? rows[t1][q] * tb.wq[q] : T(1);
       }
-      // flux at face points, projected back onto the face modes
-      T Fm[NF];
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) Fm[mf] = T(0);
-      const T ihe = e == 0 ? ih0 : (e == 1 ? ih1 : ih2);
-      constexpr int NQF = ipow(NQ, DIM - 1);
-#pragma unroll
-      for (int qf = 0; qf < NQF; ++qf) {
-        const int q0 = qf % NQ, q1 = DIM > 2 ? qf / NQ : 0;
-        T pin = T(0), pex = T(0);
-#pragma unroll
-        for (int mf = 0; mf < NF; ++mf) {
-          const int m0 = mf % N1, m1 = DIM > 2 ? mf / N1 : 0;
-          T bw = tb.Lq[m0][q0];
-          if constexpr (DIM > 2) bw = bw * tb.Lq[m1][q1];
-          pin += tin[mf] * bw;
-          pex += tex[mf] * bw;
-        }
-        // normal velocity at the face point
-        int j[3];
-        j[e] = NQ + s;
+      return [=](int q0, int q1) -> T {
+        // ((f_x f_y) f_z) in axis order, weights folded in
+        if constexpr (DIM == 2) return (E == 0 ? fe * a0[q0] : a0[q0] * fe);
+        else if constexpr (E == 0) return (fe * a0[q0]) * a1[q1];
+        else if constexpr (E == 1) return (a0[q0] * fe) * a1[q1];
+        else return (a0[q0] * a1[q1]) * fe;
+      };
+    } else {
+      return [&, E, S](int q0, int q1) -> T {
+        int j[3] = {0, 0, 0};
+        j[E] = NQ + S;
         j[t0] = q0;
-        if constexpr (DIM > 2) j[t1] = q1;
-        T ue = T(0);
-        for (int k = 0; k < nterm; ++k) {
-          if (a.v.comp[k] != e) continue;
-          ue += term_val<DIM>(vrow(k, 0), vrow(k, 1), DIM > 2 ? vrow(k, 2) : nullptr, j[0], j[1],
-                              DIM > 2 ? j[2] : 0);
-        }
-        ue *= ct;
-        const T vn = s ? ue : -ue;
-        const T up = vn > T(0) ? pin : pex;
+        if (DIM > 2) j[t1] = q1;
         T w = tb.wq[q0];
         if constexpr (DIM > 2) w = w * tb.wq[q1];
-        const T F = vn * up * w * ihe;
-#pragma unroll
-        for (int mf = 0; mf < NF; ++mf) {
-          const int m0 = mf % N1, m1 = DIM > 2 ? mf / N1 : 0;
-          T bw = tb.Lq[m0][q0];
-          if constexpr (DIM > 2) bw = bw * tb.Lq[m1][q1];
-          Fm[mf] += F * bw;
-        }
-      }
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) {
-        const int m0 = mf % N1, m1 = DIM > 2 ? mf / N1 : 0;
-        const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
-#pragma unroll
-        for (int aa = 0; aa < N1; ++aa) {
-          const T li = s ? tb.L1[aa] : tb.L0[aa];
-          R[base + aa * st[e]] -= li * Fm[mf];
-        }
-      }
+        return vel(E, j[0], j[1], j[2]) * w;
+      };
     }
-  }
+  };
+
+  // ============ upper faces: computed once, shared with the upper neighbour
+  auto do_upper = [&](auto EC) {
+    constexpr int E = decltype(EC)::value;
+    if (!work) return;
+    int nl[3] = {l[0], l[1], l[2]};
+    nl[E] += 1;
+    const bool has_nb = g[E] + 1 < m.n[E];
+    const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
+    T Fm[NF];
+    face_flux<DIM, P, E, 1, T>(tb, c, cn, has_nb, face_vel(std::integral_constant<int, E>(),
+                                                          std::integral_constant<int, 1>()), Fm);
+    scatter_face<DIM, P, E, T>(R, tb.L1, Fm, -ih[E]);
+    if (has_nb && l[E] + 1 < tl[E]) {
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) fl[(size_t)(E * NF + mf) * nt + cl] = Fm[mf];
+    }
+  };
+  do_upper(std::integral_constant<int, 0>());
+  do_upper(std::integral_constant<int, 1>());
+  if constexpr (DIM == 3) do_upper(std::integral_constant<int, 2>());
+  __syncthreads();
+  // ============ lower faces: shared flux of the lower neighbour, or own
+  auto do_lower = [&](auto EC) {
+    constexpr int E = decltype(EC)::value;
+    if (!work) return;
+    T Fm[NF];
+    const int stride = E == 0 ? 1 : (E == 1 ? tx : tx * ty);
+    if (l[E] > 0 && g[E] > 0) {
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) Fm[mf] = fl[(size_t)(E * NF + mf) * nt + cl - stride];
+      scatter_face<DIM, P, E, T>(R, tb.L0, Fm, ih[E]);
+    } else {
+      int nl[3] = {l[0], l[1], l[2]};
+      nl[E] -= 1;
+      const bool has_nb = g[E] > 0;
+      const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
+      face_flux<DIM, P, E, 0, T>(tb, c, cn, has_nb, face_vel(std::integral_constant<int, E>(),
+                                                            std::integral_constant<int, 0>()), Fm);
+      scatter_face<DIM, P, E, T>(R, tb.L0, Fm, -ih[E]);
+    }
+  };
+  do_lower(std::integral_constant<int, 0>());
+  do_lower(std::integral_constant<int, 1>());
+  if constexpr (DIM == 3) do_lower(std::integral_constant<int, 2>());
 
   // ---- combine with phi^n and store through shared memory (coalesced)
   __syncthreads();
-  const int ntile_cells = tx * ty * tz;
   T* stage_buf = box;  // reuse: [tile cell][NM]
   const bool need_n = a.combine == kRK2b || a.combine == kRK3b || a.combine == kRK3c;
   if (need_n) {
-    const int total = ntile_cells * NM;
-    for (int e2 = threadIdx.x; e2 < total; e2 += blockDim.x) {
-      const int q = e2 % NM, cl = e2 / NM;
-      const int lx = cl % tx, ly = (cl / tx) % ty, lz = cl / (tx * ty);
-      const int gx = tc.ox + lx, gy = tc.oy + ly, gz = tc.oz + lz;
-      T v = T(0);
-      const int gi = m.q2g[q];
-      if (gx < m.n[0] && gy < m.n[1] && gz < m.n[2] && gi >= 0)
-        v = a.phi_n[((long long)gx + (long long)m.n[0] * (gy + (long long)m.n[1] * gz)) * m.nb + gi];
-      stage_buf[e2] = v;
-    }
+    load_tile<DIM, NM>(m, a.phi_n, stage_buf, tc.ox, tc.oy, tc.oz, false, NM);
+    cp_async_wait_all();
     __syncthreads();
   }
   if (tc.valid) {
-    const int cl = tc.lx + tx * (tc.ly + ty * tc.lz);
 #pragma unroll
     for (int q = 0; q < NM; ++q) {
       // an inactive (zero-length) substep passes the stage input through
@@ -366,18 +506,7 @@ __global__ void __launch_bounds__(256) adv_stage_kernel(const AdvArgs<T> a) {
     }
   }
   __syncthreads();
-  {
-    const int total = ntile_cells * m.nb;
-    for (int e2 = threadIdx.x; e2 < total; e2 += blockDim.x) {
-      const int k = e2 % m.nb, cl = e2 / m.nb;
-      const int lx = cl % tx, ly = (cl / tx) % ty, lz = cl / (tx * ty);
-      const int gx = tc.ox + lx, gy = tc.oy + ly, gz = tc.oz + lz;
-      if (gx >= m.n[0] || gy >= m.n[1] || gz >= m.n[2]) continue;
-      const int q = m.g2q[k];
-      a.out[((long long)gx + (long long)m.n[0] * (gy + (long long)m.n[1] * gz)) * m.nb + k] =
-          stage_buf[(size_t)cl * NM + q];
-    }
-  }
+  store_tile<DIM, NM>(m, stage_buf, a.out, tc.ox, tc.oy, tc.oz);
 }
 
 }  // namespace flsp

@@ -139,18 +139,22 @@ struct flsp_handle {
     c.dim = dim;
     c.p = p;
     c.prec = prec;
+    c.basis = basis;
     c.m = m;
     c.stream = stream;
     return c;
   }
+  flsp_velocity_desc vel_dev;   // terms as laid out in the device tables
   VelDev veldev() const {
     VelDev v;
     std::memset(&v, 0, sizeof(v));
     v.vtab = vtab;
-    v.n_terms = vel.n_terms;
+    v.n_terms = vel_dev.n_terms;
     v.nmax = nmax;
     v.npt = npt;
-    for (int k = 0; k < vel.n_terms; ++k) v.comp[k] = vel.terms[k].comp;
+    for (int k = 0; k < vel_dev.n_terms; ++k) v.comp[k] = vel_dev.terms[k].comp;
+    v.sep1 = vel_dev.n_terms == dim;
+    for (int k = 0; k < vel_dev.n_terms; ++k) v.sep1 = v.sep1 && vel_dev.terms[k].comp == k;
     return v;
   }
 };
@@ -182,8 +186,8 @@ int sync_clock(flsp_handle* h) {
 // done outside any stream capture
 int prepare_kernels(flsp_handle* h) {
   Ctx c = h->ctx();
-  ST(adv_default_tile(c, h->vel.n_terms, h->adv_tile));
-  ST(adv_prepare(c, h->vel.n_terms, h->adv_tile));
+  ST(adv_default_tile(c, h->vel_dev.n_terms, h->adv_tile));
+  ST(adv_prepare(c, h->vel_dev.n_terms, h->adv_tile));
   ST(hj_default_tile(c, h->hj_tile));
   ST(hj_prepare(c, h->hj_tile));
   if (h->dim == 2) ST(weno_prepare(c));
@@ -338,18 +342,43 @@ int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
   return FLSP_OK;
 }
 
+// Lay the velocity terms out for the device: when every component has at
+// most one term, term k becomes component k (a zero term stands in for a
+// missing component), which selects the stage kernel's fast path.
+void layout_velocity(flsp_handle* h) {
+  const flsp_velocity_desc& v = h->vel;
+  int count[3] = {0, 0, 0};
+  for (int k = 0; k < v.n_terms; ++k) count[v.terms[k].comp]++;
+  bool sep = true;
+  for (int d = 0; d < h->dim; ++d) sep = sep && count[d] <= 1;
+  h->vel_dev = v;
+  if (!sep) return;
+  flsp_velocity_desc r = v;
+  r.n_terms = h->dim;
+  for (int d = 0; d < h->dim; ++d) {
+    flsp_vel_term zero;
+    std::memset(&zero, 0, sizeof(zero));
+    zero.comp = d;
+    zero.coeff = 0.0;
+    r.terms[d] = zero;
+  }
+  for (int k = 0; k < v.n_terms; ++k) r.terms[v.terms[k].comp] = v.terms[k];
+  h->vel_dev = r;
+}
+
 int build_vtab(flsp_handle* h) {
   const int dim = h->dim;
+  layout_velocity(h);
   const int nq = h->p + 2;
   h->npt = nq + 2;
   h->nmax = std::max(h->m.n[0], std::max(h->m.n[1], h->m.n[2]));
-  const int nt = std::max(h->vel.n_terms, 1);
+  const int nt = std::max(h->vel_dev.n_terms, 1);
   const size_t n = (size_t)nt * 3 * h->nmax * h->npt;
   std::vector<double> tabd(n, 0.0);
   double x[8], w[8];
   gauss_rule(nq, x, w);
-  for (int k = 0; k < h->vel.n_terms; ++k) {
-    const flsp_vel_term& tm = h->vel.terms[k];
+  for (int k = 0; k < h->vel_dev.n_terms; ++k) {
+    const flsp_vel_term& tm = h->vel_dev.terms[k];
     for (int ax = 0; ax < 3; ++ax)
       for (int i = 0; i < h->nmax; ++i)
         for (int j = 0; j < h->npt; ++j) {
@@ -381,9 +410,9 @@ int build_vtab(flsp_handle* h) {
   }
   // static CFL part: max over vertices of |u_spatial| / diam
   int comp[kMaxTerms];
-  for (int k = 0; k < h->vel.n_terms; ++k) comp[k] = h->vel.terms[k].comp;
+  for (int k = 0; k < h->vel_dev.n_terms; ++k) comp[k] = h->vel_dev.terms[k].comp;
   CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
-  ST(launch_static_cfl(h->ctx(), h->vtab64, h->vel.n_terms, comp, h->nmax, h->npt, h->clk));
+  ST(launch_static_cfl(h->ctx(), h->vtab64, h->vel_dev.n_terms, comp, h->nmax, h->npt, h->clk));
   CU(cudaStreamSynchronize(h->stream));
   return FLSP_OK;
 }
@@ -517,6 +546,7 @@ int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts, flsp_handl
     cudaMemcpy(h->perm, mesh->host_cell_order, sizeof(int64_t) * ncell, cudaMemcpyHostToDevice);
   }
   std::memset(&h->vel, 0, sizeof(h->vel));
+  std::memset(&h->vel_dev, 0, sizeof(h->vel_dev));
   {
     int st = prepare_kernels(h);
     if (st) return cleanup_fail(st);

@@ -35,6 +35,10 @@ struct Tab1D {
   T xl[kMaxN1], wl[kMaxN1];             // Gauss (p+1) points/weights
   T Ll[kMaxN1][kMaxN1];                 // L_a(xl)
   T Dl[kMaxN1][kMaxN1];                 // L_a'(xl)
+  // LDG lifting kernels K_s(x) = sum_a L_a(x) L_a(s), s = 0, 1, at the
+  // Gauss (p+2) points and at x = 0, 1
+  T K0q[kMaxNQ], K1q[kMaxNQ];
+  T K0v[2], K1v[2];
 };
 
 // Every translation unit of the library holds its own copy of the tables
@@ -168,6 +172,12 @@ struct VelArgs {
   int comp[kMaxTerms];
 };
 
+// next 16-byte aligned address at or after p (shared-memory sub-buffers)
+template <typename U>
+__device__ __forceinline__ U* align16(void* p) {
+  return reinterpret_cast<U*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+}
+
 // local (tile) coordinates of the thread's cell
 struct TileCoord {
   int lx, ly, lz;     // in [0, tile)
@@ -209,40 +219,124 @@ __device__ __forceinline__ int box_cells(const MeshArgs& m, int dim) {
   return (m.tile[0] + 2) * (dim > 1 ? m.tile[1] + 2 : 1) * (dim > 2 ? m.tile[2] + 2 : 1);
 }
 
-// Cooperative load of the tile and its face halo (no edges/corners) from a
-// cell-major vector into the smem box, expanded to the Q layout.  Rows of
-// cells along x are contiguous in HBM, so consecutive threads read
-// consecutive addresses.  Slots of cells outside the domain are not
-// written (boundary faces never read them).
+// ---------------------------------------------------------------------
+// asynchronous global -> shared copies (cp.async, one element each): a
+// thread issues all of its copies before waiting, so the latency of every
+// row of a tile overlaps instead of serialising row by row
+// ---------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Load of the tile and its face halo (no edges/corners) from a cell-major
+// vector into the smem box, expanded to the Q layout.  One warp per row of
+// cells along x (contiguous in HBM), lanes over the row's elements.  Slots
+// of cells outside the domain are not written (boundary faces never read
+// them).  Completes with cp_async_wait_all() + __syncthreads() by the caller.
 template <int DIM, int NM, typename T>
 __device__ __forceinline__ void load_box(const MeshArgs& m, const T* __restrict__ g,
                                          T* __restrict__ sm, int ox, int oy, int oz,
                                          bool with_halo) {
   const int tx = m.tile[0], ty = DIM > 1 ? m.tile[1] : 1, tz = DIM > 2 ? m.tile[2] : 1;
   const int h = with_halo ? 1 : 0;
-  // rows: (ly, lz) in [-h, ty+h) x [-h, tz+h), excluding corners
   const int nry = ty + 2 * (DIM > 1 ? h : 0), nrz = tz + 2 * (DIM > 2 ? h : 0);
   const int ly0 = DIM > 1 ? -h : 0, lz0 = DIM > 2 ? -h : 0;
-  for (int r = 0; r < nry * nrz; ++r) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const bool dense = m.nb == NM;   // Q basis: smem row == HBM row
+  for (int r = warp; r < nry * nrz; r += nw) {
     const int ly = ly0 + r % nry, lz = lz0 + r / nry;
     const bool yout = ly < 0 || ly >= ty, zout = lz < 0 || lz >= tz;
     if (yout && zout) continue;
     const int gy = oy + ly, gz = oz + lz;
     if (gy < 0 || gy >= m.n[1] || gz < 0 || gz >= m.n[2]) continue;
-    // interior rows get the x halo too; halo rows only the tile span
     const int lx0 = (!yout && !zout) ? -h : 0;
     const int lx1 = (!yout && !zout) ? tx + h : tx;
     const int gx0 = max(ox + lx0, 0), gx1 = min(ox + lx1, m.n[0]);
     if (gx1 <= gx0) continue;
     const long long rowcell = (long long)m.n[0] * (gy + (long long)m.n[1] * gz);
+    T* dst = sm + (size_t)box_index(m, DIM, gx0 - ox, ly, lz) * NM;
     const int count = (gx1 - gx0) * NM;
-    for (int e = threadIdx.x; e < count; e += blockDim.x) {
+    if (dense) {
+      const T* src = g + (rowcell + gx0) * NM;
+      for (int e = lane; e < count; e += 32) cp_async_elem(dst + e, src + e);
+    } else {
+      const T* src = g + (rowcell + gx0) * m.nb;
+      for (int e = lane; e < count; e += 32) {
+        const int cx = e / NM, q = e - cx * NM;
+        const int gi = m.q2g[q];
+        if (gi >= 0) cp_async_elem(dst + e, src + (long long)cx * m.nb + gi);
+        else dst[e] = T(0);
+      }
+    }
+  }
+}
+
+// Load of the tile's own cells (no halo) into [cell][NM] (stride = NM) or,
+// with transposed = true, into [NM][ld] (column = tile cell index).
+template <int DIM, int NM, typename T>
+__device__ __forceinline__ void load_tile(const MeshArgs& m, const T* __restrict__ g,
+                                          T* __restrict__ sm, int ox, int oy, int oz,
+                                          bool transposed, int ld) {
+  const int tx = m.tile[0], ty = DIM > 1 ? m.tile[1] : 1, tz = DIM > 2 ? m.tile[2] : 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < ty * tz; r += nw) {
+    const int ly = r % ty, lz = r / ty;
+    const int gy = oy + ly, gz = oz + lz;
+    const int nx = min(tx, m.n[0] - ox);
+    const int cl0 = tx * r;
+    const int count = nx * NM;
+    if (gy >= m.n[1] || gz >= m.n[2] || nx <= 0) {
+      for (int e = lane; e < tx * NM; e += 32) {
+        const int cx = e / NM, q = e - cx * NM;
+        if (transposed) sm[(size_t)q * ld + cl0 + cx] = T(0);
+        else sm[(size_t)(cl0 + cx) * NM + q] = T(0);
+      }
+      continue;
+    }
+    const T* src = g + ((long long)m.n[0] * (gy + (long long)m.n[1] * gz) + ox) * m.nb;
+    for (int e = lane; e < count; e += 32) {
       const int cx = e / NM, q = e - cx * NM;
-      const int gx = gx0 + cx;
       const int gi = m.q2g[q];
-      T v = T(0);
-      if (gi >= 0) v = g[(rowcell + gx) * m.nb + gi];
-      sm[box_index(m, DIM, gx - ox, ly, lz) * NM + q] = v;
+      T* d = transposed ? sm + (size_t)q * ld + cl0 + cx : sm + (size_t)(cl0 + cx) * NM + q;
+      if (gi >= 0) cp_async_elem(d, src + (long long)cx * m.nb + gi);
+      else *d = T(0);
+    }
+    for (int e = count + lane; e < tx * NM; e += 32) {   // cells past the domain edge
+      const int cx = e / NM, q = e - cx * NM;
+      if (transposed) sm[(size_t)q * ld + cl0 + cx] = T(0);
+      else sm[(size_t)(cl0 + cx) * NM + q] = T(0);
+    }
+  }
+}
+
+// Store of the tile's own cells from [cell][NM] smem to HBM (nb DoFs per
+// cell, g2q maps them to the Q slots), one warp per row.
+template <int DIM, int NM, typename T>
+__device__ __forceinline__ void store_tile(const MeshArgs& m, const T* __restrict__ sm,
+                                           T* __restrict__ g, int ox, int oy, int oz) {
+  const int tx = m.tile[0], ty = DIM > 1 ? m.tile[1] : 1, tz = DIM > 2 ? m.tile[2] : 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const bool dense = m.nb == NM;
+  for (int r = warp; r < ty * tz; r += nw) {
+    const int ly = r % ty, lz = r / ty;
+    const int gy = oy + ly, gz = oz + lz;
+    const int nx = min(tx, m.n[0] - ox);
+    if (gy >= m.n[1] || gz >= m.n[2] || nx <= 0) continue;
+    T* dst = g + ((long long)m.n[0] * (gy + (long long)m.n[1] * gz) + ox) * m.nb;
+    const T* src = sm + (size_t)tx * r * NM;
+    if (dense) {
+      for (int e = lane; e < nx * NM; e += 32) dst[e] = src[e];
+    } else {
+      for (int e = lane; e < nx * m.nb; e += 32) {
+        const int cx = e / m.nb, k = e - cx * m.nb;
+        dst[e] = src[(size_t)cx * NM + m.g2q[k]];
+      }
     }
   }
 }

@@ -44,7 +44,7 @@ __host__ __device__ inline size_t hj_smem_bytes(const int* tile) {
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
   size_t own0 = (size_t)nt * NM * sizeof(T);
   size_t acc = (size_t)nt * 2 * NQV * sizeof(T);
-  return box + own0 + acc + 64 * sizeof(double);
+  return box + own0 + acc + 64 * sizeof(double) + 16;
 }
 
 // RK combinations of ReinitSimulatorLDG::advance_time with the reference's
@@ -72,24 +72,13 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
   const int nt = tx * ty * tz;
   T* own0 = box + (size_t)nboxc * NM;
   T* acc = own0 + (size_t)nt * NM;
-  double* red = reinterpret_cast<double*>(acc + (size_t)nt * 2 * NQV);
+  double* red = align16<double>(acc + (size_t)nt * 2 * NQV);
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM);
 
   load_box<DIM, NM>(m, a.phi, box, tc.ox, tc.oy, tc.oz, true);
-  {  // phi0 of the tile (no halo), compact [cell][NM]
-    const int total = nt * NM;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int q = e % NM, cl = e / NM;
-      const int lx = cl % tx, ly = (cl / tx) % ty, lz = cl / (tx * ty);
-      const int gx = tc.ox + lx, gy = tc.oy + ly, gz = tc.oz + lz;
-      T v = T(0);
-      const int gi = m.q2g[q];
-      if (gx < m.n[0] && gy < m.n[1] && gz < m.n[2] && gi >= 0)
-        v = a.phi0[((long long)gx + (long long)m.n[0] * (gy + (long long)m.n[1] * gz)) * m.nb + gi];
-      own0[e] = v;
-    }
-  }
+  load_tile<DIM, NM>(m, a.phi0, own0, tc.ox, tc.oy, tc.oz, false, NM);
+  cp_async_wait_all();
   __syncthreads();
 
   const int cl = tc.lx + tx * (tc.ly + ty * tc.lz);
@@ -327,15 +316,7 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
     for (int q = 0; q < NM; ++q) sb[(size_t)cl * NM + q] = hj_combine<T>(a.rk, c[q], R[q], dt);
   }
   __syncthreads();
-  const int total = nt * m.nb;
-  for (int e2 = threadIdx.x; e2 < total; e2 += blockDim.x) {
-    const int k = e2 % m.nb, c2 = e2 / m.nb;
-    const int lx = c2 % tx, ly = (c2 / tx) % ty, lz = c2 / (tx * ty);
-    const int gx = tc.ox + lx, gy = tc.oy + ly, gz = tc.oz + lz;
-    if (gx >= m.n[0] || gy >= m.n[1] || gz >= m.n[2]) continue;
-    a.out[((long long)gx + (long long)m.n[0] * (gy + (long long)m.n[1] * gz)) * m.nb + k] =
-        sb[(size_t)c2 * NM + m.g2q[k]];
-  }
+  store_tile<DIM, NM>(m, sb, a.out, tc.ox, tc.oy, tc.oz);
 }
 
 }  // namespace flsp

@@ -37,9 +37,12 @@ int adv_prepare(const Ctx& c, int n_terms, const int* tile) {
     using T = decltype(tz);
     const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(n_terms, 1));
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "advection tile too large for shared memory");
-    cudaError_t e = cudaFuncSetAttribute(adv_stage_kernel<DIM, P, T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("adv attr: ") + cudaGetErrorString(e));
+    for (auto kern : {adv_stage_kernel<DIM, P, true, T>, adv_stage_kernel<DIM, P, false, T>}) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("adv attr: ") + cudaGetErrorString(e));
+    }
     return FLSP_OK;
   });
 }
@@ -70,7 +73,10 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     a.combine = combine;
     a.ct_explicit = ct_explicit;
     const size_t smem = adv_smem_bytes<DIM, P, T>(a.m.tile, std::max(v.n_terms, 1));
-    adv_stage_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
+    if (v.sep1)
+      adv_stage_kernel<DIM, P, true, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
+    else
+      adv_stage_kernel<DIM, P, false, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
     return launch_status("adv_stage_kernel");
   });
 }

@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "flsp_hj.cuh"
+#include "flsp_hjq.cuh"
 #include "flsp_launch.h"
 #include "flsp_tables.h"
 
@@ -20,10 +21,16 @@ int hj_default_tile(const Ctx& c, int* tile) {
     using T = decltype(tz);
     static const int c2[][3] = {{16, 16, 1}, {16, 8, 1}, {8, 8, 1}, {8, 4, 1}};
     static const int c3[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}};
-    const int(*cand)[3] = DIM == 2 ? c2 : c3;
+    // the tensor-product kernel runs 128-thread CTAs
+    static const int q2[][3] = {{16, 8, 1}, {8, 8, 1}, {8, 4, 1}, {4, 4, 1}};
+    static const int q3[][3] = {{8, 4, 4}, {4, 4, 4}, {4, 4, 2}, {4, 2, 2}};
+    const bool tq = c.basis == FLSP_BASIS_Q;
+    const int(*cand)[3] = DIM == 2 ? (tq ? q2 : c2) : (tq ? q3 : c3);
     int i = 0;
-    for (; i < 3; ++i)
-      if (hj_smem_bytes<DIM, P, T>(cand[i]) <= 200 * 1024) break;
+    for (; i < 3; ++i) {
+      const size_t b = tq ? hjq_smem_bytes<DIM, P, T>(cand[i]) : hj_smem_bytes<DIM, P, T>(cand[i]);
+      if (b <= 200 * 1024) break;
+    }
     tile[0] = cand[i][0];
     tile[1] = cand[i][1];
     tile[2] = cand[i][2];
@@ -35,10 +42,14 @@ int hj_prepare(const Ctx& c, const int* tile) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
-    const size_t smem = hj_smem_bytes<DIM, P, T>(tile);
+    const bool tq = c.basis == FLSP_BASIS_Q;
+    const size_t smem = tq ? hjq_smem_bytes<DIM, P, T>(tile) : hj_smem_bytes<DIM, P, T>(tile);
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "reinit tile too large for shared memory");
-    cudaError_t e = cudaFuncSetAttribute(hj_kernel<DIM, P, T>,
+    cudaError_t e = cudaFuncSetAttribute(tq ? hjq_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(tq ? hjq_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("hj attr: ") + cudaGetErrorString(e));
     return FLSP_OK;
   });
@@ -64,6 +75,28 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
     a.rk = rk;
     a.dt_explicit = dt_explicit;
     a.block = block;
+    // the gradient export mode uses the modal kernel for both bases
+    if (c.basis == FLSP_BASIS_Q && mode != kHJGradients) {
+      const size_t smem = hjq_smem_bytes<DIM, P, T>(a.m.tile);
+      hjq_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
+      return launch_status("hjq_kernel");
+    }
+    int tm[3];
+    if (c.basis == FLSP_BASIS_Q) {  // modal kernel with its own tile
+      Ctx cp = c;
+      cp.basis = FLSP_BASIS_P;
+      hj_default_tile(cp, tm);
+      set_tile(a.m, DIM, tm);
+      const size_t sm2 = hj_smem_bytes<DIM, P, T>(a.m.tile);
+      static bool attr_done[2][4][4] = {};
+      bool& done = attr_done[sizeof(T) == 8][DIM][P];
+      if (!done) {
+        cudaFuncSetAttribute(hj_kernel<DIM, P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
+        done = true;
+      }
+      hj_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), tm[0] * tm[1] * tm[2], sm2, c.stream>>>(a);
+      return launch_status("hj_kernel");
+    }
     const size_t smem = hj_smem_bytes<DIM, P, T>(a.m.tile);
     hj_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
     return launch_status("hj_kernel");

@@ -15,7 +15,7 @@ namespace flsp {
 int set_error(int code, const std::string& msg);
 
 struct Ctx {
-  int dim, p, prec;
+  int dim, p, prec, basis;
   MeshArgs m;          // tile fields are filled by the launchers
   cudaStream_t stream;
 };
@@ -66,6 +66,7 @@ struct VelDev {
   const void* vtab;    // T-precision table
   int n_terms, nmax, npt;
   int comp[kMaxTerms];
+  bool sep1;           // term k is the only term of component k
 };
 // tile: cells per CTA (nullptr = default); smem attribute is set on first use
 int adv_default_tile(const Ctx& c, int n_terms, int* tile);

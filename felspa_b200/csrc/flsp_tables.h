@@ -77,6 +77,25 @@ inline void fill_tab(Tab1D<T>& tb, int p) {
       }
       tb.A[a][b] = T((double)s);
     }
+  {
+    double l0[8], l1[8], tmp1[8], tmp2[8];
+    leg_all(n1, 0.0, l0, tmp1, tmp2);
+    leg_all(n1, 1.0, l1, tmp1, tmp2);
+    for (int q = 0; q < nq; ++q) {
+      leg_all(n1, x[q], v, d, dd);
+      double k0 = 0.0, k1 = 0.0;
+      for (int a = 0; a < n1; ++a) { k0 += v[a] * l0[a]; k1 += v[a] * l1[a]; }
+      tb.K0q[q] = T(k0);
+      tb.K1q[q] = T(k1);
+    }
+    for (int e = 0; e < 2; ++e) {
+      const double* le = e ? l1 : l0;
+      double k0 = 0.0, k1 = 0.0;
+      for (int a = 0; a < n1; ++a) { k0 += le[a] * l0[a]; k1 += le[a] * l1[a]; }
+      tb.K0v[e] = T(k0);
+      tb.K1v[e] = T(k1);
+    }
+  }
   gauss_rule(n1, x, w);
   for (int q = 0; q < n1; ++q) {
     tb.xl[q] = T(x[q]);

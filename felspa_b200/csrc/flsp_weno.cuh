@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(256) weno_kernel(const WenoArgs<T> a) {
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, 2);
   load_box<2, NM>(m, a.in, box, tc.ox, tc.oy, 0, true);
+  cp_async_wait_all();
   __syncthreads();
   if (!tc.valid) return;
   const T* c = box + (size_t)box_index(m, 2, tc.lx, tc.ly, 0) * NM;
