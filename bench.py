@@ -255,7 +255,7 @@ def run_ours(args):
 
     # end to end through the C ABI: pinned host state in, period, state out
     host = torch.empty(n_dofs, dtype=torch.float64, pin_memory=True).numpy()
-    host[:] = pb.get_state()
+    pb.get_state(out=host)
     e2e_ms = []
     for _ in range(args.steps):
         flush.zero_()
@@ -265,7 +265,7 @@ def run_ours(args):
         e0.record(stream)
         pb.set_state(host)
         ls.run_steps(REINIT_EVERY, sync=False)
-        host[:] = pb.get_state()
+        pb.get_state(out=host)
         e1.record(stream)
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))

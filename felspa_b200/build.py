@@ -83,7 +83,29 @@ def build(verbose=False, force=False):
         if r.returncode != 0:
             raise RuntimeError(f"nvcc link failed:\n{r.stdout}{r.stderr}")
         os.replace(LIB + ".tmp", LIB)
+    build_examples()
     return LIB
+
+
+EXAMPLES = os.path.join(HERE, "examples")
+
+
+def build_examples():
+    """C++ drivers written against include/flsp_dg.hpp, linked to the library"""
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    for f in sorted(os.listdir(EXAMPLES)):
+        if not f.endswith(".cpp"):
+            continue
+        src = os.path.join(EXAMPLES, f)
+        exe = os.path.join(EXAMPLES, f[:-4] + ".bin")
+        hdrs = [os.path.join(ROOT, "include", h) for h in ("flsp_dg.h", "flsp_dg.hpp")]
+        if not _stale(exe, [src, LIB] + hdrs):
+            continue
+        cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), src, "-o", exe,
+               "-L", HERE, "-lflsp_dg", "-Wl,-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"building {f} failed:\n{r.stdout}{r.stderr}")
 
 
 if __name__ == "__main__":

@@ -130,9 +130,11 @@ struct flsp_handle {
   flsp_ic_desc* ic_dev = nullptr;
   unsigned int* flag_dev = nullptr;
   int n_since_reinit = 0;
+  void* qbuf = nullptr;     // LDG alternating gradient (dim blocks)
+  void* rdiff = nullptr;    // LDG diffusion RHS
   int adv_tile[3] = {0, 0, 0};
   int hj_tile[3] = {0, 0, 0};
-  std::map<long long, GraphEntry> graphs;
+  std::map<unsigned long long, GraphEntry> graphs;
 
   Ctx ctx() const {
     Ctx c;
@@ -190,7 +192,15 @@ int prepare_kernels(flsp_handle* h) {
   ST(adv_prepare(c, h->vel_dev.n_terms, h->adv_tile));
   ST(hj_default_tile(c, h->hj_tile));
   ST(hj_prepare(c, h->hj_tile));
+  ST(ldg_prepare(c));
   if (h->dim == 2) ST(weno_prepare(c));
+  return FLSP_OK;
+}
+
+// LDG viscosity buffers (allocated outside any stream capture)
+int ensure_ldg_buffers(flsp_handle* h) {
+  if (!h->qbuf) CU(cudaMalloc(&h->qbuf, (size_t)h->dim * h->ndofs * h->tsize));
+  if (!h->rdiff) CU(cudaMalloc(&h->rdiff, (size_t)h->ndofs * h->tsize));
   return FLSP_OK;
 }
 
@@ -245,8 +255,14 @@ int enqueue_hj_step(flsp_handle* h, const flsp_reinit_opts* o, int phi0_idx, boo
                            adv_cfl_scaling(h->p)));
   const int src = h->cur;
   const int dst = (src == phi0_idx) ? (phi0_idx + 1) % 3 : other(src, phi0_idx);
+  const void* rdiff = nullptr;
+  if (o->viscosity > 0.0) {   // LDGDiffusionTerm of the current solution (ldg.cc:249-298)
+    ST(launch_ldg(h->ctx(), h->buf[src], h->qbuf, h->ndofs, o->viscosity, 0));
+    ST(launch_ldg(h->ctx(), h->qbuf, h->rdiff, h->ndofs, o->viscosity, 1));
+    rdiff = h->rdiff;
+  }
   ST(launch_hj(h->ctx(), h->buf[src], h->buf[phi0_idx], h->buf[dst], h->clk, kHJStep, o->rk_order, 0.0,
-               h->ndofs, h->hj_tile));
+               h->ndofs, h->hj_tile, rdiff));
   int res = dst;
   if (limiter) {
     const int lim = other(dst, phi0_idx);
@@ -299,7 +315,6 @@ int validate_reinit(const flsp_handle* h, const flsp_reinit_opts* o) {
     return fail(FLSP_ERR_BAD_ARG, "bad n_pseudo_steps");
   if (o->max_iter < 0) return fail(FLSP_ERR_BAD_ARG, "negative max_iter");
   if (o->viscosity < 0.0) return fail(FLSP_ERR_BAD_ARG, "negative viscosity");
-  if (o->viscosity > 0.0) return fail(FLSP_ERR_UNSUPPORTED, "LDG artificial viscosity not built yet");
   if (o->rk_order < 1 || o->rk_order > 3) return fail(FLSP_ERR_BAD_ARG, "reinit rk_order must be 1..3");
   (void)h;
   return FLSP_OK;
@@ -308,6 +323,7 @@ int validate_reinit(const flsp_handle* h, const flsp_reinit_opts* o) {
 // ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637)
 int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
   ST(validate_reinit(h, o));
+  if (o->viscosity > 0.0) ST(ensure_ldg_buffers(h));
   const bool limiter = reinit_limiter(h, o);
   const int phi0 = h->cur;
   ST(launch_hj_clock_reset(h->stream, h->clk));
@@ -563,6 +579,8 @@ void flsp_destroy(flsp_handle* h) {
   clear_graphs(h);
   for (int i = 0; i < 3; ++i) if (h->buf[i]) cudaFree(h->buf[i]);
   if (h->snap) cudaFree(h->snap);
+  if (h->qbuf) cudaFree(h->qbuf);
+  if (h->rdiff) cudaFree(h->rdiff);
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
   if (h->clk) cudaFree(h->clk);
@@ -800,6 +818,7 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
     if (ro.mode != FLSP_REINIT_FIXED)
       return fail(FLSP_ERR_BAD_ARG, "flsp_ls_run_steps needs a fixed-count reinit (FLSP_REINIT_FIXED)");
     ST(validate_reinit(h, &ro));
+    if (ro.viscosity > 0.0) ST(ensure_ldg_buffers(h));
   }
   CU(cudaSetDevice(h->dev));
   ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
@@ -809,8 +828,16 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
     if (to_reinit <= 0) { h->n_since_reinit = 0; continue; }
     if (done + to_reinit <= n_steps && o->execute_reinit) {
       // a full period: replay (or capture) the graph for this buffer role
-      const long long key = ((long long)h->cur << 40) ^ ((long long)to_reinit << 20) ^
-                            ((long long)ro.n_pseudo_steps << 4) ^ (reinit_limiter(h, &ro) ? 1 : 0);
+      // graph key: buffer role, period length and every reinit option
+      // (kernel arguments are baked into the captured graph)
+      unsigned long long key = 1469598103934665603ull;
+      auto mix = [&key](const void* p, size_t n) {
+        const unsigned char* b = (const unsigned char*)p;
+        for (size_t i = 0; i < n; ++i) { key ^= b[i]; key *= 1099511628211ull; }
+      };
+      mix(&h->cur, sizeof(h->cur));
+      mix(&to_reinit, sizeof(to_reinit));
+      mix(&ro, sizeof(ro));
       auto it = h->graphs.find(key);
       if (it == h->graphs.end()) {
         const int cur0 = h->cur;

@@ -34,7 +34,20 @@ struct HJArgs {
   int rk;                       // reinit RK order (all stages see the same L)
   double dt_explicit;           // used when clk == nullptr
   long long block;              // gradient block stride (ncell * nb)
+  const T* __restrict__ rdiff;  // LDG diffusion RHS per unit volume (nu > 0) or null
 };
+
+// add the cell's LDG diffusion RHS (HBM layout) to R (Q layout)
+template <int NM, typename T>
+__device__ __forceinline__ void add_rdiff(const MeshArgs& m, const T* rdiff, long long cell, T* R) {
+  if (!rdiff) return;
+  for (int k = 0; k < m.nb; ++k) {
+    const T v = rdiff[cell * m.nb + k];
+#pragma unroll
+    for (int q = 0; q < NM; ++q)
+      if (q == m.g2q[k]) R[q] += v;
+  }
+}
 
 template <int DIM, int P, typename T>
 __host__ __device__ inline size_t hj_smem_bytes(const int* tile) {
@@ -312,6 +325,7 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
   __syncthreads();
   T* sb = box;
   if (tc.valid) {
+    add_rdiff<NM>(m, a.rdiff, (long long)tc.gx + (long long)m.n[0] * (tc.gy + (long long)m.n[1] * tc.gz), R);
 #pragma unroll
     for (int q = 0; q < NM; ++q) sb[(size_t)cl * NM + q] = hj_combine<T>(a.rk, c[q], R[q], dt);
   }

@@ -444,6 +444,7 @@ __global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
   __syncthreads();
   T* sb = c0s;   // [nt][NM] now
   if (tc.valid) {
+    add_rdiff<NM>(m, a.rdiff, (long long)tc.gx + (long long)m.n[0] * (tc.gy + (long long)m.n[1] * tc.gz), R);
 #pragma unroll
     for (int q = 0; q < NM; ++q) sb[(size_t)cl * NM + q] = hj_combine<T>(a.rk, c[q], R[q], dt);
   }

@@ -4,6 +4,7 @@
 
 #include "flsp_hj.cuh"
 #include "flsp_hjq.cuh"
+#include "flsp_ldg.cuh"
 #include "flsp_launch.h"
 #include "flsp_tables.h"
 
@@ -55,8 +56,42 @@ int hj_prepare(const Ctx& c, const int* tile) {
   });
 }
 
+static const int kLdgTile2[3] = {16, 16, 1};
+static const int kLdgTile3[3] = {8, 8, 4};
+
+int ldg_prepare(const Ctx& c) {
+  return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
+    constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
+    using T = decltype(tz);
+    const size_t smem = ldg_smem_bytes<DIM, P, T>(DIM == 2 ? kLdgTile2 : kLdgTile3);
+    cudaError_t e = cudaFuncSetAttribute(ldg_kernel<DIM, P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("ldg attr: ") + cudaGetErrorString(e));
+    return FLSP_OK;
+  });
+}
+
+int launch_ldg(const Ctx& c, const void* in, void* out, long long block, double nu, int mode) {
+  return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
+    constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
+    using T = decltype(tz);
+    LdgArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.m = c.m;
+    const int* t = DIM == 2 ? kLdgTile2 : kLdgTile3;
+    set_tile(a.m, DIM, t);
+    a.in = reinterpret_cast<const T*>(in);
+    a.out = reinterpret_cast<T*>(out);
+    a.block = block;
+    a.nu = nu;
+    const size_t smem = ldg_smem_bytes<DIM, P, T>(a.m.tile);
+    ldg_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a, mode);
+    return launch_status("ldg_kernel");
+  });
+}
+
 int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClock* clk, int mode,
-              int rk, double dt_explicit, long long block, const int* tile) {
+              int rk, double dt_explicit, long long block, const int* tile, const void* rdiff) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
@@ -75,6 +110,7 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
     a.rk = rk;
     a.dt_explicit = dt_explicit;
     a.block = block;
+    a.rdiff = reinterpret_cast<const T*>(rdiff);
     // the gradient export mode uses the modal kernel for both bases
     if (c.basis == FLSP_BASIS_Q && mode != kHJGradients) {
       const size_t smem = hjq_smem_bytes<DIM, P, T>(a.m.tile);

@@ -79,7 +79,12 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
 int hj_default_tile(const Ctx& c, int* tile);
 int hj_prepare(const Ctx& c, const int* tile);
 int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClock* clk, int mode,
-              int rk, double dt_explicit, long long block, const int* tile);
+              int rk, double dt_explicit, long long block, const int* tile,
+              const void* rdiff = nullptr);
+// LDG artificial viscosity: mode 0 = alternating gradient q (DIM blocks)
+// from phi, mode 1 = diffusion RHS (per unit volume) from q
+int ldg_prepare(const Ctx& c);
+int launch_ldg(const Ctx& c, const void* in, void* out, long long block, double nu, int mode);
 
 // ---------------- misc (flsp_k_misc.cu) ----------------
 int weno_prepare(const Ctx& c);

@@ -132,8 +132,13 @@ class Problem:
         a = np.ascontiguousarray(coeffs, dtype=np.float64)
         check(load().flsp_set_state(self.h, dp(a), a.size))
 
-    def get_state(self):
-        out = np.empty(self.n_dofs)
+    def get_state(self, out=None):
+        """solution coefficients in host DoF order (into `out` when given,
+        e.g. a pinned buffer)"""
+        if out is None:
+            out = np.empty(self.n_dofs)
+        if out.dtype != np.float64 or out.size != self.n_dofs or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of n_dofs")
         check(load().flsp_get_state(self.h, dp(out), out.size))
         return out
 

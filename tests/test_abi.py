@@ -1,0 +1,116 @@
+"""The C ABI: the library loads, exports every entry point include/flsp_dg.h
+declares, the ctypes mirrors match the C struct layouts, and without a GPU
+the library fails loudly instead of falling back to the CPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from felspa_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "flsp_dg.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(flsp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_entry_points_exported(flsp):
+    L = flsp.load()
+    names = declared_functions()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(L, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", flsp.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (flsp_\w+)", out))
+    assert set(names) <= exported
+
+
+def test_prototypes_cover_header(flsp):
+    assert set(declared_functions()) == set(flsp.PROTOTYPES)
+
+
+def test_struct_layouts_match_c():
+    src = """
+#include <stdio.h>
+#include <stddef.h>
+#include "flsp_dg.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(flsp_mesh_desc), sizeof(flsp_dg_opts),
+         sizeof(flsp_factor), sizeof(flsp_vel_term), sizeof(flsp_velocity_desc), sizeof(flsp_ic_node),
+         sizeof(flsp_ic_desc), sizeof(flsp_reinit_opts), sizeof(flsp_ls_opts),
+         offsetof(flsp_ic_desc, waves));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(src)
+        gcc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+        subprocess.run([gcc, "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+    mine = [C.sizeof(abi.MeshDesc), C.sizeof(abi.DGOpts), C.sizeof(abi.Factor), C.sizeof(abi.VelTerm),
+            C.sizeof(abi.VelocityDesc), C.sizeof(abi.ICNode), C.sizeof(abi.ICDesc), C.sizeof(abi.ReinitOpts),
+            C.sizeof(abi.LSOpts), abi.ICDesc.waves.offset]
+    assert vals == mine
+
+
+def test_defaults_are_reference_defaults(flsp):
+    L = flsp.load()
+    o = abi.DGOpts()
+    L.flsp_default_dg_opts(C.byref(o))
+    assert (o.rk_order, o.cfl_max, o.basis) == (3, 0.9, abi.BASIS_P)   # AdvectControl, FE_DGP
+    r = abi.ReinitOpts()
+    L.flsp_default_reinit_opts(C.byref(r))
+    # ReinitControl (rktvd1, CFL 0.1-0.2) + AdditionalControl (max_iter 1000, band 4)
+    assert (r.mode, r.rk_order, r.cfl_max, r.max_iter, r.band_width_coeff) == (abi.REINIT_BAND, 1, 0.2, 1000, 4.0)
+    ls = abi.LSOpts()
+    L.flsp_default_ls_opts(C.byref(ls))
+    assert (ls.reinit_frequency, ls.execute_reinit) == (10, 1)   # LevelSetControl
+
+
+def _cuda_visible():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_cuda_visible(), reason="a GPU is visible")
+def test_no_gpu_fails_loudly(flsp):
+    from felspa_b200.level_set import Mesh, Problem
+    with pytest.raises(flsp.FlspError) as e:
+        Problem(Mesh(2, (8, 8)), 1)
+    assert e.value.code == abi.FLSP_ERR_NO_DEVICE
+
+
+def test_bad_arguments_rejected(flsp):
+    L = flsp.load()
+    m = abi.mesh_desc(4, (8, 8, 8))
+    o = abi.DGOpts()
+    L.flsp_default_dg_opts(C.byref(o))
+    h = C.c_void_p()
+    assert L.flsp_create(C.byref(m), C.byref(o), C.byref(h)) == abi.FLSP_ERR_BAD_ARG
+    assert b"dim" in L.flsp_last_error()
+    m = abi.mesh_desc(3, (8, 8, 8))
+    o.degree = 3
+    assert L.flsp_create(C.byref(m), C.byref(o), C.byref(h)) == abi.FLSP_ERR_UNSUPPORTED
+    assert L.flsp_create(None, C.byref(o), C.byref(h)) == abi.FLSP_ERR_BAD_ARG
+
+
+def test_product_does_not_reference_oracle():
+    """the product path never imports, links or loads the oracle"""
+    pkg = os.path.join(ROOT, "felspa_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".h")):
+                text = open(os.path.join(dirpath, f)).read()
+                assert "oracle" not in text.lower(), f

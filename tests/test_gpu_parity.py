@@ -233,3 +233,75 @@ def test_nonfinite_rejected(flsp):
     with pytest.raises(FlspError) as e:
         sim.problem.set_state(bad)
     assert e.value.code == abi.FLSP_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("dim,p,basis,mode", [(2, 1, abi.BASIS_P, abi.REINIT_BAND), (2, 2, abi.BASIS_Q, abi.REINIT_FIXED),
+                                              (3, 2, abi.BASIS_Q, abi.REINIT_FIXED)])
+def test_reinit_viscosity(oracle, flsp, dim, p, basis, mode):
+    """LDG artificial viscosity (the reference Zalesak test uses nu = 0.001)"""
+    n = (20, 20) if dim == 2 else (8, 8, 8)
+    if dim == 2:
+        ic = F.sphere((0.5137, 0.4871), 0.3) + F.sphere((0.3071, 0.3529), 0.15)
+    else:
+        ic = F.sphere((0.4137, 0.5071, 0.4529), 0.25)
+    field = F.ccw_rotation() if dim == 2 else F.deformation_3d()
+    sim, orc, phi = make_pair(oracle, dim, n, p, basis, field, ic)
+    o = abi.default_reinit_opts(mode=mode, n_pseudo_steps=4, viscosity=0.001, cfl_max=0.3)
+    nit = ReinitSimulatorLDG(sim.problem).run_iteration(o)
+    st, nit_o = orc.reinit(phi, o)
+    assert st == 0 and nit == nit_o and nit > 0
+    assert rel(sim.get_solution_vector(), phi) <= 1e-11
+
+
+@pytest.mark.parametrize("name", ["zalesak_p1_rhs", "zalesak_q2_rk3", "circles_q2_reinit", "sphere_q2_3d_rhs",
+                                  "sphere_p2_3d_grad"])
+def test_golden_fixtures(flsp, name):
+    """the library against the committed oracle fixtures (tests/golden/)"""
+    import importlib.util
+    import os
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(golden, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    dim, n, p, basis, field, ic, what = mg.cases()[name]
+    ref = np.load(os.path.join(golden, name + ".npz"))
+    sim = AdvectSimulator(Mesh(dim, n), p, basis=basis, precision=abi.FP64, cfl_max=0.1)
+    sim.initialize(ic, field)
+    assert rel(sim.get_solution_vector(), ref["phi0"]) <= TOL
+    if what == "rhs":
+        got = sim.explicit_time_derivative(0.2)
+    elif what == "advance":
+        sim.advance_time(0.05)
+        got = sim.get_solution_vector()
+        assert abs(sim.get_time() - ref["t"][0]) <= 1e-15
+    elif what == "reinit":
+        ReinitSimulatorLDG(sim.problem).run_iteration(abi.default_reinit_opts(mode=abi.REINIT_FIXED,
+                                                                              n_pseudo_steps=3))
+        got = sim.get_solution_vector()
+    else:
+        gl, gr = ReinitSimulatorLDG(sim.problem).local_left_right_gradients()
+        got = np.concatenate([gl.ravel(), gr.ravel()])
+    assert rel(got, ref["result"]) <= 1e-11
+
+
+def test_cpp_driver_matches_python(flsp):
+    """the C++ facade (include/flsp_dg.hpp) driving the Zalesak test, against
+    the same run through the Python host mirror"""
+    import os
+    import re
+    import subprocess
+    import math
+    exe = os.path.join(os.path.dirname(flsp.LIB_PATH), "examples", "zalesak_disk.bin")
+    out = subprocess.run([exe, "6", "0.001"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr
+    vals = dict(re.findall(r"^(mean \|coeff - initial\|) (\S+)$", out.stdout, re.M))
+    mesh = Mesh(2, (64, 64), (-50, -50), (50, 50), host_cell_order=dealii_hypercube_order(2, 2, 5))
+    ctl = abi.default_ls_opts(reinit_frequency=40, reinit=abi.default_reinit_opts(cfl_max=0.3, viscosity=0.001))
+    ls = LevelSetSurface(mesh, 1, basis=abi.BASIS_P, precision=abi.FP64, control=ctl)
+    disk = F.zalesak_reference()
+    ls.initialize(disk, F.rigid_rotation((0.0, 0.0), math.pi / 314.0))
+    init = ls.get_solution_vector()
+    for _ in range(6):
+        ls.advance_time(1.0)
+    mine = ls.compute_error(init)
+    assert abs(float(vals["mean |coeff - initial|"]) - mine) <= 1e-6 * mine
