@@ -33,6 +33,7 @@ IC_SPHERE, IC_RECT, IC_HEIGHT, IC_UNION, IC_DIFF, IC_INTERSECT = range(6)
 REINIT_BAND, REINIT_GLOBAL, REINIT_FIXED = range(3)
 (RED_MASS, RED_MASS_ERROR, RED_L1_INTERFACE, RED_MEAN_ABS_DIFF, RED_GRAD_DEVIATION,
  RED_MAX_ABS, RED_L2_ERROR_IC, RED_L1_INTERFACE_IC, RED_MASS_SHARP) = range(9)
+NOALLOC_MAX_CELLS = 65536 * 128   # flsp_reduce_noalloc scratch limit (cells)
 
 MAX_VEL_TERMS = 24
 MAX_IC_NODES = 32

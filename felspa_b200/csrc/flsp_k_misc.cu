@@ -1,7 +1,9 @@
 // flsp_k_misc.cu — limiter, projection, reductions, clocks, DoF order
 // (instantiations + launchers).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <string>
 
 #include "flsp_launch.h"
 #include "flsp_misc.cuh"
@@ -162,3 +164,129 @@ int launch_hj_clock_end(cudaStream_t s, DevClock* clk) {
 }
 
 }  // namespace flsp
+
+// ======================================================================
+// Allocation-free reduction (flsp_reduce_noalloc in include/flsp_dg.h).
+//
+// For callers that cannot allocate device memory (all their device memory
+// comes from their own pool / arena): the partial sums live in a file-scope
+// device array instead of a handle's buffer.  Host code must not use the
+// array's name as an address (it is a host-side stand-in), so the device
+// address is looked up once per device with cudaGetSymbolAddress while that
+// device is current, and that pointer is passed to the kernels.  Every call
+// on a device shares the array; each launch writes every partial slot it
+// reads, so nothing has to be cleared between calls, but calls that overlap
+// on the GPU race.
+// ======================================================================
+namespace {
+
+constexpr int kNoAllocBlocks = 65536;                 // 128 cells per block
+constexpr long long kNoAllocDoubles = 2LL * kNoAllocBlocks + 2;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];   // ~1 MiB
+static __device__ __align__(256) flsp_ic_desc g_noalloc_ic;
+
+struct NoAllocDevice {
+  bool ready = false;
+  double* scratch = nullptr;
+  flsp_ic_desc* ic = nullptr;
+};
+NoAllocDevice g_noalloc_dev[64];
+
+__global__ void noalloc_finalize(const double* sums, int which, long long ndofs, double* result) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double r0 = sums[0], r1 = sums[1];
+  double v = r0;
+  if (which == FLSP_RED_MASS_ERROR) v = (r0 - r1) / r1;
+  else if (which == FLSP_RED_MEAN_ABS_DIFF) v = r0 / (double)ndofs;
+  else if (which == FLSP_RED_GRAD_DEVIATION) v = r0 / r1;
+  else if (which == FLSP_RED_L2_ERROR_IC) v = sqrt(r0);
+  *result = v;
+}
+
+}  // namespace
+
+extern "C" int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis, int precision,
+                                   const void* state, const void* ref_state, int which,
+                                   const flsp_ic_desc* ic, double* result, void* stream) {
+  using namespace flsp;
+  if (!mesh || !state || !result) return set_error(FLSP_ERR_BAD_ARG, "null argument");
+  if (mesh->dim < 2 || mesh->dim > 3) return set_error(FLSP_ERR_BAD_ARG, "dim must be 2 or 3");
+  if (!supported_config(mesh->dim, degree)) return set_error(FLSP_ERR_UNSUPPORTED, "unsupported (dim, degree)");
+  if (basis != FLSP_BASIS_P && basis != FLSP_BASIS_Q) return set_error(FLSP_ERR_BAD_ARG, "bad basis");
+  if (precision != FLSP_FP64 && precision != FLSP_FP32) return set_error(FLSP_ERR_BAD_ARG, "bad precision");
+  if (which < 0 || which > FLSP_RED_MASS_SHARP) return set_error(FLSP_ERR_BAD_ARG, "bad reduction kind");
+  const bool need_ic = which == FLSP_RED_MASS_ERROR || which == FLSP_RED_L2_ERROR_IC ||
+                       which == FLSP_RED_L1_INTERFACE_IC;
+  const bool need_ref = which == FLSP_RED_L1_INTERFACE || which == FLSP_RED_MEAN_ABS_DIFF;
+  if (need_ic && !ic) return set_error(FLSP_ERR_BAD_ARG, "this reduction needs an IC");
+  if (need_ref && !ref_state) return set_error(FLSP_ERR_BAD_ARG, "this reduction needs ref_state");
+  if (ic && (ic->n_nodes < 1 || ic->n_nodes > FLSP_MAX_IC_NODES || ic->root < 0 || ic->root >= ic->n_nodes))
+    return set_error(FLSP_ERR_BAD_ARG, "bad IC description");
+  long long ncell = 1;
+  for (int d = 0; d < mesh->dim; ++d) {
+    if (mesh->n[d] < 1 || !(mesh->hi[d] > mesh->lo[d])) return set_error(FLSP_ERR_BAD_MESH, "bad mesh");
+    ncell *= mesh->n[d];
+  }
+  if (ncell > FLSP_NOALLOC_MAX_CELLS)
+    return set_error(FLSP_ERR_BAD_ARG, "mesh has " + std::to_string(ncell) + " cells; flsp_reduce_noalloc "
+                     "supports at most " + std::to_string(FLSP_NOALLOC_MAX_CELLS) + " (fixed scratch size)");
+
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(FLSP_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_error(FLSP_ERR_BAD_ARG, "device ordinal out of range");
+  NoAllocDevice& nd = g_noalloc_dev[dev];
+  if (!nd.ready) {   // once per device, with that device current
+    int st = upload_tables_misc();
+    if (st) return st;
+    e = cudaGetSymbolAddress((void**)&nd.scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    e = cudaGetSymbolAddress((void**)&nd.ic, g_noalloc_ic);
+    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    nd.ready = true;
+  }
+
+  Ctx c;
+  std::memset(&c, 0, sizeof(c));
+  c.dim = mesh->dim;
+  c.p = degree;
+  c.prec = precision;
+  c.basis = basis;
+  c.stream = (cudaStream_t)stream;
+  MeshArgs& m = c.m;
+  double d2 = 0.0, vol = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    m.n[d] = d < mesh->dim ? mesh->n[d] : 1;
+    m.lo[d] = d < mesh->dim ? mesh->lo[d] : 0.0;
+    m.h[d] = d < mesh->dim ? (mesh->hi[d] - mesh->lo[d]) / mesh->n[d] : 1.0;
+    if (d < mesh->dim) { d2 += m.h[d] * m.h[d]; vol *= m.h[d]; }
+  }
+  m.ncell = ncell;
+  m.vol = vol;
+  m.diam = std::sqrt(d2);
+  m.min_diam = m.diam;
+  const int n1 = degree + 1, cz = mesh->dim > 2 ? degree : 0;
+  std::memset(m.q2g, -1, sizeof(m.q2g));
+  std::memset(m.g2q, 0, sizeof(m.g2q));
+  int nb = 0;   // in-cell DoF order: lexicographic (Q) or PolynomialSpace (P: c outer, b, a inner)
+  for (int cc = 0; cc <= cz; ++cc)
+    for (int b = 0; b <= degree; ++b)
+      for (int a = 0; a <= degree; ++a) {
+        if (basis == FLSP_BASIS_P && a + b + cc > degree) continue;
+        const int q = a + n1 * (b + n1 * cc);
+        m.q2g[q] = (signed char)nb;
+        m.g2q[nb++] = (signed char)q;
+      }
+  m.nb = nb;
+
+  if (ic) {
+    e = cudaMemcpyAsync(nd.ic, ic, sizeof(flsp_ic_desc), cudaMemcpyHostToDevice, c.stream);
+    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("IC copy: ") + cudaGetErrorString(e));
+  }
+  double* partial = nd.scratch;
+  double* sums = nd.scratch + 2LL * kNoAllocBlocks;
+  int st = launch_reduce(c, which, state, need_ref ? ref_state : nullptr, need_ic ? nd.ic : nullptr, partial, sums);
+  if (st) return st;
+  noalloc_finalize<<<1, 1, 0, c.stream>>>(sums, which, ncell * nb, result);
+  return launch_status("noalloc_finalize");
+}

@@ -174,6 +174,20 @@ class Problem:
         return out.value
 
 
+def reduce_noalloc(mesh, fe_degree, basis, precision, state_ptr, which, result_ptr, ref_ptr=None,
+                   ic=None, stream=None):
+    """Enqueue flsp_reduce_noalloc: the reduction `which` of a caller-owned
+    device state (lexicographic cells) into the caller's device double at
+    `result_ptr`, on `stream` (a cudaStream_t handle, None = default stream),
+    without allocating device memory.  Pointers are integer device addresses."""
+    md = mesh.desc()
+    icd = C.byref(ic.desc()) if ic is not None else None
+    check(load().flsp_reduce_noalloc(C.byref(md), int(fe_degree), int(basis), int(precision),
+                                     C.c_void_p(state_ptr), C.c_void_p(ref_ptr) if ref_ptr else None,
+                                     int(which), icd, C.c_void_p(result_ptr),
+                                     C.c_void_p(stream) if stream else None))
+
+
 # ----------------------------------------------------------------------
 # reference-named simulators
 # ----------------------------------------------------------------------

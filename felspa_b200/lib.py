@@ -47,6 +47,8 @@ PROTOTYPES = {
     "flsp_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "flsp_time_kernel": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "flsp_reduce": (C.c_int, [_vp, C.c_int, C.POINTER(abi.ICDesc), _dp]),
+    "flsp_reduce_noalloc": (C.c_int, [C.POINTER(abi.MeshDesc), C.c_int, C.c_int, C.c_int, _vp, _vp,
+                                      C.c_int, C.POINTER(abi.ICDesc), _vp, _vp]),
     "flsp_default_dg_opts": (None, [C.POINTER(abi.DGOpts)]),
     "flsp_default_reinit_opts": (None, [C.POINTER(abi.ReinitOpts)]),
     "flsp_default_ls_opts": (None, [C.POINTER(abi.LSOpts)]),

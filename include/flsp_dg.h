@@ -284,6 +284,31 @@ int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch)
 int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic,
                 double* out);
 
+/* Allocation-free reduction.  No counterpart in the reference: FELSPA
+   computes these diagnostics on the host.  Same arithmetic as flsp_reduce,
+   but for callers that cannot allocate device memory: host codes that own
+   all device memory through their own pool or arena and forbid driver
+   allocations outside it.  It takes no handle: the
+   state is the caller's device array (lexicographic cells, deal.II DoF
+   order inside a cell, double for FLSP_FP64 / float for FLSP_FP32),
+   `ref_state` the caller's device array for the snapshot reductions (or
+   NULL), `ic` a host IC description (or NULL), and the scalar result is
+   written to the caller's device double `result`.  Work is enqueued on
+   `stream` (a cudaStream_t, NULL = default stream) and not waited for.
+   Scratch space is a file-scope device array of 1 MiB (partial sums of at
+   most FLSP_NOALLOC_MAX_CELLS cells); larger meshes are rejected with
+   FLSP_ERR_BAD_ARG.  The first call on a device uploads the basis tables
+   and looks up the array's device address (synchronous); make that first
+   call before any stream capture.  All calls on a device share the array
+   and it keeps the last call's contents: calls that overlap on the GPU
+   race.                                                                 */
+#define FLSP_NOALLOC_MAX_CELLS (65536LL * 128LL)
+int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis,
+                        int precision, const void* state,
+                        const void* ref_state, int which,
+                        const flsp_ic_desc* ic, double* result,
+                        void* stream);
+
 /* default option structs (reference defaults) */
 void flsp_default_dg_opts(flsp_dg_opts* o);
 void flsp_default_reinit_opts(flsp_reinit_opts* o);
