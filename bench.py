@@ -294,7 +294,7 @@ def run_ours(args):
     tr = read_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tr or {}).get("adv_stage_bytes_per_launch"),
-                "kernel": "adv_stage_kernel<3,2,float>", "ms_per_launch": ms_stage,
+                "kernel": "adv_sep_kernel<3,2,float>", "ms_per_launch": ms_stage,
                 "algorithmic_bytes_per_launch": alg_bytes_per_launch, "peak_source": peak_kind,
                 "hj_ms_per_launch": ms_hj}
 

@@ -179,10 +179,9 @@ __device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T c
   }
 }
 
-// SEP1: every velocity component is a single separable term and term k is
-// component k (the host reorders; the fields of the benchmark
-// configurations are of this form); otherwise a runtime sum over terms.
-template <int DIM, int P, bool SEP1, typename T>
+// General velocity: a runtime sum of separable terms per component.  (A
+// velocity whose components are single terms takes adv_sep_kernel.)
+template <int DIM, int P, typename T>
 __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -246,32 +245,14 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
   // velocity component `comp` (times the time factor) at table columns
   auto vel = [&](int comp, int jx, int jy, int jz) -> T {
     T u = T(0);
-    if constexpr (SEP1) {
-      u = vrow(comp, 0)[jx] * vrow(comp, 1)[jy];
-      if constexpr (DIM == 3) u = u * vrow(comp, 2)[jz];
-    } else {
-      for (int k = 0; k < nterm; ++k) {
-        if (a.v.comp[k] != comp) continue;
-        T v = vrow(k, 0)[jx] * vrow(k, 1)[jy];
-        if constexpr (DIM == 3) v = v * vrow(k, 2)[jz];
-        u += v;
-      }
+    for (int k = 0; k < nterm; ++k) {
+      if (a.v.comp[k] != comp) continue;
+      T v = vrow(k, 0)[jx] * vrow(k, 1)[jy];
+      if constexpr (DIM == 3) v = v * vrow(k, 2)[jz];
+      u += v;
     }
     return u * ct;
   };
-
-  // SEP1: x-factors of the cell with the x weights folded in
-  T Xw[DIM][NQ];
-  if constexpr (SEP1) {
-    if (work) {
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const T* xr = vrow(d, 0);
-#pragma unroll
-        for (int qx = 0; qx < NQ; ++qx) Xw[d][qx] = xr[qx] * tb.wq[qx];
-      }
-    }
-  }
 
   if (work) {
     // ============================ cell term ============================
@@ -289,26 +270,15 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
         T X1[N1], X2[N1];
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa) { X1[aa] = T(0); X2[aa] = T(0); }
-        T Yc[2];
-        if constexpr (SEP1) {
-#pragma unroll
-          for (int d = 0; d < 2; ++d) Yc[d] = vrow(d, 1)[qy] * tb.wq[qy] * ct * ih[d];
-        }
 #pragma unroll
         for (int qx = 0; qx < NQ; ++qx) {
           T phi = T(0);
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
-          T fx, fy;
-          if constexpr (SEP1) {
-            fx = phi * Xw[0][qx] * Yc[0];
-            fy = phi * Xw[1][qx] * Yc[1];
-          } else {
-            const T u0 = vel(0, qx, qy, 0), u1 = vel(1, qx, qy, 0);
-            const T w = tb.wq[qx] * tb.wq[qy] * phi;
-            fx = w * u0 * ih[0];
-            fy = w * u1 * ih[1];
-          }
+          const T u0 = vel(0, qx, qy, 0), u1 = vel(1, qx, qy, 0);
+          const T w = tb.wq[qx] * tb.wq[qy] * phi;
+          const T fx = w * u0 * ih[0];
+          const T fy = w * u1 * ih[1];
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) {
             X1[aa] += fx * tb.Dq[aa][qx];
@@ -339,18 +309,8 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
         for (int aa = 0; aa < N1; ++aa)
 #pragma unroll
           for (int b = 0; b < N1; ++b) { U1[aa][b] = T(0); U3[aa][b] = T(0); }
-        T Zc[3];
-        if constexpr (SEP1) {
-#pragma unroll
-          for (int d = 0; d < 3; ++d) Zc[d] = vrow(d, 2)[qz] * tb.wq[qz] * ct * ih[d];
-        }
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
-          T YZ[3];
-          if constexpr (SEP1) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) YZ[d] = vrow(d, 1)[qy] * tb.wq[qy] * Zc[d];
-          }
           T Py[N1];
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) {
@@ -367,18 +327,11 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
             T phi = T(0);
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
-            T fx, fy, fz;
-            if constexpr (SEP1) {
-              fx = phi * Xw[0][qx] * YZ[0];
-              fy = phi * Xw[1][qx] * YZ[1];
-              fz = phi * Xw[2][qx] * YZ[2];
-            } else {
-              const T u0 = vel(0, qx, qy, qz), u1 = vel(1, qx, qy, qz), u2 = vel(2, qx, qy, qz);
-              const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
-              fx = w * u0 * ih[0];
-              fy = w * u1 * ih[1];
-              fz = w * u2 * ih[2];
-            }
+            const T u0 = vel(0, qx, qy, qz), u1 = vel(1, qx, qy, qz), u2 = vel(2, qx, qy, qz);
+            const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
+            const T fx = w * u0 * ih[0];
+            const T fy = w * u1 * ih[1];
+            const T fz = w * u2 * ih[2];
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) {
               X1[aa] += fx * tb.Dq[aa][qx];
@@ -410,33 +363,15 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
   auto face_vel = [&](auto EC, auto SC) {
     constexpr int E = decltype(EC)::value, S = decltype(SC)::value;
     constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-    if constexpr (SEP1) {
-      const T* rows[3] = {vrow(E, 0), vrow(E, 1), DIM > 2 ? vrow(E, 2) : nullptr};
-      const T fe = rows[E][NQ + S] * ct;
-      T a0[NQ], a1[NQ];
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        a0[q] = rows[t0][q] * tb.wq[q];
-        a1[q] = DIM > 2 ? rows[t1][q] * tb.wq[q] : T(1);
-      }
-      return [=](int q0, int q1) -> T {
-        // ((f_x f_y) f_z) in axis order, weights folded in
-        if constexpr (DIM == 2) return (E == 0 ? fe * a0[q0] : a0[q0] * fe);
-        else if constexpr (E == 0) return (fe * a0[q0]) * a1[q1];
-        else if constexpr (E == 1) return (a0[q0] * fe) * a1[q1];
-        else return (a0[q0] * a1[q1]) * fe;
-      };
-    } else {
-      return [&, E, S](int q0, int q1) -> T {
-        int j[3] = {0, 0, 0};
-        j[E] = NQ + S;
-        j[t0] = q0;
-        if (DIM > 2) j[t1] = q1;
-        T w = tb.wq[q0];
-        if constexpr (DIM > 2) w = w * tb.wq[q1];
-        return vel(E, j[0], j[1], j[2]) * w;
-      };
-    }
+    return [&, E, S](int q0, int q1) -> T {
+      int j[3] = {0, 0, 0};
+      j[E] = NQ + S;
+      j[t0] = q0;
+      if (DIM > 2) j[t1] = q1;
+      T w = tb.wq[q0];
+      if constexpr (DIM > 2) w = w * tb.wq[q1];
+      return vel(E, j[0], j[1], j[2]) * w;
+    };
   };
 
   // ============ upper faces: computed once, shared with the upper neighbour

@@ -117,6 +117,7 @@ struct flsp_handle {
   bool has_snap = false;
   void* vtab = nullptr;
   double* vtab64 = nullptr;
+  void* optab = nullptr;          // separable-operator rows (sep1 velocities)
   bool has_vel = false;
   flsp_velocity_desc vel;
   int nmax = 1, npt = 1;
@@ -157,6 +158,7 @@ struct flsp_handle {
     for (int k = 0; k < vel_dev.n_terms; ++k) v.comp[k] = vel_dev.terms[k].comp;
     v.sep1 = vel_dev.n_terms == dim;
     for (int k = 0; k < vel_dev.n_terms; ++k) v.sep1 = v.sep1 && vel_dev.terms[k].comp == k;
+    v.optab = v.sep1 ? optab : nullptr;
     return v;
   }
 };
@@ -188,8 +190,8 @@ int sync_clock(flsp_handle* h) {
 // done outside any stream capture
 int prepare_kernels(flsp_handle* h) {
   Ctx c = h->ctx();
-  ST(adv_default_tile(c, h->vel_dev.n_terms, h->adv_tile));
-  ST(adv_prepare(c, h->vel_dev.n_terms, h->adv_tile));
+  ST(adv_default_tile(c, h->veldev(), h->adv_tile));
+  ST(adv_prepare(c, h->veldev(), h->adv_tile));
   ST(hj_default_tile(c, h->hj_tile));
   ST(hj_prepare(c, h->hj_tile));
   ST(ldg_prepare(c));
@@ -382,6 +384,65 @@ void layout_velocity(flsp_handle* h) {
   h->vel_dev = r;
 }
 
+// Per-axis operator rows of a velocity whose component d is the single
+// separable term d (the stage kernel's separable path, flsp_advsep.cuh).
+// For component d, axis e and cell index i along e, with g = the term's
+// axis-e factor at the cell's QGauss(p+2) points:
+//   A[a][b] = sum_q w_q g(x_q) L_b(x_q) (e == d ? L_a'(x_q) : L_a(x_q))
+//   e != d: B[a][b] = sum_q w_q |g(x_q)| L_a(x_q) L_b(x_q)  (at element boff)
+//   e == d: g(0), g(1)                                      (at element boff)
+// All in FP64 (long double sums) from the same factor values as the
+// point-wise tables, stored in the state precision.
+int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
+  if (h->optab) cudaFree(h->optab);
+  h->optab = nullptr;
+  VelDev vd = h->veldev();
+  if (!vd.sep1) return FLSP_OK;
+  const int n1 = h->p + 1, nq = h->p + 2, nn = n1 * n1;
+  const int boff = ((nn + 3) / 4) * 4, opw = 2 * boff;
+  const size_t nrow = (size_t)h->dim * 3 * h->nmax;
+  std::vector<double> op(nrow * opw, 0.0);
+  double x[8], w[8], lv[8][8], ld[8][8];
+  gauss_rule(nq, x, w);
+  for (int q = 0; q < nq; ++q) {
+    double dd[8];
+    leg_all(n1, x[q], lv[q], ld[q], dd);
+  }
+  for (int d = 0; d < h->dim; ++d)
+    for (int e = 0; e < h->dim; ++e)
+      for (int i = 0; i < h->m.n[e]; ++i) {
+        const size_t r = ((size_t)d * 3 + e) * h->nmax + i;
+        const double* gq = &tabd[r * h->npt];   // term d == component d
+        double* row = &op[r * opw];
+        for (int al = 0; al < n1; ++al)
+          for (int be = 0; be < n1; ++be) {
+            long double sa = 0.0L, sb = 0.0L;
+            for (int q = 0; q < nq; ++q) {
+              const long double t = (long double)w[q] * gq[q] * lv[q][be];
+              sa += t * (e == d ? ld[q][al] : lv[q][al]);
+              sb += (long double)w[q] * std::fabs(gq[q]) * lv[q][be] * lv[q][al];
+            }
+            row[al * n1 + be] = (double)sa;
+            if (e != d) row[boff + al * n1 + be] = (double)sb;
+          }
+        if (e == d) {
+          row[boff] = gq[nq];          // xi = 0
+          row[boff + 1] = gq[nq + 1];  // xi = 1
+        }
+      }
+  const size_t n = op.size();
+  if (h->prec == FLSP_FP64) {
+    CU(cudaMalloc(&h->optab, n * sizeof(double)));
+    CU(cudaMemcpy(h->optab, op.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> of(n);
+    for (size_t i = 0; i < n; ++i) of[i] = (float)op[i];
+    CU(cudaMalloc(&h->optab, n * sizeof(float)));
+    CU(cudaMemcpy(h->optab, of.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return FLSP_OK;
+}
+
 int build_vtab(flsp_handle* h) {
   const int dim = h->dim;
   layout_velocity(h);
@@ -424,6 +485,7 @@ int build_vtab(flsp_handle* h) {
     CU(cudaMalloc(&h->vtab, n * sizeof(float)));
     CU(cudaMemcpy(h->vtab, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   }
+  ST(build_optab(h, tabd));
   // static CFL part: max over vertices of |u_spatial| / diam
   int comp[kMaxTerms];
   for (int k = 0; k < h->vel_dev.n_terms; ++k) comp[k] = h->vel_dev.terms[k].comp;
@@ -583,6 +645,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->rdiff) cudaFree(h->rdiff);
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
+  if (h->optab) cudaFree(h->optab);
   if (h->clk) cudaFree(h->clk);
   if (h->clk_host) cudaFreeHost(h->clk_host);
   if (h->perm) cudaFree(h->perm);

@@ -67,10 +67,13 @@ struct VelDev {
   int n_terms, nmax, npt;
   int comp[kMaxTerms];
   bool sep1;           // term k is the only term of component k
+  const void* optab;   // per-axis operator rows of a sep1 velocity (T precision), or null
 };
+// stage kernel of this velocity: separable-operator kernel when optab is set
+inline bool use_sep_kernel(const VelDev& v) { return v.sep1 && v.optab != nullptr; }
 // tile: cells per CTA (nullptr = default); smem attribute is set on first use
-int adv_default_tile(const Ctx& c, int n_terms, int* tile);
-int adv_prepare(const Ctx& c, int n_terms, const int* tile);
+int adv_default_tile(const Ctx& c, const VelDev& v, int* tile);
+int adv_prepare(const Ctx& c, const VelDev& v, const int* tile);
 int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* phin, void* out,
                      const DevClock* clk, int stage, int combine, double ct_explicit,
                      const int* tile);

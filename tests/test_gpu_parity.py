@@ -65,6 +65,41 @@ def test_advect_rhs_3d(oracle, flsp, p, basis):
         assert rel(sim.explicit_time_derivative(t), orc.advect_rhs(phi, t)) <= TOL
 
 
+def drifting_deformation_3d():
+    """3D deformation plus a uniform drift: two separable terms per
+    component, so the stage runs the point-wise quadrature kernel."""
+    base = F.deformation_3d()
+    drift = F.constant((0.3, -0.2, 0.1))
+    return F.VelocityField(3, base.terms + drift.terms, time_kind=base.time_kind, ta=base.ta,
+                           tb=base.tb, name="drifting_deformation_3d")
+
+
+@pytest.mark.parametrize("p,basis", CASES_2D)
+def test_advect_rhs_2d_multiterm(oracle, flsp, p, basis):
+    # 8-mode Fourier stream function: several terms per component
+    field = F.fourier_stream_2d(seed=1007)
+    sim, orc, phi = make_pair(oracle, 2, (22, 19), p, basis, field, F.zalesak_disk())
+    for t in (0.0, 0.4):
+        assert rel(sim.explicit_time_derivative(t), orc.advect_rhs(phi, t)) <= TOL
+
+
+@pytest.mark.parametrize("p,basis", CASES_3D)
+def test_advect_rhs_3d_multiterm(oracle, flsp, p, basis):
+    ic = F.sphere((0.35, 0.35, 0.35), 0.15)
+    sim, orc, phi = make_pair(oracle, 3, (9, 8, 10), p, basis, drifting_deformation_3d(), ic)
+    for t in (0.0, 0.7):
+        assert rel(sim.explicit_time_derivative(t), orc.advect_rhs(phi, t)) <= TOL
+
+
+@pytest.mark.parametrize("p,basis", CASES_3D)
+def test_advect_rhs_3d_missing_component(oracle, flsp, p, basis):
+    # plume rolls: no y component (a zero term stands in for it)
+    ic = F.perturbed_plane(seed=3)
+    sim, orc, phi = make_pair(oracle, 3, (8, 9, 10), p, basis, F.plume_3d(), ic)
+    for t in (0.0, 1.3):
+        assert rel(sim.explicit_time_derivative(t), orc.advect_rhs(phi, t)) <= TOL
+
+
 @pytest.mark.parametrize("rk", [1, 2, 3])
 def test_advance_2d(oracle, flsp, rk):
     mesh = Mesh(2, (32, 32))
@@ -220,6 +255,17 @@ def test_fp32_mode_close(oracle, flsp):
     for prec in (abi.FP32, abi.FP64):
         s = AdvectSimulator(Mesh(3, (16, 16, 16)), 2, basis=abi.BASIS_Q, precision=prec, cfl_max=0.1)
         s.initialize(ic, F.deformation_3d())
+        s.advance_steps(20)
+        sims.append(s.get_solution_vector())
+    assert rel(sims[0], sims[1]) <= 1e-4
+
+
+def test_fp32_mode_close_multiterm(oracle, flsp):
+    ic = F.sphere((0.35, 0.35, 0.35), 0.15)
+    sims = []
+    for prec in (abi.FP32, abi.FP64):
+        s = AdvectSimulator(Mesh(3, (12, 12, 12)), 2, basis=abi.BASIS_Q, precision=prec, cfl_max=0.1)
+        s.initialize(ic, drifting_deformation_3d())
         s.advance_steps(20)
         sims.append(s.get_solution_vector())
     assert rel(sims[0], sims[1]) <= 1e-4
