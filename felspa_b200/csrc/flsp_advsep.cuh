@@ -54,7 +54,17 @@ struct AdvSepArgs {
   double dt_explicit;
 };
 
-// tile box with face halo, operator rows of the tile, upper-face fluxes
+// Face-flux slots of a tile along axis E: every face normal to E that
+// touches a tile cell, i.e. tile[E] + 1 faces per line along E.  Slot s of
+// a line is the face below tile cell s (s = tile[E]: the tile's top face).
+__host__ __device__ inline int sep_face_slots(const int* tile, int dim, int E) {
+  int n = 1;
+  for (int d = 0; d < dim; ++d) n *= tile[d] + (d == E ? 1 : 0);
+  return n;
+}
+
+// shared memory: tile box with face halo | operator rows of the tile |
+// face fluxes per axis (reused for the tile's R before the store)
 template <int DIM, int P, typename T>
 __host__ __device__ inline size_t sep_smem_bytes(const int* tile) {
   constexpr int N1 = P + 1, NM = ipow(N1, DIM), NF = ipow(N1, DIM - 1), OPW = sep_opw<P>();
@@ -63,7 +73,9 @@ __host__ __device__ inline size_t sep_smem_bytes(const int* tile) {
   const int span = tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0);
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
   size_t ops = (size_t)DIM * span * OPW * sizeof(T);
-  size_t fl = (size_t)DIM * NF * nt * sizeof(T);
+  size_t fl = 0;
+  for (int E = 0; E < DIM; ++E) fl += (size_t)NF * sep_face_slots(tile, DIM, E);
+  fl = (fl > (size_t)nt * NM ? fl : (size_t)nt * NM) * sizeof(T);
   return box + ops + fl + 16;
 }
 
@@ -220,12 +232,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   const MeshArgs& m = a.m;
   const int nboxc = box_cells(m, DIM);
   const int tx = m.tile[0], ty = m.tile[1], tz = m.tile[2];
+  const int tl[3] = {tx, ty, tz};
   const int nt = tx * ty * tz;
   const int span = tx + ty + (DIM > 2 ? tz : 0);
   const int roff[3] = {0, tx, tx + ty};   // first row of each axis within a component
   // box holds NM values per cell; keep the operator rows 16-byte aligned
   T* ops = align16<T>(box + (size_t)nboxc * NM);
-  T* fl = ops + (size_t)DIM * span * OPW;   // [DIM][NF][nt]
+  T* fl = ops + (size_t)DIM * span * OPW;   // face fluxes, then the tile's R
+  int flo[3] = {0, 0, 0};                   // section offsets of the face fluxes
+  for (int E = 1; E < DIM; ++E) flo[E] = flo[E - 1] + NF * sep_face_slots(m.tile, DIM, E - 1);
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM);
 
@@ -257,127 +272,179 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   const T ih[3] = {T(1.0 / m.h[0]), T(1.0 / m.h[1]), T(DIM > 2 ? 1.0 / m.h[2] : 1.0)};
   const int g[3] = {tc.gx, tc.gy, tc.gz};
   const int l[3] = {tc.lx, tc.ly, tc.lz};
-  const int tl[3] = {tx, ty, tz};
   const bool work = tc.valid && active;
 
-  auto row = [&](int d, int e) -> const T* { return ops + (size_t)(d * span + roff[e] + l[e]) * OPW; };
+  auto rowp = [&](int d, int e, int le) -> const T* {
+    return ops + (size_t)(d * span + roff[e] + le) * OPW;
+  };
+  // face-flux slot of the face below local cell lc along E (lc[E] in [0, tile[E]])
+  auto slot = [&](int E, const int* lc) -> int {
+    const int e0 = tl[0] + (E == 0), e1 = tl[1] + (E == 1);
+    return lc[0] + e0 * (lc[1] + (DIM > 2 ? e1 * lc[2] : 0));
+  };
+  auto flux_at = [&](int E, int mf, int sl) -> T& {
+    return fl[flo[E] + (size_t)mf * sep_face_slots(m.tile, DIM, E) + sl];
+  };
 
-  T R[NM];
-  T c[NM];
-#pragma unroll
-  for (int q = 0; q < NM; ++q) R[q] = T(0);
-  if (tc.valid) {
-#pragma unroll
-    for (int q = 0; q < NM; ++q) c[q] = box[(size_t)me * NM + q];
-  }
-
-  if (work) {
-    // ============================ cell term ============================
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      T M0[N1][N1], M1[N1][N1], M2[N1][N1];
-      load_op<N1, T>(row(d, 0), M0);
-      load_op<N1, T>(row(d, 1), M1);
-      if constexpr (DIM > 2) load_op<N1, T>(row(d, 2), M2);
-      apply_sep_acc<DIM, N1, T>(M0, M1, M2, c, R, ct * ih[d]);
-    }
-  }
-
-  // flux F through the face normal to E in +e_E, from the traces of the
-  // lower (Tm) and upper (Tp) cell; g_EE at the face is `fe`
-  auto face_flux_sep = [&](auto EC, const T* Tm, const T* Tp, bool interior, T fe, T* F) {
+  // flux through the face normal to E in +e_E between the lower cell (L1
+  // trace of cm) and the upper cell (L0 trace of cp); a missing side takes
+  // the other side's trace (domain boundary: own trace).  Tangential
+  // operator rows at local coordinates lc, g_EE at the face = fe.
+  auto face_flux_sep = [&](auto EC, const T* cm, const T* cp, bool has_m, bool has_p, const int* lc,
+                           T fe, T* F) {
     constexpr int E = decltype(EC)::value;
     constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-    T S[NF], D[NF];
+    T Tm[NF], Tp[NF], S[NF], D[NF];
+    if (has_m) face_trace<DIM, N1, E, T>(cm, tb.L1, Tm);
+    if (has_p) face_trace<DIM, N1, E, T>(cp, tb.L0, Tp);
 #pragma unroll
     for (int mf = 0; mf < NF; ++mf) {
+      if (!has_m) Tm[mf] = Tp[mf];
+      if (!has_p) Tp[mf] = Tm[mf];
       S[mf] = T(0.5) * (Tm[mf] + Tp[mf]);
       D[mf] = T(0.5) * (Tm[mf] - Tp[mf]);
     }
     const T s1 = ct * fe;
-    face_apply<DIM, N1, BOFF, T>(row(E, t0), DIM > 2 ? row(E, t1) : nullptr, S, D, s1, s1 < T(0) ? -s1 : s1,
-                           interior, F);
+    face_apply<DIM, N1, BOFF, T>(rowp(E, t0, lc[t0]), DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr, S, D, s1,
+                                 s1 < T(0) ? -s1 : s1, has_m && has_p, F);
   };
 
-  // ============ upper faces: computed once, shared with the upper neighbour
-  auto do_upper = [&](auto EC) {
-    constexpr int E = decltype(EC)::value;
-    if (!work) return;
-    int nl[3] = {l[0], l[1], l[2]};
-    nl[E] += 1;
-    const bool has_nb = g[E] + 1 < m.n[E];
-    T Tm[NF], Tp[NF], F[NF];
-    face_trace<DIM, N1, E, T>(c, tb.L1, Tm);
-    if (has_nb) {
-      const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
-      face_trace<DIM, N1, E, T>(cn, tb.L0, Tp);
-    } else {
+  T R[NM];
 #pragma unroll
-      for (int mf = 0; mf < NF; ++mf) Tp[mf] = Tm[mf];
+  for (int q = 0; q < NM; ++q) R[q] = T(0);
+
+  if (work) {
+    T c[NM];
+#pragma unroll
+    for (int q = 0; q < NM; ++q) c[q] = box[(size_t)me * NM + q];
+    // ============================ cell term ============================
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      T M0[N1][N1], M1[N1][N1], M2[N1][N1];
+      load_op<N1, T>(rowp(d, 0, l[0]), M0);
+      load_op<N1, T>(rowp(d, 1, l[1]), M1);
+      if constexpr (DIM > 2) load_op<N1, T>(rowp(d, 2, l[2]), M2);
+      apply_sep_acc<DIM, N1, T>(M0, M1, M2, c, R, ct * ih[d]);
     }
-    face_flux_sep(EC, Tm, Tp, has_nb, row(E, E)[BOFF + 1], F);
-    scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
-    if (has_nb && l[E] + 1 < tl[E]) {
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) fl[(size_t)(E * NF + mf) * nt + cl] = F[mf];
-    }
-  };
-  do_upper(std::integral_constant<int, 0>());
-  do_upper(std::integral_constant<int, 1>());
-  if constexpr (DIM == 3) do_upper(std::integral_constant<int, 2>());
-  __syncthreads();
-  // ============ lower faces: shared flux of the lower neighbour, or own
-  auto do_lower = [&](auto EC) {
-    constexpr int E = decltype(EC)::value;
-    if (!work) return;
-    T F[NF];
-    const int stride = E == 0 ? 1 : (E == 1 ? tx : tx * ty);
-    if (l[E] > 0 && g[E] > 0) {
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) F[mf] = fl[(size_t)(E * NF + mf) * nt + cl - stride];
-    } else {
+    // ===== upper faces: own flux, shared with the upper neighbour via slot l[E] + 1
+    auto do_upper = [&](auto EC) {
+      constexpr int E = decltype(EC)::value;
       int nl[3] = {l[0], l[1], l[2]};
-      nl[E] -= 1;
-      const bool has_nb = g[E] > 0;
-      T Tm[NF], Tp[NF];
-      face_trace<DIM, N1, E, T>(c, tb.L0, Tp);
-      if (has_nb) {
-        const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
-        face_trace<DIM, N1, E, T>(cn, tb.L1, Tm);
-      } else {
+      nl[E] += 1;
+      const bool has_nb = g[E] + 1 < m.n[E];
+      const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
+      T F[NF];
+      face_flux_sep(EC, c, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F);
+      scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
+      const int sl = slot(E, nl);
 #pragma unroll
-        for (int mf = 0; mf < NF; ++mf) Tm[mf] = Tp[mf];
-      }
-      face_flux_sep(EC, Tm, Tp, has_nb, row(E, E)[BOFF], F);
-    }
-    scatter_face<DIM, P, E, T>(R, tb.L0, F, ih[E]);
-  };
-  do_lower(std::integral_constant<int, 0>());
-  do_lower(std::integral_constant<int, 1>());
-  if constexpr (DIM == 3) do_lower(std::integral_constant<int, 2>());
+      for (int mf = 0; mf < NF; ++mf) flux_at(E, mf, sl) = F[mf];
+    };
+    do_upper(std::integral_constant<int, 0>());
+    do_upper(std::integral_constant<int, 1>());
+    if constexpr (DIM == 3) do_upper(std::integral_constant<int, 2>());
+  }
 
-  // ---- combine with phi^n and store through shared memory (coalesced)
-  __syncthreads();
-  T* stage_buf = box;  // reuse: [tile cell][NM]
-  const bool need_n = a.combine == kRK2b || a.combine == kRK3b || a.combine == kRK3c;
-  if (need_n) {
-    load_tile<DIM, NM>(m, a.phi_n, stage_buf, tc.ox, tc.oy, tc.oz, false, NM);
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  if (tc.valid) {
+  // ===== the tile's lower boundary faces (slot 0 of every line), as work
+  // items: axis E's items start at a warp boundary so that a warp serves
+  // one axis
+  if (active) {
+    int nitem[3], ibase[3], tot = 0;
+    for (int E = 0; E < DIM; ++E) {
+      nitem[E] = nt / tl[E];
+      ibase[E] = tot;
+      tot += (nitem[E] + 31) & ~31;
+    }
+    for (int it = threadIdx.x; it < tot; it += blockDim.x) {
+      auto do_item = [&](auto EC) {
+        constexpr int E = decltype(EC)::value;
+        const int k = it - ibase[E];
+        if (k < 0 || k >= nitem[E]) return;
+        // tile cell with local coordinate 0 along E; the others from k
+        constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+        int lc[3] = {0, 0, 0};
+        lc[t0] = k % tl[t0];
+        if (DIM > 2) lc[t1] = k / tl[t0];
+        const int gc[3] = {(E == 0 ? 0 : lc[0]) + tc.ox, (E == 1 ? 0 : lc[1]) + tc.oy,
+                           DIM > 2 ? (E == 2 ? 0 : lc[2]) + tc.oz : 0};
+        if (gc[0] >= m.n[0] || gc[1] >= m.n[1] || (DIM > 2 && gc[2] >= m.n[2])) return;
+        int ll[3] = {lc[0], lc[1], lc[2]};
+        ll[E] -= 1;
+        const bool has_m = gc[E] > 0;
+        const T* cp = box + (size_t)box_index(m, DIM, lc[0], lc[1], lc[2]) * NM;
+        const T* cm = box + (size_t)box_index(m, DIM, ll[0], ll[1], ll[2]) * NM;
+        T F[NF];
+        face_flux_sep(EC, cm, cp, has_m, true, lc, rowp(E, E, 0)[BOFF], F);
+        const int sl = slot(E, lc);
 #pragma unroll
-    for (int q = 0; q < NM; ++q) {
-      T res = c[q];
-      if (active) {
-        const T pn = need_n ? stage_buf[(size_t)cl * NM + q] : T(0);
-        res = combine_value<T>(a.combine, c[q], pn, R[q], dt);
-      }
-      stage_buf[(size_t)cl * NM + q] = res;
+        for (int mf = 0; mf < NF; ++mf) flux_at(E, mf, sl) = F[mf];
+      };
+      do_item(std::integral_constant<int, 0>());
+      do_item(std::integral_constant<int, 1>());
+      if constexpr (DIM == 3) do_item(std::integral_constant<int, 2>());
     }
   }
   __syncthreads();
-  store_tile<DIM, NM>(m, stage_buf, a.out, tc.ox, tc.oy, tc.oz);
+  // ===== lower faces: every cell reads slot l[E]
+  if (work) {
+    auto do_lower = [&](auto EC) {
+      constexpr int E = decltype(EC)::value;
+      const int sl = slot(E, l);
+      T F[NF];
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) F[mf] = flux_at(E, mf, sl);
+      scatter_face<DIM, P, E, T>(R, tb.L0, F, ih[E]);
+    };
+    do_lower(std::integral_constant<int, 0>());
+    do_lower(std::integral_constant<int, 1>());
+    if constexpr (DIM == 3) do_lower(std::integral_constant<int, 2>());
+  }
+  __syncthreads();   // face fluxes consumed: the region now holds R [cell][NM]
+  T* rbuf = fl;
+  if (work) {
+#pragma unroll
+    for (int q = 0; q < NM; ++q) rbuf[(size_t)cl * NM + q] = R[q];
+  }
+  __syncthreads();
+
+  // ---- RK combination fused into the coalesced store: one warp per row of
+  // cells along x; stage input from the box, phi^n straight from HBM
+  const bool need_n = a.combine == kRK2b || a.combine == kRK3b || a.combine == kRK3c;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const bool dense = m.nb == NM;
+  for (int r = warp; r < ty * tz; r += nw) {
+    const int ly = r % ty, lz = r / ty;
+    const int gy = tc.oy + ly, gz = tc.oz + lz;
+    const int nx = min(tx, m.n[0] - tc.ox);
+    if (gy >= m.n[1] || gz >= m.n[2] || nx <= 0) continue;
+    const long long gbase = ((long long)m.n[0] * (gy + (long long)m.n[1] * gz) + tc.ox) * m.nb;
+    const T* cs = box + (size_t)box_index(m, DIM, 0, ly, lz) * NM;
+    const T* rs = rbuf + (size_t)tx * r * NM;
+    if (dense) {
+#pragma unroll 4
+      for (int e = lane; e < nx * NM; e += 32) {
+        const T cv = cs[e];
+        T res = cv;
+        if (active) {
+          const T pn = need_n ? __ldg(a.phi_n + gbase + e) : T(0);
+          res = combine_value<T>(a.combine, cv, pn, rs[e], dt);
+        }
+        a.out[gbase + e] = res;
+      }
+    } else {
+      for (int e = lane; e < nx * m.nb; e += 32) {
+        const int cx = e / m.nb, k = e - cx * m.nb;
+        const int q = cx * NM + m.g2q[k];
+        const T cv = cs[q];
+        T res = cv;
+        if (active) {
+          const T pn = need_n ? __ldg(a.phi_n + gbase + e) : T(0);
+          res = combine_value<T>(a.combine, cv, pn, rs[q], dt);
+        }
+        a.out[gbase + e] = res;
+      }
+    }
+  }
 }
 
 }  // namespace flsp
