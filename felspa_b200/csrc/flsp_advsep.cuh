@@ -18,6 +18,12 @@
 //   boundary T+ = T- (own trace, zero-Neumann inflow), so the second term
 //   vanishes); R- -= L(1) F / h_E, R+ += L(0) F / h_E.
 //
+// The CTA's halo box (one bulk copy per row of cells, each row keeping its
+// 16-byte phase from HBM so that 27-value cells need no splitting) and its
+// operator rows arrive by TMA bulk copies on one mbarrier; the RK
+// combination is fused into a coalesced store that prefetches phi^n into
+// registers.  Tile shapes are compile-time.
+//
 // The per-axis operators are tabulated once per velocity on the host in
 // FP64 (optab, one row per component d, axis e and cell index i:
 // A_de then, at element BOFF, B_de, or for e == d A_dd then g_dd(0),
@@ -43,7 +49,9 @@ template <typename T>
 struct AdvSepArgs {
   MeshArgs m;
   const T* __restrict__ optab;   // [(d*3 + e) * nmax + i][OPW]
-  int nmax;
+  int nmax;                      // row stride per (d, e): >= n[e] + kOpRowPad (a tile's
+                                 // bulk copy of its rows never leaves the table)
+  int* err;                      // device error word (DevClock::err)
   const T* __restrict__ phi_s;
   const T* __restrict__ phi_n;
   T* __restrict__ out;
@@ -54,30 +62,58 @@ struct AdvSepArgs {
   double dt_explicit;
 };
 
-// Face-flux slots of a tile along axis E: every face normal to E that
-// touches a tile cell, i.e. tile[E] + 1 faces per line along E.  Slot s of
-// a line is the face below tile cell s (s = tile[E]: the tile's top face).
-__host__ __device__ inline int sep_face_slots(const int* tile, int dim, int E) {
-  int n = 1;
-  for (int d = 0; d < dim; ++d) n *= tile[d] + (d == E ? 1 : 0);
-  return n;
+// In-cell DoF index (HBM order) of Q-layout mode q (a + N1 b + N1^2 c):
+// itself for FE_DGQLegendre, the PolynomialSpace position (c outer, b,
+// a inner, a + b + c <= P) for FE_DGP, -1 for a mode outside P-space.
+template <int DIM, int P, bool PB>
+__host__ __device__ constexpr int q2g_c(int q) {
+  const int N1 = P + 1;
+  const int a = q % N1, b = (q / N1) % N1, c = DIM > 2 ? q / (N1 * N1) : 0;
+  if (!PB) return q;
+  if (a + b + c > P) return -1;
+  int idx = 0;
+  for (int cc = 0; cc < c; ++cc)
+    for (int bb = 0; bb <= P - cc; ++bb) idx += P - bb - cc + 1;
+  for (int bb = 0; bb < b; ++bb) idx += P - bb - c + 1;
+  return idx + a;
 }
 
-// shared memory: tile box with face halo | operator rows of the tile |
-// face fluxes per axis (reused for the tile's R before the store)
-template <int DIM, int P, typename T>
-__host__ __device__ inline size_t sep_smem_bytes(const int* tile) {
-  constexpr int N1 = P + 1, NM = ipow(N1, DIM), NF = ipow(N1, DIM - 1), OPW = sep_opw<P>();
-  const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
-  const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
-  const int span = tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0);
-  size_t box = (size_t)bx * by * bz * NM * sizeof(T);
-  size_t ops = (size_t)DIM * span * OPW * sizeof(T);
-  size_t fl = 0;
-  for (int E = 0; E < DIM; ++E) fl += (size_t)NF * sep_face_slots(tile, DIM, E);
-  fl = (fl > (size_t)nt * NM ? fl : (size_t)nt * NM) * sizeof(T);
-  return box + ops + fl + 16;
+// a cell's coefficients from its box copy (HBM order) in the Q layout
+template <int DIM, int P, bool PB, typename T>
+__device__ __forceinline__ void load_cell(const T* __restrict__ src, T* cq) {
+  constexpr int NM = ipow(P + 1, DIM);
+#pragma unroll
+  for (int q = 0; q < NM; ++q) {
+    const int gi = q2g_c<DIM, P, PB>(q);
+    cq[q] = gi >= 0 ? src[gi] : T(0);
+  }
 }
+
+// Shared-memory plan of the separable stage kernel for a compile-time tile
+// TX x TY x TZ (TZ = 1 in 2D): mbarrier | halo box rows | operator rows |
+// face fluxes (reused for the tile's R).  Box rows: (TY+2)(TZ+2) slots of
+// SLOT bytes, each holding the row's cells x in [ox-1, ox+TX] from the
+// 16-byte-aligned address at or below the first one.
+template <int DIM, int P, bool PB, int TX, int TY, int TZ, typename T>
+struct SepPlan {
+  static constexpr int N1 = P + 1, NM = ipow(N1, DIM), NF = ipow(N1, DIM - 1);
+  static constexpr int NBG = PB ? (DIM == 2 ? (P + 1) * (P + 2) / 2 : (P + 1) * (P + 2) * (P + 3) / 6) : NM;
+  static constexpr int OPW = sep_opw<P>();
+  static constexpr int NT = TX * TY * TZ;
+  static constexpr int BY = DIM > 1 ? TY + 2 : 1, BZ = DIM > 2 ? TZ + 2 : 1;
+  static constexpr int NROWS = BY * BZ;
+  static constexpr int NMB = NBG * (int)sizeof(T);           // bytes per cell in HBM
+  static constexpr int SLOT = (((TX + 2) * NMB + 30) + 15) / 16 * 16;
+  static constexpr int SPAN = TX + TY + (DIM > 2 ? TZ : 0);
+  static constexpr int SL0 = (TX + 1) * TY * TZ, SL1 = TX * (TY + 1) * TZ,
+                       SL2 = DIM > 2 ? TX * TY * (TZ + 1) : 0;
+  static constexpr int FLN = NF * (SL0 + SL1 + SL2);
+  static constexpr int FLE = FLN > NT * NM ? FLN : NT * NM;  // elements
+  static constexpr size_t OFF_BOX = 16;
+  static constexpr size_t OFF_OPS = OFF_BOX + (size_t)NROWS * SLOT;
+  static constexpr size_t OFF_FL = OFF_OPS + (size_t)DIM * SPAN * OPW * sizeof(T);
+  static constexpr size_t BYTES = OFF_FL + (size_t)FLE * sizeof(T);
+};
 
 // N1 x N1 operator block from shared memory (16-byte aligned)
 template <int N1, typename T>
@@ -223,86 +259,136 @@ __device__ __forceinline__ void face_trace(const T* c, const T* Lside, T* tr) {
 
 // FP32 tiles fit two CTAs per SM (<= 128 registers); an FP64 tile takes most
 // of an SM's shared memory, so FP64 gets the full register file
-template <int DIM, int P, typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(const AdvSepArgs<T> a) {
-  constexpr int N1 = P + 1, NM = ipow(N1, DIM), NF = ipow(N1, DIM - 1);
-  constexpr int OPW = sep_opw<P>(), BOFF = sep_boff<P>();
+template <int DIM, int P, bool PB, int TX, int TY, int TZ, typename T>
+__global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
+    adv_sep_kernel(const AdvSepArgs<T> a) {
+  using PL = SepPlan<DIM, P, PB, TX, TY, TZ, T>;
+  constexpr int N1 = PL::N1, NM = PL::NM, NF = PL::NF, OPW = PL::OPW, BOFF = sep_boff<P>();
+  constexpr int NBG = PL::NBG;
+  constexpr int NT = PL::NT, NMB = PL::NMB, SPAN = PL::SPAN;
+  constexpr int TL[3] = {TX, TY, TZ};
+  constexpr int ROFF[3] = {0, TX, TX + TY};            // first row of each axis within a component
+  constexpr int FLO[3] = {0, NF * PL::SL0, NF * (PL::SL0 + PL::SL1)};
+  constexpr int SLN[3] = {PL::SL0, PL::SL1, PL::SL2};
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* box = reinterpret_cast<T*>(smem_raw);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
+  unsigned char* boxb = smem_raw + PL::OFF_BOX;
+  T* ops = reinterpret_cast<T*>(smem_raw + PL::OFF_OPS);
+  T* fl = reinterpret_cast<T*>(smem_raw + PL::OFF_FL);
   const MeshArgs& m = a.m;
-  const int nboxc = box_cells(m, DIM);
-  const int tx = m.tile[0], ty = m.tile[1], tz = m.tile[2];
-  const int tl[3] = {tx, ty, tz};
-  const int nt = tx * ty * tz;
-  const int span = tx + ty + (DIM > 2 ? tz : 0);
-  const int roff[3] = {0, tx, tx + ty};   // first row of each axis within a component
-  // box holds NM values per cell; keep the operator rows 16-byte aligned
-  T* ops = align16<T>(box + (size_t)nboxc * NM);
-  T* fl = ops + (size_t)DIM * span * OPW;   // face fluxes, then the tile's R
-  int flo[3] = {0, 0, 0};                   // section offsets of the face fluxes
-  for (int E = 1; E < DIM; ++E) flo[E] = flo[E - 1] + NF * sep_face_slots(m.tile, DIM, E - 1);
   const Tab1D<T>& tb = tab<T>(P);
-  const TileCoord tc = tile_coord(m, DIM);
 
-  // ---- operator rows of this tile: ops[(d*span + roff[e] + li)*OPW + k]
-  {
-    const int total = DIM * span * OPW;
-    for (int e2 = threadIdx.x; e2 < total; e2 += blockDim.x) {
-      const int k = e2 % OPW;
-      const int r = e2 / OPW;
-      const int li = r % span;
-      const int d = r / span;
-      int axis, gi;
-      if (li < tx) { axis = 0; gi = tc.ox + li; }
-      else if (li < tx + ty) { axis = 1; gi = tc.oy + (li - tx); }
-      else { axis = 2; gi = tc.oz + (li - tx - ty); }
-      gi = min(gi, m.n[axis] - 1);
-      ops[(size_t)r * OPW + k] = a.optab[((size_t)(d * 3 + axis) * a.nmax + gi) * OPW + k];
+  // tile and cell coordinates
+  int b = blockIdx.x;
+  const int ox = (b % m.ntile[0]) * TX;
+  b /= m.ntile[0];
+  const int oy = DIM > 1 ? (b % m.ntile[1]) * TY : 0;
+  const int oz = DIM > 2 ? (b / m.ntile[1]) * TZ : 0;
+  const int l[3] = {(int)threadIdx.x % TX, ((int)threadIdx.x / TX) % TY, DIM > 2 ? (int)threadIdx.x / (TX * TY) : 0};
+  const int g[3] = {ox + l[0], oy + l[1], oz + l[2]};
+  const bool valid = g[0] < m.n[0] && g[1] < m.n[1] && (DIM < 3 || g[2] < m.n[2]);
+  const int gx0 = max(ox - 1, 0), gx1 = min(ox + TX + 1, m.n[0]);
+
+  // address of the box copy of the cell at local coordinates (lx, ly, lz)
+  auto cellp = [&](int lx, int ly, int lz) -> const T* {
+    const int rr = DIM > 2 ? (ly + 1) + PL::BY * (lz + 1) : ly + 1;
+    const unsigned rowcell = (unsigned)m.n[0] * (unsigned)((oy + ly) + m.n[1] * (DIM > 2 ? oz + lz : 0));
+    const unsigned phase = ((rowcell + (unsigned)gx0) * (unsigned)NMB) & 15u;
+    return reinterpret_cast<const T*>(boxb + (size_t)rr * PL::SLOT + phase + (ox + lx - gx0) * NMB);
+  };
+
+  // ---- staging: box rows and operator rows by bulk copies (warp 0)
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const char* gsrc = reinterpret_cast<const char*>(a.phi_s);
+    // pass 0 counts the bytes, pass 1 issues the copies
+    unsigned bytes = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+        __syncwarp();
+      }
+      for (int rr = lane; rr < PL::NROWS; rr += 32) {
+        const int ly = (DIM > 1 ? rr % PL::BY : 0) - 1, lz = DIM > 2 ? rr / PL::BY - 1 : 0;
+        const bool yout = ly < 0 || ly >= TY, zout = DIM > 2 && (lz < 0 || lz >= TZ);
+        if (yout && zout) continue;
+        const int gy = oy + ly, gz = oz + lz;
+        if (gy < 0 || gy >= m.n[1] || (DIM > 2 && (gz < 0 || gz >= m.n[2]))) continue;
+        const long long rowcell = (long long)m.n[0] * (gy + (long long)m.n[1] * (DIM > 2 ? gz : 0));
+        const long long s0 = (rowcell + gx0) * NMB, s1 = (rowcell + gx1) * NMB;
+        const long long a0 = s0 & ~15LL, a1 = (s1 + 15) & ~15LL;
+        if (pass == 0) bytes += (unsigned)(a1 - a0);
+        else bulk_g2s(boxb + (size_t)rr * PL::SLOT, gsrc + a0, (unsigned)(a1 - a0), bar);
+      }
+      for (int k = lane; k < DIM * DIM; k += 32) {
+        const int d = k / DIM, e = k % DIM;
+        const int o = e == 0 ? ox : (e == 1 ? oy : oz);
+        const unsigned nbytes = (unsigned)(TL[e] * OPW * sizeof(T));
+        if (pass == 0) bytes += nbytes;
+        else
+          bulk_g2s(ops + (size_t)(d * SPAN + ROFF[e]) * OPW,
+                   a.optab + ((size_t)(d * 3 + e) * a.nmax + o) * OPW, nbytes, bar);
+      }
     }
   }
-  load_box<DIM, NM>(m, a.phi_s, box, tc.ox, tc.oy, tc.oz, true);
-  cp_async_wait_all();
-  __syncthreads();
+  if (!mbar_wait(bar, 0, 1 << 22)) {
+    if (threadIdx.x == 0 && a.err) atomicOr(a.err, kErrCopyTimeout);
+    mbar_wait(bar, 0, 1 << 22);   // give copies in flight a last chance to land
+  }
 
   const T ct = a.clk ? T(a.clk->ct[a.stage]) : T(a.ct_explicit);
   const T dt = a.clk ? T(a.clk->dt) : T(a.dt_explicit);
   const bool active = a.clk ? (a.clk->active != 0) : true;
-  const int cl = tc.lx + tx * (tc.ly + ty * tc.lz);
-  const int me = box_index(m, DIM, tc.lx, tc.ly, tc.lz);
+  const int cl = threadIdx.x;
   const T ih[3] = {T(1.0 / m.h[0]), T(1.0 / m.h[1]), T(DIM > 2 ? 1.0 / m.h[2] : 1.0)};
-  const int g[3] = {tc.gx, tc.gy, tc.gz};
-  const int l[3] = {tc.lx, tc.ly, tc.lz};
-  const bool work = tc.valid && active;
+  const bool work = valid && active;
 
   auto rowp = [&](int d, int e, int le) -> const T* {
-    return ops + (size_t)(d * span + roff[e] + le) * OPW;
+    return ops + (size_t)(d * SPAN + ROFF[e] + le) * OPW;
   };
-  // face-flux slot of the face below local cell lc along E (lc[E] in [0, tile[E]])
-  auto slot = [&](int E, const int* lc) -> int {
-    const int e0 = tl[0] + (E == 0), e1 = tl[1] + (E == 1);
+  // face-flux slot of the face below local cell lc along E (lc[E] in [0, TL[E]])
+  auto slot = [&](auto EC, const int* lc) -> int {
+    constexpr int E = decltype(EC)::value;
+    constexpr int e0 = TX + (E == 0), e1 = TY + (E == 1);
     return lc[0] + e0 * (lc[1] + (DIM > 2 ? e1 * lc[2] : 0));
   };
-  auto flux_at = [&](int E, int mf, int sl) -> T& {
-    return fl[flo[E] + (size_t)mf * sep_face_slots(m.tile, DIM, E) + sl];
+  auto flux_at = [&](auto EC, int mf, int sl) -> T& {
+    constexpr int E = decltype(EC)::value;
+    return fl[FLO[E] + mf * SLN[E] + sl];
   };
 
   // flux through the face normal to E in +e_E between the lower cell (L1
-  // trace of cm) and the upper cell (L0 trace of cp); a missing side takes
+  // trace of the box copy cm) and the upper cell (L0 trace of the box copy
+  // cp); a missing side takes
   // the other side's trace (domain boundary: own trace).  Tangential
   // operator rows at local coordinates lc, g_EE at the face = fe.
   auto face_flux_sep = [&](auto EC, const T* cm, const T* cp, bool has_m, bool has_p, const int* lc,
                            T fe, T* F) {
     constexpr int E = decltype(EC)::value;
     constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-    T Tm[NF], Tp[NF], S[NF], D[NF];
-    if (has_m) face_trace<DIM, N1, E, T>(cm, tb.L1, Tm);
-    if (has_p) face_trace<DIM, N1, E, T>(cp, tb.L0, Tp);
+    // traces straight from the box copies (Q layout), or through the
+    // P-space expansion
+    auto trace = [&](const T* src, const T* Ls, T* tr) {
+      if constexpr (PB) {
+        T cq[NM];
+        load_cell<DIM, P, PB, T>(src, cq);
+        face_trace<DIM, N1, E, T>(cq, Ls, tr);
+      } else {
+        face_trace<DIM, N1, E, T>(src, Ls, tr);
+      }
+    };
+    T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
+    if (has_m) trace(cm, tb.L1, S);
+    if (has_p) trace(cp, tb.L0, D);
 #pragma unroll
     for (int mf = 0; mf < NF; ++mf) {
-      if (!has_m) Tm[mf] = Tp[mf];
-      if (!has_p) Tp[mf] = Tm[mf];
-      S[mf] = T(0.5) * (Tm[mf] + Tp[mf]);
-      D[mf] = T(0.5) * (Tm[mf] - Tp[mf]);
+      const T tm = has_m ? S[mf] : D[mf], tp = has_p ? D[mf] : S[mf];
+      S[mf] = T(0.5) * (tm + tp);
+      D[mf] = T(0.5) * (tm - tp);
     }
     const T s1 = ct * fe;
     face_apply<DIM, N1, BOFF, T>(rowp(E, t0, lc[t0]), DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr, S, D, s1,
@@ -314,17 +400,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   for (int q = 0; q < NM; ++q) R[q] = T(0);
 
   if (work) {
-    T c[NM];
+    const T* cme = cellp(l[0], l[1], l[2]);
+    {
+      T c[NM];
+      load_cell<DIM, P, PB, T>(cme, c);
+      // ============================ cell term ============================
 #pragma unroll
-    for (int q = 0; q < NM; ++q) c[q] = box[(size_t)me * NM + q];
-    // ============================ cell term ============================
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      T M0[N1][N1], M1[N1][N1], M2[N1][N1];
-      load_op<N1, T>(rowp(d, 0, l[0]), M0);
-      load_op<N1, T>(rowp(d, 1, l[1]), M1);
-      if constexpr (DIM > 2) load_op<N1, T>(rowp(d, 2, l[2]), M2);
-      apply_sep_acc<DIM, N1, T>(M0, M1, M2, c, R, ct * ih[d]);
+      for (int d = 0; d < DIM; ++d) {
+        T M0[N1][N1], M1[N1][N1], M2[N1][N1];
+        load_op<N1, T>(rowp(d, 0, l[0]), M0);
+        load_op<N1, T>(rowp(d, 1, l[1]), M1);
+        if constexpr (DIM > 2) load_op<N1, T>(rowp(d, 2, l[2]), M2);
+        apply_sep_acc<DIM, N1, T>(M0, M1, M2, c, R, ct * ih[d]);
+      }
     }
     // ===== upper faces: own flux, shared with the upper neighbour via slot l[E] + 1
     auto do_upper = [&](auto EC) {
@@ -332,13 +420,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
       int nl[3] = {l[0], l[1], l[2]};
       nl[E] += 1;
       const bool has_nb = g[E] + 1 < m.n[E];
-      const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
+      const T* cn = cellp(nl[0], nl[1], nl[2]);
       T F[NF];
-      face_flux_sep(EC, c, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F);
+      face_flux_sep(EC, cme, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F);
       scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
-      const int sl = slot(E, nl);
+      const int sl = slot(EC, nl);
 #pragma unroll
-      for (int mf = 0; mf < NF; ++mf) flux_at(E, mf, sl) = F[mf];
+      for (int mf = 0; mf < NF; ++mf) flux_at(EC, mf, sl) = F[mf];
     };
     do_upper(std::integral_constant<int, 0>());
     do_upper(std::integral_constant<int, 1>());
@@ -346,38 +434,35 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   }
 
   // ===== the tile's lower boundary faces (slot 0 of every line), as work
-  // items: axis E's items start at a warp boundary so that a warp serves
+  // items; axis E's items start at a warp boundary so that a warp serves
   // one axis
   if (active) {
-    int nitem[3], ibase[3], tot = 0;
-    for (int E = 0; E < DIM; ++E) {
-      nitem[E] = nt / tl[E];
-      ibase[E] = tot;
-      tot += (nitem[E] + 31) & ~31;
-    }
-    for (int it = threadIdx.x; it < tot; it += blockDim.x) {
+    constexpr int NI0 = NT / TX, NI1 = NT / TY, NI2 = DIM > 2 ? NT / TZ : 0;
+    constexpr int IB1 = (NI0 + 31) & ~31, IB2 = IB1 + ((NI1 + 31) & ~31);
+    constexpr int TOT = IB2 + ((NI2 + 31) & ~31);
+    constexpr int NIT[3] = {NI0, NI1, NI2}, IBS[3] = {0, IB1, IB2};
+    for (int it = threadIdx.x; it < TOT; it += NT) {
       auto do_item = [&](auto EC) {
         constexpr int E = decltype(EC)::value;
-        const int k = it - ibase[E];
-        if (k < 0 || k >= nitem[E]) return;
+        const int k = it - IBS[E];
+        if (k < 0 || k >= NIT[E]) return;
         // tile cell with local coordinate 0 along E; the others from k
         constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
         int lc[3] = {0, 0, 0};
-        lc[t0] = k % tl[t0];
-        if (DIM > 2) lc[t1] = k / tl[t0];
-        const int gc[3] = {(E == 0 ? 0 : lc[0]) + tc.ox, (E == 1 ? 0 : lc[1]) + tc.oy,
-                           DIM > 2 ? (E == 2 ? 0 : lc[2]) + tc.oz : 0};
+        lc[t0] = k % TL[t0];
+        if (DIM > 2) lc[t1] = k / TL[t0];
+        const int gc[3] = {ox + lc[0], oy + lc[1], oz + lc[2]};
         if (gc[0] >= m.n[0] || gc[1] >= m.n[1] || (DIM > 2 && gc[2] >= m.n[2])) return;
         int ll[3] = {lc[0], lc[1], lc[2]};
         ll[E] -= 1;
         const bool has_m = gc[E] > 0;
-        const T* cp = box + (size_t)box_index(m, DIM, lc[0], lc[1], lc[2]) * NM;
-        const T* cm = box + (size_t)box_index(m, DIM, ll[0], ll[1], ll[2]) * NM;
+        const T* cp = cellp(lc[0], lc[1], lc[2]);
+        const T* cm = cellp(ll[0], ll[1], ll[2]);
         T F[NF];
         face_flux_sep(EC, cm, cp, has_m, true, lc, rowp(E, E, 0)[BOFF], F);
-        const int sl = slot(E, lc);
+        const int sl = slot(EC, lc);
 #pragma unroll
-        for (int mf = 0; mf < NF; ++mf) flux_at(E, mf, sl) = F[mf];
+        for (int mf = 0; mf < NF; ++mf) flux_at(EC, mf, sl) = F[mf];
       };
       do_item(std::integral_constant<int, 0>());
       do_item(std::integral_constant<int, 1>());
@@ -389,10 +474,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   if (work) {
     auto do_lower = [&](auto EC) {
       constexpr int E = decltype(EC)::value;
-      const int sl = slot(E, l);
+      const int sl = slot(EC, l);
       T F[NF];
 #pragma unroll
-      for (int mf = 0; mf < NF; ++mf) F[mf] = flux_at(E, mf, sl);
+      for (int mf = 0; mf < NF; ++mf) F[mf] = flux_at(EC, mf, sl);
       scatter_face<DIM, P, E, T>(R, tb.L0, F, ih[E]);
     };
     do_lower(std::integral_constant<int, 0>());
@@ -408,38 +493,66 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) adv_sep_kernel(co
   __syncthreads();
 
   // ---- RK combination fused into the coalesced store: one warp per row of
-  // cells along x; stage input from the box, phi^n straight from HBM
+  // cells along x; stage input from the box, phi^n from HBM, all of a
+  // lane's phi^n loads issued before the first use
   const bool need_n = a.combine == kRK2b || a.combine == kRK3b || a.combine == kRK3c;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const bool dense = m.nb == NM;
-  for (int r = warp; r < ty * tz; r += nw) {
-    const int ly = r % ty, lz = r / ty;
-    const int gy = tc.oy + ly, gz = tc.oz + lz;
-    const int nx = min(tx, m.n[0] - tc.ox);
-    if (gy >= m.n[1] || gz >= m.n[2] || nx <= 0) continue;
-    const long long gbase = ((long long)m.n[0] * (gy + (long long)m.n[1] * gz) + tc.ox) * m.nb;
-    const T* cs = box + (size_t)box_index(m, DIM, 0, ly, lz) * NM;
-    const T* rs = rbuf + (size_t)tx * r * NM;
-    if (dense) {
-#pragma unroll 4
-      for (int e = lane; e < nx * NM; e += 32) {
+  constexpr int NW = NT / 32, NROW = TY * TZ, ROWE = TX * NBG;
+  constexpr int RPW = (NROW + NW - 1) / NW, KPR = (ROWE + 31) / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = min(TX, m.n[0] - ox);
+  if constexpr (!PB) {
+    // rows in chunks of CH, a chunk's phi^n loads all in flight together
+    constexpr int CH = RPW * KPR > 16 ? (RPW > 2 ? 2 : RPW) : RPW;
+#pragma unroll
+    for (int j0 = 0; j0 < RPW; j0 += CH) {
+      T pn[CH][KPR];
+#pragma unroll
+      for (int jj = 0; jj < CH; ++jj) {
+        const int r = warp + NW * (j0 + jj);
+        const int ly = r % TY, lz = r / TY;
+        const bool rok = j0 + jj < RPW && r < NROW && oy + ly < m.n[1] && (DIM < 3 || oz + lz < m.n[2]);
+        const long long gbase =
+            ((long long)m.n[0] * ((oy + ly) + (long long)m.n[1] * (DIM > 2 ? oz + lz : 0)) + ox) * NM;
+#pragma unroll
+        for (int k = 0; k < KPR; ++k) {
+          const int e = lane + 32 * k;
+          pn[jj][k] = (need_n && active && rok && e < nx * NM) ? __ldg(a.phi_n + gbase + e) : T(0);
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < CH; ++jj) {
+        const int r = warp + NW * (j0 + jj);
+        const int ly = r % TY, lz = r / TY;
+        if (!(j0 + jj < RPW && r < NROW && oy + ly < m.n[1] && (DIM < 3 || oz + lz < m.n[2]))) continue;
+        const long long gbase =
+            ((long long)m.n[0] * ((oy + ly) + (long long)m.n[1] * (DIM > 2 ? oz + lz : 0)) + ox) * NM;
+        const T* cs = cellp(0, ly, lz);
+        const T* rs = rbuf + (size_t)TX * r * NM;
+#pragma unroll
+        for (int k = 0; k < KPR; ++k) {
+          const int e = lane + 32 * k;
+          if (e >= nx * NM) continue;
+          const T cv = cs[e];
+          a.out[gbase + e] = active ? combine_value<T>(a.combine, cv, pn[jj][k], rs[e], dt) : cv;
+        }
+      }
+    }
+  } else {
+    for (int r = warp; r < NROW; r += NW) {
+      const int ly = r % TY, lz = r / TY;
+      const int gy = oy + ly, gz = oz + lz;
+      if (gy >= m.n[1] || (DIM > 2 && gz >= m.n[2]) || nx <= 0) continue;
+      const long long gbase = ((long long)m.n[0] * (gy + (long long)m.n[1] * (DIM > 2 ? gz : 0)) + ox) * NBG;
+      const T* cs = cellp(0, ly, lz);
+      const T* rs = rbuf + (size_t)TX * r * NM;
+      for (int e = lane; e < nx * NBG; e += 32) {
+        const int cx = e / NBG, kk = e - cx * NBG;
+        const int q = cx * NM + m.g2q[kk];
         const T cv = cs[e];
         T res = cv;
         if (active) {
-          const T pn = need_n ? __ldg(a.phi_n + gbase + e) : T(0);
-          res = combine_value<T>(a.combine, cv, pn, rs[e], dt);
-        }
-        a.out[gbase + e] = res;
-      }
-    } else {
-      for (int e = lane; e < nx * m.nb; e += 32) {
-        const int cx = e / m.nb, k = e - cx * m.nb;
-        const int q = cx * NM + m.g2q[k];
-        const T cv = cs[q];
-        T res = cv;
-        if (active) {
-          const T pn = need_n ? __ldg(a.phi_n + gbase + e) : T(0);
-          res = combine_value<T>(a.combine, cv, pn, rs[q], dt);
+          const T pnv = need_n ? __ldg(a.phi_n + gbase + e) : T(0);
+          res = combine_value<T>(a.combine, cv, pnv, rs[q], dt);
         }
         a.out[gbase + e] = res;
       }

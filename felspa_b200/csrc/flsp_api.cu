@@ -89,6 +89,8 @@ int upload_tables(int dev) {
   ST(upload_tables_adv());
   ST(upload_tables_hj());
   ST(upload_tables_misc());
+  ST(upload_tables_sep2());
+  ST(upload_tables_sep3());
   if (dev >= 0 && dev < 64) g_tables_ready[dev] = true;
   return FLSP_OK;
 }
@@ -118,6 +120,7 @@ struct flsp_handle {
   void* vtab = nullptr;
   double* vtab64 = nullptr;
   void* optab = nullptr;          // separable-operator rows (sep1 velocities)
+  int opstride = 0;               // rows per (component, axis) in optab
   bool has_vel = false;
   flsp_velocity_desc vel;
   int nmax = 1, npt = 1;
@@ -159,6 +162,8 @@ struct flsp_handle {
     v.sep1 = vel_dev.n_terms == dim;
     for (int k = 0; k < vel_dev.n_terms; ++k) v.sep1 = v.sep1 && vel_dev.terms[k].comp == k;
     v.optab = v.sep1 ? optab : nullptr;
+    v.opstride = opstride;
+    v.err = clk ? &clk->err : nullptr;
     return v;
   }
 };
@@ -180,10 +185,16 @@ int ensure_partial(flsp_handle* h, int n) {
   return FLSP_OK;
 }
 
+int device_error(int err) {
+  if (err & kErrCopyTimeout)
+    return fail(FLSP_ERR_TIMEOUT, "a kernel's wait for its bulk copies ran out (results invalid)");
+  return FLSP_OK;
+}
+
 int sync_clock(flsp_handle* h) {
   CU(cudaMemcpyAsync(h->clk_host, h->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
-  return FLSP_OK;
+  return device_error(h->clk_host->err);
 }
 
 // kernel configuration of this handle (tiles, shared-memory attributes);
@@ -400,7 +411,9 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
   if (!vd.sep1) return FLSP_OK;
   const int n1 = h->p + 1, nq = h->p + 2, nn = n1 * n1;
   const int boff = ((nn + 3) / 4) * 4, opw = 2 * boff;
-  const size_t nrow = (size_t)h->dim * 3 * h->nmax;
+  // a tile copies its rows in one piece: pad each (d, e) block past the mesh
+  const int stride = h->nmax + kOpRowPad;
+  const size_t nrow = (size_t)h->dim * 3 * stride;
   std::vector<double> op(nrow * opw, 0.0);
   double x[8], w[8], lv[8][8], ld[8][8];
   gauss_rule(nq, x, w);
@@ -413,7 +426,7 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
       for (int i = 0; i < h->m.n[e]; ++i) {
         const size_t r = ((size_t)d * 3 + e) * h->nmax + i;
         const double* gq = &tabd[r * h->npt];   // term d == component d
-        double* row = &op[r * opw];
+        double* row = &op[(((size_t)d * 3 + e) * stride + i) * opw];
         for (int al = 0; al < n1; ++al)
           for (int be = 0; be < n1; ++be) {
             long double sa = 0.0L, sb = 0.0L;
@@ -440,6 +453,7 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
     CU(cudaMalloc(&h->optab, n * sizeof(float)));
     CU(cudaMemcpy(h->optab, of.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   }
+  h->opstride = stride;
   return FLSP_OK;
 }
 
@@ -601,7 +615,8 @@ int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts, flsp_handl
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup_fail(fail(FLSP_ERR_CUDA, "stream creation failed"));
   for (int i = 0; i < 3; ++i)
-    if (cudaMalloc(&h->buf[i], h->ndofs * h->tsize) != cudaSuccess)
+    // padded: the stage kernel's bulk row copies round their ends up to 16 bytes
+    if (cudaMalloc(&h->buf[i], h->ndofs * h->tsize + kStatePad) != cudaSuccess)
       return cleanup_fail(fail(FLSP_ERR_OOM, "state allocation failed"));
   if (cudaMalloc(&h->clk, sizeof(DevClock)) != cudaSuccess ||
       cudaMallocHost(&h->clk_host, sizeof(DevClock)) != cudaSuccess ||
@@ -944,8 +959,7 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
 int flsp_sync(flsp_handle* h) {
   if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
   CU(cudaSetDevice(h->dev));
-  CU(cudaStreamSynchronize(h->stream));
-  return FLSP_OK;
+  return sync_clock(h);
 }
 
 int flsp_stream(const flsp_handle* h, void** stream) {

@@ -341,4 +341,49 @@ __device__ __forceinline__ void store_tile(const MeshArgs& m, const T* __restric
   }
 }
 
+// ---------------------------------------------------------------------
+// Bulk asynchronous copies (TMA engine, cp.async.bulk) completing on a
+// shared-memory mbarrier.  Copies are plain global -> own-CTA shared
+// memory: no cluster multicast.  Both addresses 16-byte aligned, size a
+// multiple of 16.
+// ---------------------------------------------------------------------
+constexpr int kErrCopyTimeout = 1;   // DevClock::err bit: a bulk-copy wait ran out
+constexpr int kOpRowPad = 32;        // operator-table rows past the mesh per (d, e) block
+constexpr int kStatePad = 256;       // bytes past the end of every state buffer
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// one arrival that also announces the bytes the phase waits for
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Wait for phase `parity` of the barrier, at most max_iter polls (each
+// try_wait may itself suspend for a while); false when it ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int max_iter) {
+  const unsigned a = smem_u32(bar);
+  for (int it = 0; it < max_iter; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 }  // namespace flsp

@@ -3,7 +3,6 @@
 #include <cstring>
 
 #include "flsp_advect.cuh"
-#include "flsp_advsep.cuh"
 #include "flsp_launch.h"
 #include "flsp_tables.h"
 
@@ -15,53 +14,75 @@ int upload_tables_adv() {
   return FLSP_OK;
 }
 
-// shared memory of the stage kernel that serves velocity v
-template <int DIM, int P, typename T>
-static size_t stage_smem(const VelDev& v, const int* tile) {
-  return use_sep_kernel(v) ? sep_smem_bytes<DIM, P, T>(tile)
-                           : adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1));
+static int sep_unit(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* bytes,
+                    const void* in = nullptr, const void* phin = nullptr, void* out = nullptr,
+                    const DevClock* clk = nullptr, int stage = 0, int combine = 0, double ct = 0.0) {
+  if (c.dim == 2) return sep2_call(what, c, v, tile, bytes, in, phin, out, clk, stage, combine, ct);
+  return sep3_call(what, c, v, tile, bytes, in, phin, out, clk, stage, combine, ct);
 }
 
 int adv_default_tile(const Ctx& c, const VelDev& v, int* tile) {
+  static const int c2[][3] = {{32, 8, 1}, {16, 16, 1}, {16, 8, 1}, {8, 8, 1}};
+  static const int c3[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}};
+  const int(*cand)[3] = c.dim == 2 ? c2 : c3;
+  const int ncand = c.dim == 2 ? 4 : 3;   // 4x4x2 only for the quadrature kernel
+  if (use_sep_kernel(v)) {
+    // separable kernel: the first shape with two CTAs per SM, else the
+    // first that fits
+    int pick = -1;
+    for (int pass = 0; pass < 2 && pick < 0; ++pass)
+      for (int i = 0; i < ncand && pick < 0; ++i) {
+        size_t b = 0;
+        const int st = sep_unit(0, c, &v, cand[i], &b);
+        if (st) return st;
+        if (b <= (pass == 0 ? 113u * 1024u : 227u * 1024u)) pick = i;
+      }
+    if (pick < 0) return set_error(FLSP_ERR_UNSUPPORTED, "no separable tile fits in shared memory");
+    for (int d = 0; d < 3; ++d) tile[d] = cand[pick][d];
+    return FLSP_OK;
+  }
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
-    static const int c2[][3] = {{32, 8, 1}, {16, 16, 1}, {16, 8, 1}, {8, 8, 1}};
-    static const int c3[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}};
-    const int(*cand)[3] = DIM == 2 ? c2 : c3;
+    const int(*cq)[3] = DIM == 2 ? c2 : c3;
     int i = 0;
     for (; i < 3; ++i)
-      if (stage_smem<DIM, P, T>(v, cand[i]) <= 200 * 1024) break;
-    tile[0] = cand[i][0];
-    tile[1] = cand[i][1];
-    tile[2] = cand[i][2];
+      if (adv_smem_bytes<DIM, P, T>(cq[i], std::max(v.n_terms, 1)) <= 200 * 1024) break;
+    tile[0] = cq[i][0];
+    tile[1] = cq[i][1];
+    tile[2] = cq[i][2];
     return FLSP_OK;
   });
 }
 
 int adv_prepare(const Ctx& c, const VelDev& v, const int* tile) {
+  if (use_sep_kernel(v)) return sep_unit(1, c, &v, tile, nullptr);
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
-    const size_t smem = std::max(adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1)),
-                                 sep_smem_bytes<DIM, P, T>(tile));
+    const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1));
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "advection tile too large for shared memory");
-    auto attr = [&](auto kern) -> int {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-      if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("adv attr: ") + cudaGetErrorString(e));
-      return FLSP_OK;
-    };
-    int st = attr(adv_stage_kernel<DIM, P, T>);
-    if (st == FLSP_OK) st = attr(adv_sep_kernel<DIM, P, T>);
-    return st;
+    cudaError_t e = cudaFuncSetAttribute(adv_stage_kernel<DIM, P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(adv_stage_kernel<DIM, P, T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("adv attr: ") + cudaGetErrorString(e));
+    return FLSP_OK;
   });
 }
 
 int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* phin, void* out,
                      const DevClock* clk, int stage, int combine, double ct_explicit,
                      const int* tile) {
+  if (use_sep_kernel(v)) {
+    int t[3];
+    if (tile) { t[0] = tile[0]; t[1] = tile[1]; t[2] = tile[2]; }
+    else {
+      const int st = adv_default_tile(c, v, t);
+      if (st) return st;
+    }
+    return sep_unit(2, c, &v, t, nullptr, in, phin, out, clk, stage, combine, ct_explicit);
+  }
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
@@ -72,23 +93,6 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     if (tile) { t[0] = tile[0]; t[1] = tile[1]; t[2] = tile[2]; }
     else adv_default_tile(c, v, t);
     set_tile(a.m, DIM, t);
-    if (use_sep_kernel(v)) {
-      AdvSepArgs<T> b;
-      std::memset(&b, 0, sizeof(b));
-      b.m = a.m;
-      b.optab = reinterpret_cast<const T*>(v.optab);
-      b.nmax = v.nmax;
-      b.phi_s = reinterpret_cast<const T*>(in);
-      b.phi_n = reinterpret_cast<const T*>(phin);
-      b.out = reinterpret_cast<T*>(out);
-      b.clk = clk;
-      b.stage = stage;
-      b.combine = combine;
-      b.ct_explicit = ct_explicit;
-      const size_t smem = sep_smem_bytes<DIM, P, T>(a.m.tile);
-      adv_sep_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(b);
-      return launch_status("adv_sep_kernel");
-    }
     a.v.vtab = reinterpret_cast<const T*>(v.vtab);
     a.v.n_terms = v.n_terms;
     a.v.nmax = v.nmax;

@@ -1,0 +1,18 @@
+// flsp_k_sep3.cu — separable stage kernel, 3D instances.
+#include "flsp_k_sep.cuh"
+#include "flsp_tables.h"
+
+namespace flsp {
+
+int upload_tables_sep3() {
+  cudaError_t e = upload_tables_here();
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
+  return FLSP_OK;
+}
+
+int sep3_call(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* bytes, const void* in,
+              const void* phin, void* out, const DevClock* clk, int stage, int combine, double ct_explicit) {
+  return sep_call<3>(what, c, v, tile, bytes, in, phin, out, clk, stage, combine, ct_explicit);
+}
+
+}  // namespace flsp

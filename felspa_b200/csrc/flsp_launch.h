@@ -60,6 +60,10 @@ inline int launch_status(const char* what) {
 int upload_tables_adv();
 int upload_tables_hj();
 int upload_tables_misc();
+int upload_tables_sep2();
+int upload_tables_sep3();
+
+
 
 // ---------------- advection (flsp_k_adv.cu) ----------------
 struct VelDev {
@@ -68,9 +72,17 @@ struct VelDev {
   int comp[kMaxTerms];
   bool sep1;           // term k is the only term of component k
   const void* optab;   // per-axis operator rows of a sep1 velocity (T precision), or null
+  int opstride;        // operator rows per (component, axis) in optab
+  int* err;            // device error word (DevClock::err)
 };
 // stage kernel of this velocity: separable-operator kernel when optab is set
 inline bool use_sep_kernel(const VelDev& v) { return v.sep1 && v.optab != nullptr; }
+// separable stage kernel units: what = 0 shared-memory bytes of the tile,
+// 1 kernel attributes, 2 launch (flsp_k_sep.cuh)
+int sep2_call(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* bytes, const void* in,
+              const void* phin, void* out, const DevClock* clk, int stage, int combine, double ct_explicit);
+int sep3_call(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* bytes, const void* in,
+              const void* phin, void* out, const DevClock* clk, int stage, int combine, double ct_explicit);
 // tile: cells per CTA (nullptr = default); smem attribute is set on first use
 int adv_default_tile(const Ctx& c, const VelDev& v, int* tile);
 int adv_prepare(const Ctx& c, const VelDev& v, const int* tile);
