@@ -109,6 +109,37 @@ class ReinitOpts(C.Structure):
     ]
 
 
+class TrainOpts(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("batch", C.c_int),
+        ("lr", C.c_double),
+        ("beta1", C.c_double),
+        ("beta2", C.c_double),
+        ("eps", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
+class LearnedOpts(C.Structure):
+    _fields_ = [
+        ("band_cells", C.c_double),
+        ("max_residual", C.c_double),
+        ("fallback", ReinitOpts),
+    ]
+
+
+class LearnedStats(C.Structure):
+    _fields_ = [
+        ("n_band", C.c_int64),
+        ("n_fallback", C.c_int64),
+        ("hj_ran", C.c_int),
+    ]
+
+
+MLP_IN, MLP_HIDDEN, MLP_OUT = 82, 256, 9
+
+
 class LSOpts(C.Structure):
     _fields_ = [
         ("reinit_frequency", C.c_int),

@@ -17,6 +17,7 @@
 
 #include "flsp_dg.h"
 #include "flsp_launch.h"
+#include "flsp_mlp.h"
 #include "flsp_tables.h"
 
 using namespace flsp;
@@ -138,6 +139,15 @@ struct flsp_handle {
   void* rdiff = nullptr;    // LDG diffusion RHS
   int adv_tile[3] = {0, 0, 0};
   int hj_tile[3] = {0, 0, 0};
+  // learned reinitialisation scratch (allocated on first use)
+  int* lrn_flags = nullptr;   // ncell band flags, then per-band-cell fallback flags
+  int* lrn_work = nullptr;    // block counts / offsets of the band compaction
+  int* lrn_cells = nullptr;   // band cells (ncell)
+  int* lrn_count = nullptr;   // [0] band cells, [1] fallback cells
+  int* lrn_count_host = nullptr;   // pinned mirror
+  void* lrn_save = nullptr;   // one state vector
+  float* lrn_feat = nullptr;  // band patch features
+  int64_t lrn_feat_cap = 0;
   std::map<unsigned long long, GraphEntry> graphs;
 
   Ctx ctx() const {
@@ -509,6 +519,47 @@ int build_vtab(flsp_handle* h) {
   return FLSP_OK;
 }
 
+// ---- learned reinitialisation helpers
+int learned_check(const flsp_handle* h, const flsp_mlp* net) {
+  if (h->dim != 2 || h->p != 2 || h->basis != FLSP_BASIS_Q)
+    return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: 2D, degree 2, Q basis only");
+  if (std::fabs(h->m.h[0] - h->m.h[1]) > 1e-12 * h->m.h[0])
+    return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: square cells only");
+  if (net && net->dev != h->dev) return fail(FLSP_ERR_BAD_ARG, "network and problem on different devices");
+  return FLSP_OK;
+}
+
+int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
+  const int64_t ncell = h->m.ncell;
+  if (!h->lrn_flags) {
+    const int64_t nblk = (ncell + 255) / 256;
+    CU(cudaMalloc(&h->lrn_flags, (size_t)ncell * sizeof(int)));
+    CU(cudaMalloc(&h->lrn_work, (size_t)(2 * nblk + 2) * sizeof(int)));
+    CU(cudaMalloc(&h->lrn_cells, (size_t)ncell * sizeof(int)));
+    CU(cudaMalloc(&h->lrn_count, 2 * sizeof(int)));
+    CU(cudaMallocHost(&h->lrn_count_host, 2 * sizeof(int)));
+    CU(cudaMalloc(&h->lrn_save, (size_t)h->ndofs * h->tsize + kStatePad));
+  }
+  if (h->lrn_feat_cap < nfeat) {
+    if (h->lrn_feat) cudaFree(h->lrn_feat);
+    h->lrn_feat = nullptr;
+    CU(cudaMalloc(&h->lrn_feat, (size_t)nfeat * FLSP_MLP_IN * sizeof(float)));
+    h->lrn_feat_cap = nfeat;
+  }
+  return FLSP_OK;
+}
+
+// band cells of the current state: |mean phi| <= band_cells * h; returns the count
+int select_band(flsp_handle* h, double band_cells, int64_t* n) {
+  ST(ensure_learned_buffers(h, 0));
+  ST(launch_band_select(h->stream, h->prec, h->buf[h->cur], h->m.ncell, band_cells * h->m.h[0], h->lrn_flags,
+                        h->lrn_work, h->lrn_cells, h->lrn_count));
+  CU(cudaMemcpyAsync(h->lrn_count_host, h->lrn_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  *n = h->lrn_count_host[0];
+  return FLSP_OK;
+}
+
 }  // namespace
 
 // ==================================================================
@@ -661,6 +712,10 @@ void flsp_destroy(flsp_handle* h) {
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
   if (h->optab) cudaFree(h->optab);
+  void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_save, h->lrn_feat};
+  for (void* q : lrn)
+    if (q) cudaFree(q);
+  if (h->lrn_count_host) cudaFreeHost(h->lrn_count_host);
   if (h->clk) cudaFree(h->clk);
   if (h->clk_host) cudaFreeHost(h->clk_host);
   if (h->perm) cudaFree(h->perm);
@@ -1040,6 +1095,103 @@ int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic, double* out) 
     case FLSP_RED_L2_ERROR_IC: *out = std::sqrt(r[0]); break;
     default: *out = r[0];
   }
+  return FLSP_OK;
+}
+
+// ---- learned reinitialisation (no counterpart in the reference)
+int flsp_mlp_collect(flsp_mlp* net, flsp_handle* h, double band_cells, const flsp_reinit_opts* target,
+                     int64_t* n_added) {
+  if (!net || !h || !target) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (!(band_cells > 0.0)) return fail(FLSP_ERR_BAD_ARG, "band_cells must be positive");
+  CU(cudaSetDevice(h->dev));
+  ST(learned_check(h, net));
+  ST(validate_reinit(h, target));
+  int64_t n = 0;
+  ST(select_band(h, band_cells, &n));
+  ST(mlp_ensure_pairs(net, net->n_pairs + n));
+  const double hh = h->m.h[0];
+  ST(launch_patch_features(h->stream, h->prec, h->buf[h->cur], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n,
+                           net->feat + net->n_pairs * FLSP_MLP_IN));
+  CU(cudaMemcpyAsync(h->lrn_save, h->buf[h->cur], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  int nit = 0;
+  ST(run_reinit(h, target, &nit));
+  ST(launch_patch_targets(h->stream, h->prec, h->lrn_save, h->buf[h->cur], hh, h->lrn_cells, n,
+                          net->targ + net->n_pairs * FLSP_MLP_OUT));
+  CU(cudaStreamSynchronize(h->stream));
+  net->n_pairs += n;
+  if (n_added) *n_added = n;
+  return FLSP_OK;
+}
+
+void flsp_default_learned_opts(flsp_learned_opts* o) {
+  if (!o) return;
+  o->band_cells = 6.0;
+  o->max_residual = 0.05;
+  fill_reinit_defaults(&o->fallback);
+  o->fallback.mode = FLSP_REINIT_FIXED;
+  o->fallback.n_pseudo_steps = 20;
+}
+
+int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o, flsp_learned_stats* stats) {
+  if (!h || !net || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (!(o->band_cells > 0.0) || !(o->max_residual > 0.0)) return fail(FLSP_ERR_BAD_ARG, "bad learned options");
+  CU(cudaSetDevice(h->dev));
+  ST(learned_check(h, net));
+  ST(validate_reinit(h, &o->fallback));
+  int64_t n = 0;
+  ST(select_band(h, o->band_cells, &n));
+  const double hh = h->m.h[0];
+  const int pre = h->cur;
+  const int out = other(pre, -1);
+  flsp_learned_stats stl = {n, 0, 0};
+  if (n > 0) {
+    ST(ensure_learned_buffers(h, n));
+    ST(mlp_ensure_cap(net, n));
+    ST(launch_patch_features(h->stream, h->prec, h->buf[pre], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n,
+                             h->lrn_feat));
+    // the network runs on its own stream: order it after the features
+    cudaEvent_t ev;
+    CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaEventRecord(ev, h->stream);
+    cudaStreamWaitEvent(net->stream, ev, 0);
+    int st = mlp_pack_input(net, h->lrn_feat, nullptr, n);
+    if (st == FLSP_OK) st = mlp_forward_dev(net, n, false);
+    cudaEventRecord(ev, net->stream);
+    cudaStreamWaitEvent(h->stream, ev, 0);
+    cudaEventDestroy(ev);
+    ST(st);
+    ST(launch_apply_delta(h->stream, h->prec, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, n, net->y, 16));
+    // band cells whose result is not distance-like enough take the HJ sweep
+    ST(launch_residual_flags(h->stream, h->prec, h->buf[out], h->m.n[0], hh, h->lrn_cells, n, o->max_residual,
+                             h->lrn_flags, h->lrn_count + 1));
+    CU(cudaMemcpyAsync(h->lrn_count_host + 1, h->lrn_count + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    int e = 0;
+    CU(cudaMemcpy(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(FLSP_ERR_TIMEOUT, "a tensor-core kernel's pipeline wait ran out");
+    stl.n_fallback = h->lrn_count_host[1];
+  } else {
+    CU(cudaMemcpyAsync(h->buf[out], h->buf[pre], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  if (stl.n_fallback > 0) {
+    // keep the network's result, run the sweep from the pre-reinit state,
+    // then put the network's result back everywhere but the flagged cells
+    CU(cudaMemcpyAsync(h->lrn_save, h->buf[out], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+    h->cur = pre;
+    int nit = 0;
+    ST(run_reinit(h, &o->fallback, &nit));
+    const int hj = h->cur;
+    const int res = other(hj, -1);
+    CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+    ST(launch_merge_cells(h->stream, h->prec, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, n));
+    h->cur = res;
+    stl.hj_ran = 1;
+  } else {
+    h->cur = out;
+  }
+  CU(cudaStreamSynchronize(h->stream));
+  h->n_since_reinit = 0;
+  if (stats) *stats = stl;
   return FLSP_OK;
 }
 

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libflsp_dg.so")
 _lib = None
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int)
 _i64p = C.POINTER(C.c_int64)
 _vp = C.c_void_p
@@ -52,6 +53,21 @@ PROTOTYPES = {
     "flsp_default_dg_opts": (None, [C.POINTER(abi.DGOpts)]),
     "flsp_default_reinit_opts": (None, [C.POINTER(abi.ReinitOpts)]),
     "flsp_default_ls_opts": (None, [C.POINTER(abi.LSOpts)]),
+    "flsp_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    "flsp_mlp_destroy": (None, [_vp]),
+    "flsp_mlp_n_params": (C.c_int, [_i64p]),
+    "flsp_mlp_get_params": (C.c_int, [_vp, _fp, C.c_int64]),
+    "flsp_mlp_set_params": (C.c_int, [_vp, _fp, C.c_int64]),
+    "flsp_mlp_forward": (C.c_int, [_vp, _fp, C.c_int64, _fp]),
+    "flsp_mlp_backward": (C.c_int, [_vp, _fp, _fp, C.c_int64, _fp]),
+    "flsp_mlp_collect": (C.c_int, [_vp, _vp, C.c_double, C.POINTER(abi.ReinitOpts), _i64p]),
+    "flsp_mlp_n_pairs": (C.c_int, [_vp, _i64p]),
+    "flsp_mlp_clear_pairs": (C.c_int, [_vp]),
+    "flsp_mlp_train": (C.c_int, [_vp, C.POINTER(abi.TrainOpts), _dp]),
+    "flsp_mlp_eval": (C.c_int, [_vp, _dp]),
+    "flsp_reinit_learned": (C.c_int, [_vp, _vp, C.POINTER(abi.LearnedOpts), C.POINTER(abi.LearnedStats)]),
+    "flsp_default_train_opts": (None, [C.POINTER(abi.TrainOpts)]),
+    "flsp_default_learned_opts": (None, [C.POINTER(abi.LearnedOpts)]),
 }
 
 
@@ -82,6 +98,10 @@ def check(code):
         msg = load().flsp_last_error()
         raise FlspError(code, msg.decode() if msg else "")
     return code
+
+
+def fp(a):
+    return a.ctypes.data_as(_fp)
 
 
 def dp(a):

@@ -309,6 +309,79 @@ int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis,
                         const flsp_ic_desc* ic, double* result,
                         void* stream);
 
+/* ------------------------------------------------------------------
+   Learned reinitialisation (no counterpart in the reference: its
+   ReinitSimulatorLDG, src/level_set/reinit.cc:386-637, only has the HJ
+   sweep, which stays here as the fallback and as the source of the
+   training targets).  2D, degree 2, Q basis.  Input of the network: the
+   3 x 3 patch of cells around a cell, 9 coefficients each, divided by the
+   cell size h, plus 64 h (82 values, cell rows y outer, x inner; cells
+   outside the domain repeat the nearest inside cell).  Output: the change
+   of the centre cell's 9 coefficients under the reinitialisation, divided
+   by h.  82 -> 256 -> 256 -> 256 -> 256 -> 9, GELU hidden layers, BF16
+   weights on the tensor cores, FP32 accumulation and master weights.
+   Parameters: W1 [256][82], b1[256], W2 [256][256], b2, W3, b3, W4, b4,
+   W5 [9][256], b5[9] (row-major W[out][in]).
+   ------------------------------------------------------------------ */
+#define FLSP_MLP_IN 82
+#define FLSP_MLP_HIDDEN 256
+#define FLSP_MLP_OUT 9
+
+typedef struct flsp_mlp flsp_mlp;
+
+typedef struct flsp_train_opts {
+  int64_t steps;           /* Adam steps                                  */
+  int batch;               /* pairs per step (default 8192)               */
+  double lr;               /* default 1e-3                                */
+  double beta1, beta2, eps;/* default 0.9, 0.999, 1e-8                    */
+  uint64_t seed;           /* batch sampling                              */
+} flsp_train_opts;
+
+typedef struct flsp_learned_opts {
+  double band_cells;       /* cells with |mean phi| <= band_cells * h are
+                              redistanced by the network (default 6)      */
+  double max_residual;     /* a cell whose mean ||grad phi| - 1| after the
+                              network exceeds this takes the HJ result
+                              (default 0.05)                              */
+  flsp_reinit_opts fallback;   /* the HJ sweep used for those cells     */
+} flsp_learned_opts;
+
+typedef struct flsp_learned_stats {
+  int64_t n_band;          /* cells the network redistanced               */
+  int64_t n_fallback;      /* of those, cells that took the HJ result     */
+  int hj_ran;              /* the fallback sweep ran                      */
+} flsp_learned_stats;
+
+int flsp_mlp_create(int device, uint64_t seed, flsp_mlp** out);
+void flsp_mlp_destroy(flsp_mlp* net);
+int flsp_mlp_n_params(int64_t* n);
+int flsp_mlp_get_params(flsp_mlp* net, float* params, int64_t n);
+int flsp_mlp_set_params(flsp_mlp* net, const float* params, int64_t n);
+/* y[batch][9] = net(x[batch][82]), host arrays */
+int flsp_mlp_forward(flsp_mlp* net, const float* x, int64_t batch, float* y);
+/* gradient of sum_b dy[b] . y[b] w.r.t. every parameter (summed over the
+   batch, parameter layout above), host arrays */
+int flsp_mlp_backward(flsp_mlp* net, const float* x, const float* dy, int64_t batch,
+                      float* grad);
+/* training pairs from a handle (2D, degree 2, Q basis, square cells): the
+   band cells' patches of the current state, then the handle is
+   reinitialised with `target` and the centre cells' changes are the
+   targets.  The handle is left reinitialised. */
+int flsp_mlp_collect(flsp_mlp* net, flsp_handle* h, double band_cells,
+                     const flsp_reinit_opts* target, int64_t* n_added);
+int flsp_mlp_n_pairs(const flsp_mlp* net, int64_t* n);
+int flsp_mlp_clear_pairs(flsp_mlp* net);
+/* Adam on the MSE of the collected pairs; *loss = mean loss of the last
+   steps (may be NULL) */
+int flsp_mlp_train(flsp_mlp* net, const flsp_train_opts* o, double* loss);
+/* mean squared error of the network on the collected pairs */
+int flsp_mlp_eval(flsp_mlp* net, double* loss);
+/* learned reinitialisation of the handle's state (replaces flsp_reinit) */
+int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o,
+                        flsp_learned_stats* stats);
+void flsp_default_train_opts(flsp_train_opts* o);
+void flsp_default_learned_opts(flsp_learned_opts* o);
+
 /* default option structs (reference defaults) */
 void flsp_default_dg_opts(flsp_dg_opts* o);
 void flsp_default_reinit_opts(flsp_reinit_opts* o);

@@ -1,0 +1,161 @@
+"""Learned reinitialisation on the GPU: the tensor-core MLP (BF16
+operands, FP32 accumulation) against the oracle's FP64 MLP, training on
+pairs produced by the HJ sweep, and the band / fallback logic of
+flsp_reinit_learned.
+
+Tolerances: the GPU rounds weights, inputs and every hidden activation to
+BF16 (8-bit mantissa); with the weights and inputs rounded the same way
+for the oracle, the remaining difference is the activations' rounding,
+bounded here by 2e-2 of the largest output and 3e-2 (relative Frobenius)
+for each parameter gradient.
+"""
+import numpy as np
+import pytest
+
+from felspa_b200 import abi, fields as F
+from felspa_b200.learned import MLP, WIDTHS, default_learned_opts, param_layout, split_params
+from felspa_b200.level_set import Mesh, Problem
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a):
+    torch = pytest.importorskip("torch")
+    return torch.tensor(np.asarray(a, dtype=np.float32)).to(torch.bfloat16).float().numpy().astype(np.float64)
+
+
+def random_params(rng):
+    p = []
+    for name, off, shape in param_layout():
+        if name.startswith("W"):
+            p.append(rng.uniform(-1.5, 1.5, size=shape) / np.sqrt(shape[1]))
+        else:
+            p.append(rng.uniform(-0.1, 0.1, size=shape))
+    return np.concatenate([a.ravel() for a in p]).astype(np.float32)
+
+
+def oracle_weights(p):
+    v = split_params(p.astype(np.float64))
+    Ws = [bf16(v[f"W{l}"]) for l in range(1, 6)]
+    bs = [v[f"b{l}"].copy() for l in range(1, 6)]
+    return Ws, bs
+
+
+@pytest.fixture(scope="module")
+def net():
+    n = MLP(device=0, seed=3)
+    yield n
+    n.close()
+
+
+def test_forward_matches_oracle(net, oracle):
+    rng = np.random.default_rng(11)
+    p = random_params(rng)
+    net.set_params(p)
+    x = rng.standard_normal((300, WIDTHS[0])).astype(np.float32)
+    y = net.forward(x)
+    Ws, bs = oracle_weights(p)
+    ref = oracle.mlp_forward(Ws, bs, bf16(x))
+    assert np.all(np.isfinite(y))
+    assert np.max(np.abs(y - ref)) <= 2e-2 * np.max(np.abs(ref))
+
+
+def test_backward_matches_oracle(net, oracle):
+    rng = np.random.default_rng(12)
+    p = random_params(rng)
+    net.set_params(p)
+    B = 384
+    x = rng.standard_normal((B, WIDTHS[0])).astype(np.float32)
+    dy = (rng.standard_normal((B, WIDTHS[-1])) / B).astype(np.float32)
+    g = net.backward(x, dy)
+    Ws, bs = oracle_weights(p)
+    dW, db = oracle.mlp_backward(Ws, bs, bf16(x), bf16(dy))
+    gv = split_params(g.astype(np.float64))
+    for l in range(5):
+        for got, ref in ((gv[f"W{l + 1}"], dW[l]), (gv[f"b{l + 1}"], db[l])):
+            err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+            assert err <= 3e-2, (l, err)
+
+
+def test_backward_two_calls_identical(net):
+    rng = np.random.default_rng(13)
+    net.set_params(random_params(rng))
+    x = rng.standard_normal((256, WIDTHS[0])).astype(np.float32)
+    dy = rng.standard_normal((256, WIDTHS[-1])).astype(np.float32)
+    assert np.array_equal(net.backward(x, dy), net.backward(x, dy))
+
+
+def make_problem(n=64, seed=0, precision=abi.FP32):
+    pb = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=precision, cfl_max=0.1)
+    pb.set_velocity(F.fourier_stream_2d(seed=1000 + seed))
+    pb.project(F.circles_union(1000 + seed))
+    return pb
+
+
+def advance(pb, n_steps):
+    from felspa_b200.lib import check, load
+    check(load().flsp_advance_steps(pb.h, int(n_steps), 1e30))
+
+
+def test_training_reduces_loss():
+    net = MLP(device=0, seed=5)
+    for s in range(6):
+        pb = make_problem(64, s)
+        for _ in range(3):
+            advance(pb, 20)
+            net.collect(pb, band_cells=6.0)
+        pb.close()
+    assert net.n_pairs > 2000
+    before = net.eval()
+    last = net.train(steps=300, batch=1024, lr=1e-3, seed=2)
+    after = net.eval()
+    assert np.isfinite(last) and np.isfinite(after)
+    assert after < 0.5 * before, (before, after)
+    net.close()
+
+
+def test_learned_band_and_forced_fallback():
+    net = MLP(device=0, seed=6)
+    pb = make_problem(48, 7, precision=abi.FP64)
+    advance(pb, 30)
+    pre = pb.get_state()
+    h = 1.0 / 48
+    band = np.abs(pre.reshape(-1, 9)[:, 0]) <= 6.0 * h
+    # every band cell fails a zero residual bound: the HJ sweep fills the band
+    st = net.reinit(pb, default_learned_opts(max_residual=1e-12))
+    assert st["n_band"] == int(band.sum()) and st["n_band"] > 0
+    assert st["n_fallback"] == st["n_band"] and st["hj_ran"]
+    got = pb.get_state().reshape(-1, 9)
+    pb.set_state(pre)
+    from felspa_b200.lib import check, load
+    import ctypes as C
+    o = abi.ReinitOpts()
+    load().flsp_default_reinit_opts(C.byref(o))
+    o.mode = abi.REINIT_FIXED
+    o.n_pseudo_steps = 20
+    nit = C.c_int(0)
+    check(load().flsp_reinit(pb.h, C.byref(o), C.byref(nit)))
+    hj = pb.get_state().reshape(-1, 9)
+    assert np.array_equal(got[band], hj[band])
+    assert np.array_equal(got[~band], pre.reshape(-1, 9)[~band])
+    pb.close()
+    net.close()
+
+
+def test_learned_reinit_after_training():
+    net = MLP(device=0, seed=8)
+    for s in range(4):
+        pb = make_problem(64, 20 + s)
+        for _ in range(3):
+            advance(pb, 20)
+            net.collect(pb, band_cells=6.0)
+        pb.close()
+    net.train(steps=400, batch=2048, lr=1e-3, seed=3)
+    pb = make_problem(64, 40)
+    advance(pb, 40)
+    st = net.reinit(pb, default_learned_opts())
+    out = pb.get_state()
+    assert np.all(np.isfinite(out))
+    assert st["n_band"] > 0 and 0 <= st["n_fallback"] <= st["n_band"]
+    pb.close()
+    net.close()
