@@ -148,6 +148,11 @@ struct flsp_handle {
   void* lrn_save = nullptr;   // one state vector
   float* lrn_feat = nullptr;  // band patch features
   int64_t lrn_feat_cap = 0;
+  // compute-restricted narrow band of the reinitialisation
+  int* nb_flags = nullptr;    // ncell band flags
+  int* nb_lists = nullptr;    // 3 tile lists of ncell entries (HJ, LDG, WENO)
+  int* nb_counts = nullptr;   // their device counts
+  bool nb_use[3] = {false, false, false};   // lists in force for the launches
   std::map<unsigned long long, GraphEntry> graphs;
 
   Ctx ctx() const {
@@ -157,7 +162,13 @@ struct flsp_handle {
     c.prec = prec;
     c.basis = basis;
     c.m = m;
+    c.m.tiles = nullptr;
+    c.m.n_tiles = nullptr;
     c.stream = stream;
+    for (int k = 0; k < 3; ++k) {
+      c.nb_tiles[k] = nb_use[k] ? nb_lists + (size_t)k * m.ncell : nullptr;
+      c.nb_count[k] = nb_use[k] ? nb_counts + k : nullptr;
+    }
     return c;
   }
   flsp_velocity_desc vel_dev;   // terms as laid out in the device tables
@@ -339,8 +350,55 @@ int validate_reinit(const flsp_handle* h, const flsp_reinit_opts* o) {
   if (o->max_iter < 0) return fail(FLSP_ERR_BAD_ARG, "negative max_iter");
   if (o->viscosity < 0.0) return fail(FLSP_ERR_BAD_ARG, "negative viscosity");
   if (o->rk_order < 1 || o->rk_order > 3) return fail(FLSP_ERR_BAD_ARG, "reinit rk_order must be 1..3");
+  if (o->narrow_band && !(o->band_cells > 0.0)) return fail(FLSP_ERR_BAD_ARG, "narrow band needs band_cells > 0");
   (void)h;
   return FLSP_OK;
+}
+
+// Compute-restricted narrow band (flsp_reinit_opts::narrow_band): only the
+// tiles within two cells of the band |mean phi0| <= band_cells * min_diam
+// are swept (kernel grids keep their size, blocks past the device-side tile
+// count return at once, so nothing here waits for the host); the other
+// state buffers start as copies of phi0 so that untouched tiles stay
+// consistent, and at the end the cells outside the band get phi0 back.
+// Enqueue only: usable inside a stream capture.
+int ensure_band_buffers(flsp_handle* h) {
+  if (!h->nb_flags) {
+    CU(cudaMalloc(&h->nb_flags, (size_t)h->m.ncell * sizeof(int)));
+    CU(cudaMalloc(&h->nb_lists, 3 * (size_t)h->m.ncell * sizeof(int)));
+    CU(cudaMalloc(&h->nb_counts, 3 * sizeof(int)));
+  }
+  return FLSP_OK;
+}
+
+// (buffers allocated beforehand by ensure_band_buffers)
+int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter) {
+  Ctx c = h->ctx();
+  ST(launch_band_flags(c, h->buf[phi0], o->band_cells * h->m.min_diam, h->nb_flags));
+  const int margin = 2;
+  ST(launch_band_tiles(c, h->nb_flags, h->hj_tile, margin, h->nb_lists, h->nb_counts));
+  h->nb_use[kNbHJ] = true;
+  if (o->viscosity > 0.0) {
+    ST(launch_band_tiles(c, h->nb_flags, h->dim == 2 ? kLdgTile2 : kLdgTile3, margin,
+                         h->nb_lists + (size_t)kNbLdg * h->m.ncell, h->nb_counts + kNbLdg));
+    h->nb_use[kNbLdg] = true;
+    CU(cudaMemsetAsync(h->qbuf, 0, (size_t)h->dim * h->ndofs * h->tsize, h->stream));
+    CU(cudaMemsetAsync(h->rdiff, 0, (size_t)h->ndofs * h->tsize, h->stream));
+  }
+  if (limiter) {
+    ST(launch_band_tiles(c, h->nb_flags, kWenoTile, margin, h->nb_lists + (size_t)kNbWeno * h->m.ncell,
+                         h->nb_counts + kNbWeno));
+    h->nb_use[kNbWeno] = true;
+  }
+  for (int i = 0; i < 3; ++i)
+    if (i != phi0)
+      CU(cudaMemcpyAsync(h->buf[i], h->buf[phi0], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  return FLSP_OK;
+}
+
+int band_end(flsp_handle* h, int phi0) {
+  for (int k = 0; k < 3; ++k) h->nb_use[k] = false;
+  return launch_band_restore(h->ctx(), h->buf[phi0], h->buf[h->cur], h->nb_flags);
 }
 
 // ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637)
@@ -349,36 +407,53 @@ int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
   if (o->viscosity > 0.0) ST(ensure_ldg_buffers(h));
   const bool limiter = reinit_limiter(h, o);
   const int phi0 = h->cur;
-  ST(launch_hj_clock_reset(h->stream, h->clk));
-  // CFL estimate of the first pseudo-step: gradients of the initial state
-  ST(launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, o->rk_order, 0.0,
-               h->ndofs, h->hj_tile));
-  int it = 0;
-  if (o->mode == FLSP_REINIT_FIXED) {
-    for (it = 0; it < o->n_pseudo_steps; ++it) ST(enqueue_hj_step(h, o, phi0, limiter));
-  } else {
-    double horizon;
-    if (o->mode == FLSP_REINIT_GLOBAL) {
-      double r[2];
-      ST(reduce_dev(h, FLSP_RED_MAX_ABS, h->buf[phi0], nullptr, false, r));
-      horizon = 1.2 * r[0];
-    } else {
-      horizon = o->band_width_coeff * h->m.min_diam;
-    }
-    double cum = 0.0;
-    while (cum < horizon && it <= o->max_iter) {
-      ST(enqueue_hj_step(h, o, phi0, limiter));
-      ++it;
-      ST(sync_clock(h));
-      cum = h->clk_host->hj_cum;
-      if (!std::isfinite(cum) || !(h->clk_host->hj_dt > 0.0))
-        return fail(FLSP_ERR_NONFINITE, "reinit pseudo-time step is not positive/finite");
+  const bool narrow = o->narrow_band != 0;
+  if (narrow) {
+    ST(ensure_band_buffers(h));
+    const int st = band_begin(h, o, phi0, limiter);
+    if (st) {
+      for (int k = 0; k < 3; ++k) h->nb_use[k] = false;
+      return st;
     }
   }
-  if (n_iter) *n_iter = it;
-  if (o->mode == FLSP_REINIT_BAND && it == o->max_iter)
-    return fail(FLSP_ERR_BAND_NOT_REACHED, "reinit reached max_iter before the band width");
-  return FLSP_OK;
+  auto sweep = [&]() -> int {
+    ST(launch_hj_clock_reset(h->stream, h->clk));
+    // CFL estimate of the first pseudo-step: gradients of the initial state
+    ST(launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, o->rk_order, 0.0,
+                 h->ndofs, h->hj_tile));
+    int it = 0;
+    if (o->mode == FLSP_REINIT_FIXED) {
+      for (it = 0; it < o->n_pseudo_steps; ++it) ST(enqueue_hj_step(h, o, phi0, limiter));
+    } else {
+      double horizon;
+      if (o->mode == FLSP_REINIT_GLOBAL) {
+        double r[2];
+        ST(reduce_dev(h, FLSP_RED_MAX_ABS, h->buf[phi0], nullptr, false, r));
+        horizon = 1.2 * r[0];
+      } else {
+        horizon = o->band_width_coeff * h->m.min_diam;
+      }
+      double cum = 0.0;
+      while (cum < horizon && it <= o->max_iter) {
+        ST(enqueue_hj_step(h, o, phi0, limiter));
+        ++it;
+        ST(sync_clock(h));
+        cum = h->clk_host->hj_cum;
+        if (!std::isfinite(cum) || !(h->clk_host->hj_dt > 0.0))
+          return fail(FLSP_ERR_NONFINITE, "reinit pseudo-time step is not positive/finite");
+      }
+    }
+    if (n_iter) *n_iter = it;
+    if (o->mode == FLSP_REINIT_BAND && it == o->max_iter)
+      return fail(FLSP_ERR_BAND_NOT_REACHED, "reinit reached max_iter before the band width");
+    return FLSP_OK;
+  };
+  int st = sweep();
+  if (narrow) {
+    const int st2 = band_end(h, phi0);
+    if (st == FLSP_OK) st = st2;
+  }
+  return st;
 }
 
 // Lay the velocity terms out for the device: when every component has at
@@ -712,7 +787,8 @@ void flsp_destroy(flsp_handle* h) {
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
   if (h->optab) cudaFree(h->optab);
-  void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_save, h->lrn_feat};
+  void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_save, h->lrn_feat,
+                 h->nb_flags, h->nb_lists, h->nb_counts};
   for (void* q : lrn)
     if (q) cudaFree(q);
   if (h->lrn_count_host) cudaFreeHost(h->lrn_count_host);
@@ -974,6 +1050,7 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
       auto it = h->graphs.find(key);
       if (it == h->graphs.end()) {
         const int cur0 = h->cur;
+        if (ro.narrow_band) ST(ensure_band_buffers(h));
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
         int st = FLSP_OK;
@@ -981,11 +1058,16 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
         if (st == FLSP_OK) {
           const bool limiter = reinit_limiter(h, &ro);
           const int phi0 = h->cur;
-          st = launch_hj_clock_reset(h->stream, h->clk);
+          if (ro.narrow_band) st = band_begin(h, &ro, phi0, limiter);
+          if (st == FLSP_OK) st = launch_hj_clock_reset(h->stream, h->clk);
           if (st == FLSP_OK)
             st = launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, ro.rk_order, 0.0,
                            h->ndofs, h->hj_tile);
           for (int k = 0; k < ro.n_pseudo_steps && st == FLSP_OK; ++k) st = enqueue_hj_step(h, &ro, phi0, limiter);
+          if (ro.narrow_band) {
+            const int st2 = band_end(h, phi0);
+            if (st == FLSP_OK) st = st2;
+          }
         }
         cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
         if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); h->cur = cur0; return st; }
@@ -1130,6 +1212,8 @@ void flsp_default_learned_opts(flsp_learned_opts* o) {
   fill_reinit_defaults(&o->fallback);
   o->fallback.mode = FLSP_REINIT_FIXED;
   o->fallback.n_pseudo_steps = 20;
+  o->fallback.narrow_band = 1;   // the sweep only needs to cover the band
+  o->fallback.band_cells = o->band_cells;
 }
 
 int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o, flsp_learned_stats* stats) {

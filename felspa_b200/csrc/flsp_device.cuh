@@ -159,6 +159,10 @@ struct MeshArgs {
   signed char g2q[64];  // in-cell DoF index -> Q-layout mode
   int tile[3];       // CTA tile in cells
   int ntile[3];      // tiles per axis
+  // compute-restricted narrow band: block b serves tile tiles[b]; blocks
+  // at or past *n_tiles have no tile (null: block b serves tile b)
+  const int* tiles;
+  const int* n_tiles;
 };
 
 // separable velocity: vtab[((k*3 + axis) * nmax + i) * npt + j]
@@ -186,9 +190,14 @@ struct TileCoord {
   int ox, oy, oz;     // tile origin
 };
 
+// a block of a narrow-band launch with no tile to serve (uniform per block)
+__device__ __forceinline__ bool tile_inactive(const MeshArgs& m) {
+  return m.tiles != nullptr && (int)blockIdx.x >= *m.n_tiles;
+}
+
 __device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim) {
   TileCoord c;
-  int b = blockIdx.x;
+  int b = m.tiles ? m.tiles[blockIdx.x] : (int)blockIdx.x;
   const int bx = b % m.ntile[0];
   b /= m.ntile[0];
   const int by = dim > 1 ? b % m.ntile[1] : 0;

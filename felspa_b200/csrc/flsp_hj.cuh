@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
   T* acc = own0 + (size_t)nt * NM;
   double* red = align16<double>(acc + (size_t)nt * 2 * NQV);
   const Tab1D<T>& tb = tab<T>(P);
+  if (tile_inactive(m)) return;
   const TileCoord tc = tile_coord(m, DIM);
 
   load_box<DIM, NM>(m, a.phi, box, tc.ox, tc.oy, tc.oz, true);

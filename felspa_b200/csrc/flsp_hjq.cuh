@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
   T* jn = c0s + (size_t)ntp * NM;           // [2*DIM*NQF][nt]
   double* red = align16<double>(jn + (size_t)nt * 2 * DIM * NQF);
   const Tab1D<T>& tb = tab<T>(P);
+  if (tile_inactive(m)) return;
   const TileCoord tc = tile_coord(m, DIM);
 
   load_box<DIM, NM>(m, a.phi, box, tc.ox, tc.oy, tc.oz, true);

@@ -56,8 +56,6 @@ int hj_prepare(const Ctx& c, const int* tile) {
   });
 }
 
-static const int kLdgTile2[3] = {16, 16, 1};
-static const int kLdgTile3[3] = {8, 8, 4};
 
 int ldg_prepare(const Ctx& c) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
@@ -80,6 +78,7 @@ int launch_ldg(const Ctx& c, const void* in, void* out, long long block, double 
     a.m = c.m;
     const int* t = DIM == 2 ? kLdgTile2 : kLdgTile3;
     set_tile(a.m, DIM, t);
+    apply_band(c, kNbLdg, a.m);
     a.in = reinterpret_cast<const T*>(in);
     a.out = reinterpret_cast<T*>(out);
     a.block = block;
@@ -112,6 +111,7 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
     a.block = block;
     a.rdiff = reinterpret_cast<const T*>(rdiff);
     // the gradient export mode uses the modal kernel for both bases
+    if (mode != kHJGradients) apply_band(c, kNbHJ, a.m);   // the gradient export uses no band
     if (c.basis == FLSP_BASIS_Q && mode != kHJGradients) {
       const size_t smem = hjq_smem_bytes<DIM, P, T>(a.m.tile);
       hjq_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
@@ -119,6 +119,8 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
     }
     int tm[3];
     if (c.basis == FLSP_BASIS_Q) {  // modal kernel with its own tile
+      a.m.tiles = nullptr;
+      a.m.n_tiles = nullptr;
       Ctx cp = c;
       cp.basis = FLSP_BASIS_P;
       hj_default_tile(cp, tm);

@@ -18,7 +18,6 @@ int upload_tables_misc() {
   return FLSP_OK;
 }
 
-static const int kWenoTile[3] = {16, 16, 1};
 
 int weno_prepare(const Ctx& c) {
   if (c.dim != 2) return set_error(FLSP_ERR_UNSUPPORTED, "WENO limiter is 2D only (reinit.cc:475-478)");
@@ -48,6 +47,7 @@ int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count) {
       std::memset(&a, 0, sizeof(a));
       a.m = c.m;
       set_tile(a.m, 2, kWenoTile);
+      apply_band(c, kNbWeno, a.m);
       a.in = reinterpret_cast<const T*>(in);
       a.out = reinterpret_cast<T*>(out);
       a.count = count;
@@ -290,3 +290,85 @@ extern "C" int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int b
   noalloc_finalize<<<1, 1, 0, c.stream>>>(sums, which, ncell * nb, result);
   return launch_status("noalloc_finalize");
 }
+
+// ======================================================================
+// Compute-restricted narrow band of the reinitialisation (no counterpart
+// in the reference, whose sweep covers every cell).
+// ======================================================================
+namespace flsp {
+namespace {
+
+template <typename T>
+__global__ void band_flags_kernel(const T* __restrict__ phi0, long long ncell, int nb, double thr,
+                                  int* __restrict__ flags) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+       c += (long long)gridDim.x * blockDim.x)
+    flags[c] = fabs((double)phi0[c * nb]) <= thr ? 1 : 0;
+}
+
+// one thread per tile: any flagged cell in the tile grown by `margin`?
+__global__ void band_tiles_kernel(const int* __restrict__ flags, MeshArgs m, int dim, int margin,
+                                  int* __restrict__ list, int* __restrict__ count) {
+  const long long ntiles = (long long)m.ntile[0] * m.ntile[1] * m.ntile[2];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(t % m.ntile[0]), by = (int)((t / m.ntile[0]) % m.ntile[1]),
+              bz = (int)(t / ((long long)m.ntile[0] * m.ntile[1]));
+    const int lo[3] = {bx * m.tile[0] - margin, by * m.tile[1] - margin, dim > 2 ? bz * m.tile[2] - margin : 0};
+    const int hi[3] = {(bx + 1) * m.tile[0] + margin, (by + 1) * m.tile[1] + margin,
+                       dim > 2 ? (bz + 1) * m.tile[2] + margin : 1};
+    bool any = false;
+    for (int z = max(lo[2], 0); z < min(hi[2], m.n[2]) && !any; ++z)
+      for (int y = max(lo[1], 0); y < min(hi[1], m.n[1]) && !any; ++y)
+        for (int x = max(lo[0], 0); x < min(hi[0], m.n[0]); ++x)
+          if (flags[x + (long long)m.n[0] * (y + (long long)m.n[1] * z)]) {
+            any = true;
+            break;
+          }
+    if (any) list[atomicAdd(count, 1)] = (int)t;
+  }
+}
+
+template <typename T>
+__global__ void band_restore_kernel(const T* __restrict__ phi0, T* __restrict__ out, const int* __restrict__ flags,
+                                    long long ncell, int nb) {
+  const long long total = ncell * nb;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x)
+    if (!flags[e / nb]) out[e] = phi0[e];
+}
+
+}  // namespace
+
+int launch_band_flags(const Ctx& c, const void* phi0, double thr, int* flags) {
+  const int blocks = grid_for(c.m.ncell);
+  if (c.prec == FLSP_FP64)
+    band_flags_kernel<double><<<blocks, 256, 0, c.stream>>>((const double*)phi0, c.m.ncell, c.m.nb, thr, flags);
+  else
+    band_flags_kernel<float><<<blocks, 256, 0, c.stream>>>((const float*)phi0, c.m.ncell, c.m.nb, thr, flags);
+  return launch_status("band_flags_kernel");
+}
+
+int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margin, int* list, int* count) {
+  MeshArgs m = c.m;
+  m.tiles = nullptr;
+  m.n_tiles = nullptr;
+  set_tile(m, c.dim, tile);
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), c.stream);
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("band tiles: ") + cudaGetErrorString(e));
+  band_tiles_kernel<<<grid_for(nblocks(m)), 256, 0, c.stream>>>(flags, m, c.dim, margin, list, count);
+  return launch_status("band_tiles_kernel");
+}
+
+int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags) {
+  const int blocks = grid_for(c.m.ncell * c.m.nb);
+  if (c.prec == FLSP_FP64)
+    band_restore_kernel<double><<<blocks, 256, 0, c.stream>>>((const double*)phi0, (double*)out, flags, c.m.ncell,
+                                                              c.m.nb);
+  else
+    band_restore_kernel<float><<<blocks, 256, 0, c.stream>>>((const float*)phi0, (float*)out, flags, c.m.ncell,
+                                                             c.m.nb);
+  return launch_status("band_restore_kernel");
+}
+
+}  // namespace flsp

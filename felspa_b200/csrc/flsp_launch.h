@@ -14,11 +14,36 @@ namespace flsp {
 
 int set_error(int code, const std::string& msg);
 
+// narrow-band tile lists, one per kernel family (their tile shapes differ)
+enum NarrowBandKind : int { kNbHJ = 0, kNbLdg = 1, kNbWeno = 2 };
+
 struct Ctx {
   int dim, p, prec, basis;
   MeshArgs m;          // tile fields are filled by the launchers
   cudaStream_t stream;
+  const int* nb_tiles[3];   // active tile lists (null: every tile)
+  const int* nb_count[3];   // device counts of the lists
 };
+
+// tile shapes of the LDG viscosity and WENO limiter kernels
+inline constexpr int kLdgTile2[3] = {16, 16, 1};
+inline constexpr int kLdgTile3[3] = {8, 8, 4};
+inline constexpr int kWenoTile[3] = {16, 16, 1};
+
+// narrow band: flags[c] = 1 for cells with |mean phi0| <= thr; then the
+// list of tiles of shape `tile` that hold a flagged cell within `margin`
+// cells of the tile (device count in *count, order of the list arbitrary:
+// each tile is computed independently)
+int launch_band_flags(const Ctx& c, const void* phi0, double thr, int* flags);
+int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margin, int* list, int* count);
+// out[c] = phi0[c] for cells with flags[c] == 0
+int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags);
+
+// restrict a launch's MeshArgs to the narrow-band tile list of `kind`
+inline void apply_band(const Ctx& c, int kind, MeshArgs& m) {
+  m.tiles = c.nb_tiles[kind];
+  m.n_tiles = c.nb_count[kind];
+}
 
 inline bool supported_config(int dim, int p) {
   return (dim == 2 && p >= 1 && p <= 3) || (dim == 3 && p >= 1 && p <= 2);

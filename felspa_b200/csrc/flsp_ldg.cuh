@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(256) ldg_kernel(const LdgArgs<T> a, int mode) 
   T* box = reinterpret_cast<T*>(smem_raw);
   const MeshArgs& m = a.m;
   const Tab1D<T>& tb = tab<T>(P);
+  if (tile_inactive(m)) return;
   const TileCoord tc = tile_coord(m, DIM);
   const T kp = T(0.5 + 1.0 / sqrt((double)DIM)), km = T(0.5 - 1.0 / sqrt((double)DIM));
   const int g[3] = {tc.gx, tc.gy, tc.gz};

@@ -60,6 +60,7 @@ __global__ void __launch_bounds__(256) weno_kernel(const WenoArgs<T> a) {
   T* box = reinterpret_cast<T*>(smem_raw);
   const MeshArgs& m = a.m;
   const Tab1D<T>& tb = tab<T>(P);
+  if (tile_inactive(m)) return;
   const TileCoord tc = tile_coord(m, 2);
   load_box<2, NM>(m, a.in, box, tc.ox, tc.oy, 0, true);
   cp_async_wait_all();

@@ -133,6 +133,8 @@ def test_learned_band_and_forced_fallback():
     load().flsp_default_reinit_opts(C.byref(o))
     o.mode = abi.REINIT_FIXED
     o.n_pseudo_steps = 20
+    o.narrow_band = 1     # the fallback's default: the sweep restricted to the band
+    o.band_cells = 6.0
     nit = C.c_int(0)
     check(load().flsp_reinit(pb.h, C.byref(o), C.byref(nit)))
     hj = pb.get_state().reshape(-1, 9)
