@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="short run for ncu: set-up, 2 reinit periods, no timing loops")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-vs-plain reinitialisation comparison (2D, ~1 min)")
     return ap.parse_args()
 
 
@@ -329,10 +331,42 @@ def run_ours(args):
         "clocks": clocks,
         "accuracy": {"area_rel_change": (area1 - area0) / area0},
     }
+    if world == 1 and not args.no_learned:
+        line["learned_vs_plain"] = learned_comparison()
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def learned_comparison():
+    """Learned (tensor-core MLP) vs plain HJ reinitialisation on the 2D
+    degree-2 slotted-disk revolution; the network is trained here, on the
+    GPU, on pairs produced by the plain sweep."""
+    from felspa_b200.learned import learned_vs_plain
+    r = learned_vs_plain(n=256, instances=16, train_steps=12000)
+    runs = {}
+    for x in r["runs"]:
+        key = x["method"]
+        if key == "plain" and x.get("graph_replay"):
+            key = "plain_graph"
+        if key == "learned" and x.get("max_residual", 0) > 1e6:
+            key = "learned_no_fallback"
+        runs[key] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in x.items()
+                     if k not in ("method", "mesh", "graph_replay")}
+    best_plain = max(runs["plain"]["dof_steps_per_s"], runs["plain_graph"]["dof_steps_per_s"])
+    return {
+        "workload": "2D degree-2 Q slotted disk (centre (0.5,0.75), r 0.15, slot 0.05x0.25), 256^2, one CCW "
+                    "revolution, CFL 0.1, FP32, reinit every 40 steps; L1 interface error and area change vs "
+                    "the initial shape; wall clock of the whole run",
+        "plain_reinit": "reference LF HJ sweep, 5 fixed pseudo-steps, LDG viscosity 1e-3, CFL 0.1",
+        "learned_reinit": "MLP 82-256x4-9 (BF16 tcgen05) over the 6-cell band; fallback = the plain sweep "
+                          "restricted to the band, for cells with mean ||grad phi|-1| > 0.05",
+        "training": {k: (round(v, 8) if isinstance(v, float) else v) for k, v in r["training"].items()},
+        "runs": runs,
+        "learned_vs_best_plain_speed": runs["learned"]["dof_steps_per_s"] / best_plain,
+        "learned_no_fallback_vs_best_plain_speed": runs["learned_no_fallback"]["dof_steps_per_s"] / best_plain,
+    }
 
 
 def main():

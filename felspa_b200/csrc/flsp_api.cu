@@ -612,7 +612,7 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
     CU(cudaMalloc(&h->lrn_work, (size_t)(2 * nblk + 2) * sizeof(int)));
     CU(cudaMalloc(&h->lrn_cells, (size_t)ncell * sizeof(int)));
     CU(cudaMalloc(&h->lrn_count, 2 * sizeof(int)));
-    CU(cudaMallocHost(&h->lrn_count_host, 2 * sizeof(int)));
+    CU(cudaMallocHost(&h->lrn_count_host, 4 * sizeof(int)));
     CU(cudaMalloc(&h->lrn_save, (size_t)h->ndofs * h->tsize + kStatePad));
   }
   if (h->lrn_feat_cap < nfeat) {
@@ -1192,7 +1192,7 @@ int flsp_mlp_collect(flsp_mlp* net, flsp_handle* h, double band_cells, const fls
   ST(select_band(h, band_cells, &n));
   ST(mlp_ensure_pairs(net, net->n_pairs + n));
   const double hh = h->m.h[0];
-  ST(launch_patch_features(h->stream, h->prec, h->buf[h->cur], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n,
+  ST(launch_patch_features(h->stream, h->prec, h->buf[h->cur], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n, nullptr,
                            net->feat + net->n_pairs * FLSP_MLP_IN));
   CU(cudaMemcpyAsync(h->lrn_save, h->buf[h->cur], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
   int nit = 0;
@@ -1222,41 +1222,43 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   CU(cudaSetDevice(h->dev));
   ST(learned_check(h, net));
   ST(validate_reinit(h, &o->fallback));
-  int64_t n = 0;
-  ST(select_band(h, o->band_cells, &n));
+  // every launch is sized for all cells; the band's size stays on the device
+  // (kernels past it return at once), so the host waits only once, for the
+  // counts that decide the fallback
+  const int64_t ncell = h->m.ncell;
+  ST(ensure_learned_buffers(h, ncell));
+  ST(mlp_ensure_cap(net, ncell));
   const double hh = h->m.h[0];
   const int pre = h->cur;
   const int out = other(pre, -1);
-  flsp_learned_stats stl = {n, 0, 0};
-  if (n > 0) {
-    ST(ensure_learned_buffers(h, n));
-    ST(mlp_ensure_cap(net, n));
-    ST(launch_patch_features(h->stream, h->prec, h->buf[pre], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n,
-                             h->lrn_feat));
-    // the network runs on its own stream: order it after the features
+  const int* nband = h->lrn_count;
+  ST(launch_band_select(h->stream, h->prec, h->buf[pre], ncell, o->band_cells * hh, h->lrn_flags, h->lrn_work,
+                        h->lrn_cells, h->lrn_count));
+  ST(launch_patch_features(h->stream, h->prec, h->buf[pre], h->m.n[0], h->m.n[1], hh, h->lrn_cells, ncell, nband,
+                           h->lrn_feat));
+  {
+    // the network runs on its own stream: order it after the features and back
     cudaEvent_t ev;
     CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     cudaEventRecord(ev, h->stream);
     cudaStreamWaitEvent(net->stream, ev, 0);
-    int st = mlp_pack_input(net, h->lrn_feat, nullptr, n);
-    if (st == FLSP_OK) st = mlp_forward_dev(net, n, false);
+    int st = mlp_pack_input(net, h->lrn_feat, nullptr, ncell, nband);
+    if (st == FLSP_OK) st = mlp_forward_dev(net, ncell, false, nband);
     cudaEventRecord(ev, net->stream);
     cudaStreamWaitEvent(h->stream, ev, 0);
     cudaEventDestroy(ev);
     ST(st);
-    ST(launch_apply_delta(h->stream, h->prec, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, n, net->y, 16));
-    // band cells whose result is not distance-like enough take the HJ sweep
-    ST(launch_residual_flags(h->stream, h->prec, h->buf[out], h->m.n[0], hh, h->lrn_cells, n, o->max_residual,
-                             h->lrn_flags, h->lrn_count + 1));
-    CU(cudaMemcpyAsync(h->lrn_count_host + 1, h->lrn_count + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    int e = 0;
-    CU(cudaMemcpy(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) return fail(FLSP_ERR_TIMEOUT, "a tensor-core kernel's pipeline wait ran out");
-    stl.n_fallback = h->lrn_count_host[1];
-  } else {
-    CU(cudaMemcpyAsync(h->buf[out], h->buf[pre], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
   }
+  ST(launch_apply_delta(h->stream, h->prec, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, ncell, nband,
+                        net->y, 16));
+  // band cells whose result is not distance-like enough take the HJ sweep
+  ST(launch_residual_flags(h->stream, h->prec, h->buf[out], h->m.n[0], hh, h->lrn_cells, ncell, nband,
+                           o->max_residual, h->lrn_flags, h->lrn_count + 1));
+  CU(cudaMemcpyAsync(h->lrn_count_host, h->lrn_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(h->lrn_count_host + 2, net->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  if (h->lrn_count_host[2]) return fail(FLSP_ERR_TIMEOUT, "a tensor-core kernel's pipeline wait ran out");
+  flsp_learned_stats stl = {h->lrn_count_host[0], h->lrn_count_host[1], 0};
   if (stl.n_fallback > 0) {
     // keep the network's result, run the sweep from the pre-reinit state,
     // then put the network's result back everywhere but the flagged cells
@@ -1267,13 +1269,14 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
     const int hj = h->cur;
     const int res = other(hj, -1);
     CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
-    ST(launch_merge_cells(h->stream, h->prec, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, n));
+    ST(launch_merge_cells(h->stream, h->prec, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, stl.n_band,
+                          nullptr));
     h->cur = res;
     stl.hj_ran = 1;
+    CU(cudaStreamSynchronize(h->stream));
   } else {
     h->cur = out;
   }
-  CU(cudaStreamSynchronize(h->stream));
   h->n_since_reinit = 0;
   if (stats) *stats = stl;
   return FLSP_OK;

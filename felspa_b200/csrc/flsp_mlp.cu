@@ -34,8 +34,11 @@ static int grid_of(long long n, int threads = 256) {
 // + k * ld_c] inside rows x cols, zero in the padding
 __global__ void k_pack(const float* __restrict__ src, const int* __restrict__ idx, long long ld_r,
                        long long ld_c, int rows, int cols, float scale, __nv_bfloat16* __restrict__ dst,
-                       int R, int K) {
-  const long long total = (long long)R * K;
+                       int R, int K, const int* __restrict__ rows_dev) {
+  // with a device-side row count only the 128-row tiles that hold rows are written
+  if (rows_dev) rows = min(rows, *rows_dev);
+  const int Rw = rows_dev ? min(R, ((rows + 127) / 128) * 128) : R;
+  const long long total = (long long)Rw * K;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(e / K), k = (int)(e % K);
@@ -157,8 +160,10 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __re
 // ---- level-set patch kernels (2D, degree 2, Q basis: 9 coefficients / cell)
 template <typename T>
 __global__ void k_patch_features(const T* __restrict__ s, int nx, int ny, float ih, float hfeat,
-                                 const int* __restrict__ cells, long long n, float* __restrict__ feat) {
+                                 const int* __restrict__ cells, long long n, const int* __restrict__ n_dev,
+                                 float* __restrict__ feat) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n_dev) n = min(n, (long long)*n_dev);
   if (t >= n * 9) return;
   const long long i = t / 9;
   const int j = (int)(t % 9);   // patch cell: dy outer, dx inner
@@ -185,8 +190,9 @@ __global__ void k_patch_targets(const T* __restrict__ pre, const T* __restrict__
 
 template <typename T>
 __global__ void k_apply_delta(T* __restrict__ out, double h, const int* __restrict__ cells, long long n,
-                              const float* __restrict__ y, int ldy) {
+                              const int* __restrict__ n_dev, const float* __restrict__ y, int ldy) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n_dev) n = min(n, (long long)*n_dev);
   if (t >= n * 9) return;
   const long long i = t / 9;
   const int q = (int)(t % 9);
@@ -230,9 +236,10 @@ __global__ void k_band_compact(const int* __restrict__ flags, long long ncell, c
 
 // mean of ||grad phi| - 1| over the 3 x 3 Gauss points of each listed cell
 template <typename T>
-__global__ void k_residual(const T* __restrict__ s, double ih, const int* __restrict__ cells, long long n, double thr,
-                           int* __restrict__ flags, int* __restrict__ count) {
+__global__ void k_residual(const T* __restrict__ s, double ih, const int* __restrict__ cells, long long n,
+                           const int* __restrict__ n_dev, double thr, int* __restrict__ flags, int* __restrict__ count) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n_dev) n = min(n, (long long)*n_dev);
   if (i >= n) return;
   const T* c = s + (long long)cells[i] * 9;
   const double g[3] = {0.5 - 0.5 * 0.7745966692414834, 0.5, 0.5 + 0.5 * 0.7745966692414834};
@@ -261,8 +268,9 @@ __global__ void k_residual(const T* __restrict__ s, double ih, const int* __rest
 
 template <typename T>
 __global__ void k_merge(const T* __restrict__ src, T* __restrict__ out, const int* __restrict__ cells,
-                        const int* __restrict__ flags, long long n) {
+                        const int* __restrict__ flags, long long n, const int* __restrict__ n_dev) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (n_dev) n = min(n, (long long)*n_dev);
   if (t >= n * 9) return;
   const long long i = t / 9;
   if (!flags[i]) return;
@@ -351,13 +359,13 @@ static int repack(flsp_mlp* net) {
     const float* W = net->p + L.w_off;
     const long long nw = (long long)L.n_pad * L.k_pad;
     k_pack<<<grid_of(nw), 256, 0, net->stream>>>(W, nullptr, L.n_in, 1, L.n_out, L.n_in, 1.0f, net->wp[l], L.n_pad,
-                                                L.k_pad);
+                                                L.k_pad, nullptr);
     MST(launch_status("k_pack"));
     if (net->wtp[l]) {
       const long long nt = (long long)net->wt_rows[l] * net->wt_k[l];
       // W^T: rows = inputs, K = outputs
       k_pack<<<grid_of(nt), 256, 0, net->stream>>>(W, nullptr, 1, L.n_in, L.n_in, L.n_out, 1.0f, net->wtp[l],
-                                                  net->wt_rows[l], net->wt_k[l]);
+                                                  net->wt_rows[l], net->wt_k[l], nullptr);
       MST(launch_status("k_pack"));
     }
     MCU(cudaMemsetAsync(net->bp[l], 0, (size_t)L.n_pad * 4, net->stream));
@@ -366,13 +374,14 @@ static int repack(flsp_mlp* net) {
   return FLSP_OK;
 }
 
-int mlp_pack_input(flsp_mlp* net, const float* feat, const int* idx, int64_t n) {
+int mlp_pack_input(flsp_mlp* net, const float* feat, const int* idx, int64_t n, const int* rows_dev) {
   const long long R = round128(n);
-  k_pack<<<grid_of(R * 128), 256, 0, net->stream>>>(feat, idx, kMlpIn, 1, (int)n, kMlpIn, 1.0f, net->x, (int)R, 128);
+  k_pack<<<grid_of(R * 128), 256, 0, net->stream>>>(feat, idx, kMlpIn, 1, (int)n, kMlpIn, 1.0f, net->x, (int)R, 128,
+                                                    rows_dev);
   return launch_status("k_pack");
 }
 
-int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train) {
+int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train, const int* rows_dev) {
   const int R = (int)round128(n);
   const __nv_bfloat16* in = net->x;
   for (int l = 0; l < 4; ++l) {
@@ -388,6 +397,7 @@ int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train) {
     a.out_k = 256;
     a.gd_out = train ? net->gd[l] : nullptr;
     a.err = net->err;
+    a.rows_dev = rows_dev;
     MST(gemm<kEpiHidden>(net->stream, a));
     in = net->act[l];
   }
@@ -404,6 +414,7 @@ int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train) {
   a.n_valid = 16;
   a.m_valid = R;
   a.err = net->err;
+  a.rows_dev = rows_dev;
   return gemm<kEpiOutput>(net->stream, a);
 }
 
@@ -624,8 +635,8 @@ int flsp_mlp_forward(flsp_mlp* net, const float* x, int64_t batch, float* y) {
   MCU(cudaMallocAsync(&fdev, (size_t)batch * kMlpIn * 4, net->stream));
   std::memcpy(net->hbuf, x, (size_t)batch * kMlpIn * 4);
   cudaMemcpyAsync(fdev, net->hbuf, (size_t)batch * kMlpIn * 4, cudaMemcpyHostToDevice, net->stream);
-  int st = mlp_pack_input(net, fdev, nullptr, batch);
-  if (st == FLSP_OK) st = mlp_forward_dev(net, batch, false);
+  int st = mlp_pack_input(net, fdev, nullptr, batch, nullptr);
+  if (st == FLSP_OK) st = mlp_forward_dev(net, batch, false, nullptr);
   cudaFreeAsync(fdev, net->stream);
   MST(st);
   MST(check_err(net));
@@ -645,8 +656,8 @@ int flsp_mlp_backward(flsp_mlp* net, const float* x, const float* dy, int64_t ba
   MCU(cudaMallocAsync(&dydev, (size_t)batch * kMlpOut * 4, net->stream));
   MCU(cudaMemcpyAsync(fdev, x, (size_t)batch * kMlpIn * 4, cudaMemcpyHostToDevice, net->stream));
   MCU(cudaMemcpyAsync(dydev, dy, (size_t)batch * kMlpOut * 4, cudaMemcpyHostToDevice, net->stream));
-  int st = mlp_pack_input(net, fdev, nullptr, batch);
-  if (st == FLSP_OK) st = mlp_forward_dev(net, batch, true);
+  int st = mlp_pack_input(net, fdev, nullptr, batch, nullptr);
+  if (st == FLSP_OK) st = mlp_forward_dev(net, batch, true, nullptr);
   if (st == FLSP_OK) st = output_grad(net, batch, dydev, nullptr);
   if (st == FLSP_OK) st = mlp_backward_dev(net, batch);
   cudaFreeAsync(fdev, net->stream);
@@ -715,8 +726,8 @@ int flsp_mlp_train(flsp_mlp* net, const flsp_train_opts* o, double* loss) {
     }
     const int* bidx = net->idx + pos;
     pos += B;
-    MST(mlp_pack_input(net, net->feat, bidx, B));
-    MST(mlp_forward_dev(net, B, true));
+    MST(mlp_pack_input(net, net->feat, bidx, B, nullptr));
+    MST(mlp_forward_dev(net, B, true, nullptr));
     MST(output_grad(net, B, nullptr, bidx));
     MST(mlp_backward_dev(net, B));
     net->adam_t += 1;
@@ -748,8 +759,8 @@ int flsp_mlp_eval(flsp_mlp* net, double* loss) {
   double total = 0.0;
   for (int64_t p0 = 0; p0 < net->n_pairs; p0 += chunk) {
     const int64_t n = std::min<int64_t>(chunk, net->n_pairs - p0);
-    MST(mlp_pack_input(net, net->feat + p0 * kMlpIn, nullptr, n));
-    MST(mlp_forward_dev(net, n, false));
+    MST(mlp_pack_input(net, net->feat + p0 * kMlpIn, nullptr, n, nullptr));
+    MST(mlp_forward_dev(net, n, false, nullptr));
     // loss only (the gradient buffers are scratch here)
     const int R = (int)round128(n);
     const int nblk = R / 256 + 1;
@@ -775,11 +786,11 @@ namespace flsp {
 #define DISPATCH_T(prec, F) ((prec) == FLSP_FP64 ? F(double) : F(float))
 
 int launch_patch_features(cudaStream_t s, int prec, const void* state, int nx, int ny, double h, const int* cells,
-                          int64_t n, float* feat) {
+                          int64_t n, const int* n_dev, float* feat) {
   if (n <= 0) return FLSP_OK;
   const long long t = n * 9;
   const int blocks = (int)((t + 255) / 256);
-#define L_(T) (k_patch_features<T><<<blocks, 256, 0, s>>>((const T*)state, nx, ny, (float)(1.0 / h), (float)(64.0 * h), cells, n, feat), 0)
+#define L_(T) (k_patch_features<T><<<blocks, 256, 0, s>>>((const T*)state, nx, ny, (float)(1.0 / h), (float)(64.0 * h), cells, n, n_dev, feat), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_patch_features");
@@ -796,12 +807,12 @@ int launch_patch_targets(cudaStream_t s, int prec, const void* pre, const void* 
 }
 
 int launch_apply_delta(cudaStream_t s, int prec, const void* pre, void* out, int64_t ndofs, double h, const int* cells,
-                       int64_t n, const float* y, int ldy) {
+                       int64_t n, const int* n_dev, const float* y, int ldy) {
   const size_t es = prec == FLSP_FP64 ? 8 : 4;
   if (pre != out) MCU(cudaMemcpyAsync(out, pre, (size_t)ndofs * es, cudaMemcpyDeviceToDevice, s));
   if (n <= 0) return FLSP_OK;
   const int blocks = (int)((n * 9 + 255) / 256);
-#define L_(T) (k_apply_delta<T><<<blocks, 256, 0, s>>>((T*)out, h, cells, n, y, ldy), 0)
+#define L_(T) (k_apply_delta<T><<<blocks, 256, 0, s>>>((T*)out, h, cells, n, n_dev, y, ldy), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_apply_delta");
@@ -823,22 +834,22 @@ int launch_band_select(cudaStream_t s, int prec, const void* state, int64_t ncel
 }
 
 int launch_residual_flags(cudaStream_t s, int prec, const void* state, int nx, double h, const int* cells, int64_t n,
-                          double thr, int* flags, int* count_dev) {
+                          const int* n_dev, double thr, int* flags, int* count_dev) {
   (void)nx;
   MCU(cudaMemsetAsync(count_dev, 0, sizeof(int), s));
   if (n <= 0) return FLSP_OK;
   const int blocks = (int)((n + 127) / 128);
-#define L_(T) (k_residual<T><<<blocks, 128, 0, s>>>((const T*)state, 1.0 / h, cells, n, thr, flags, count_dev), 0)
+#define L_(T) (k_residual<T><<<blocks, 128, 0, s>>>((const T*)state, 1.0 / h, cells, n, n_dev, thr, flags, count_dev), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_residual");
 }
 
 int launch_merge_cells(cudaStream_t s, int prec, const void* src, void* out, const int* cells, const int* flags,
-                       int64_t n) {
+                       int64_t n, const int* n_dev) {
   if (n <= 0) return FLSP_OK;
   const int blocks = (int)((n * 9 + 255) / 256);
-#define L_(T) (k_merge<T><<<blocks, 256, 0, s>>>((const T*)src, (T*)out, cells, flags, n), 0)
+#define L_(T) (k_merge<T><<<blocks, 256, 0, s>>>((const T*)src, (T*)out, cells, flags, n, n_dev), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_merge");

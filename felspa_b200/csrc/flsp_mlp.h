@@ -76,22 +76,27 @@ namespace flsp {
 
 int mlp_ensure_cap(flsp_mlp* net, int64_t rows);
 int mlp_ensure_pairs(flsp_mlp* net, int64_t n);
-// forward of rows [0, n) of net->x (packed); train = keep GELU' for backward
-int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train);
+// forward of rows [0, n) of net->x (packed); train = keep GELU' for backward.
+// rows_dev (optional): a device-side row count <= n; the operand geometry
+// stays that of n rows, work past the count is skipped on the device.
+int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train, const int* rows_dev);
 // pack n feature rows (fp32 n x 82, row stride 82; gathered through idx if
-// non-null) into net->x
-int mlp_pack_input(flsp_mlp* net, const float* feat, const int* idx, int64_t n);
+// non-null) into net->x (rows_dev as above)
+int mlp_pack_input(flsp_mlp* net, const float* feat, const int* idx, int64_t n, const int* rows_dev);
 
+// The list launchers below take an upper bound n for their grids and an
+// optional device-side count n_dev <= n of the cells actually listed.
+//
 // patch features of the listed cells of a 2D degree-2 Q-basis state
 // (lexicographic cells, 9 coefficients each), fp32 n x 82
 int launch_patch_features(cudaStream_t s, int prec, const void* state, int nx, int ny, double h,
-                          const int* cells, int64_t n, float* feat);
+                          const int* cells, int64_t n, const int* n_dev, float* feat);
 // targets (post - pre) / h of the listed cells' coefficients, fp32 n x 9
 int launch_patch_targets(cudaStream_t s, int prec, const void* pre, const void* post, double h,
                          const int* cells, int64_t n, float* targ);
 // out = pre; out[cells] += h * y[:, 0:9] (y row stride ldy)
 int launch_apply_delta(cudaStream_t s, int prec, const void* pre, void* out, int64_t ndofs, double h,
-                       const int* cells, int64_t n, const float* y, int ldy);
+                       const int* cells, int64_t n, const int* n_dev, const float* y, int ldy);
 // band cells |c0| <= band * h, compacted in increasing cell order; count
 // to *count_dev; work holds 2 * ceil(ncell / 256) + 1 ints
 int launch_band_select(cudaStream_t s, int prec, const void* state, int64_t ncell, double thr, int* flags,
@@ -99,9 +104,9 @@ int launch_band_select(cudaStream_t s, int prec, const void* state, int64_t ncel
 // cells of the list whose mean of ||grad phi| - 1| over the 3 x 3 Gauss
 // points exceeds thr: flags[i] = 1 and a count (in *count_dev)
 int launch_residual_flags(cudaStream_t s, int prec, const void* state, int nx, double h, const int* cells,
-                          int64_t n, double thr, int* flags, int* count_dev);
+                          int64_t n, const int* n_dev, double thr, int* flags, int* count_dev);
 // out[cells[i]] = src[cells[i]] where flags[i]
 int launch_merge_cells(cudaStream_t s, int prec, const void* src, void* out, const int* cells,
-                       const int* flags, int64_t n);
+                       const int* flags, int64_t n, const int* n_dev);
 
 }  // namespace flsp

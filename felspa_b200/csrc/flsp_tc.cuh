@@ -119,6 +119,7 @@ struct TcGemmArgs {
   float* y;                   // fp32 row-major output (output / store)
   int ldy, n_valid, m_valid;
   int* err;                   // device error word
+  const int* rows_dev;        // if set: only row tiles below this device-side count do work
 };
 
 __device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -140,6 +141,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * kTcBM;
+  if (a.rows_dev && m0 >= *a.rows_dev) return;   // uniform per CTA, before any barrier or TMEM
   const int nk = a.K / kTcBK;
   uint32_t ncols = 32;
   while ((int)ncols < N) ncols <<= 1;

@@ -140,3 +140,138 @@ class MLP:
         st = abi.LearnedStats()
         check(load().flsp_reinit_learned(problem.h, self.h, C.byref(o), C.byref(st)))
         return {"n_band": st.n_band, "n_fallback": st.n_fallback, "hj_ran": bool(st.hj_ran)}
+
+
+# ----------------------------------------------------------------------
+# learned vs plain HJ reinitialisation (the comparison of the benchmark)
+# ----------------------------------------------------------------------
+def plain_reinit_opts(n_pseudo_steps=5, viscosity=1e-3, cfl_max=0.1):
+    """The plain HJ sweep of the comparison: the reference's Lax-Friedrichs
+    scheme in fixed-count mode with the artificial viscosity of its own
+    Zalesak test and the lower of that test's two reinit CFL numbers
+    (tests/test_zalesak_disk.cc:252-257).  Under repeated reinitialisation
+    the scheme diverges without the viscosity, and at 256^2 and finer also
+    with CFL 0.3."""
+    return abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=n_pseudo_steps, viscosity=viscosity,
+                                   cfl_max=cfl_max)
+
+
+def slotted_disk(seed):
+    r = np.random.default_rng(seed)
+    from . import fields as F
+    cx, cy = r.uniform(0.3, 0.7, 2)
+    rad = r.uniform(0.1, 0.2)
+    return F.zalesak_disk(center=(float(cx), float(cy)), radius=float(rad), slot_width=float(r.uniform(0.03, 0.08)),
+                          slot_depth=float(r.uniform(0.5, 1.6) * rad))
+
+
+def collect_training_pairs(net, n=128, instances=24, periods=10, every=40, target=None, band_cells=6.0):
+    """Pairs from random instances (unions of circles and slotted disks; the
+    velocity alternates between an 8-mode Fourier stream function, which
+    distorts the level set, and a rigid rotation about a random centre,
+    which keeps it distance-like; seeds 1000 + i): advance `every` steps,
+    record the band patches, reinitialise with `target`."""
+    from . import fields as F
+    from .level_set import Mesh, Problem
+    target = target if target is not None else plain_reinit_opts()
+    for i in range(instances):
+        pb = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+        if (i // 2) % 2 == 0:
+            pb.set_velocity(F.fourier_stream_2d(seed=1000 + i))
+        else:
+            r = np.random.default_rng(3000 + i)
+            c = r.uniform(0.4, 0.6, 2)
+            pb.set_velocity(F.ccw_rotation(center=(float(c[0]), float(c[1])),
+                                           omega=float(2 * np.pi * r.uniform(0.5, 1.5))))
+        pb.project(F.circles_union(1000 + i) if i % 2 == 0 else slotted_disk(2000 + i))
+        for _ in range(periods):
+            check(load().flsp_advance_steps(pb.h, int(every), 1e30))
+            net.collect(pb, band_cells, target)
+        pb.close()
+    return net.n_pairs
+
+
+def zalesak_run(method, net=None, n=128, every=40, T=1.0, plain=None, max_residual=0.05, use_graph=False):
+    """One revolution of the slotted disk (centre (0.5, 0.75), r 0.15, slot
+    0.05 x 0.25) under the counter-clockwise rotation, degree-2 Q basis,
+    FP32, CFL 0.1, reinitialised every `every` steps by `method` ("none",
+    "plain" or "learned").  Wall-clock time of the whole run (every
+    reinitialisation included); L1 interface error and area change against
+    the initial shape (FP64 device reductions)."""
+    import time
+    from . import fields as F
+    from .level_set import Mesh, Problem
+    L = load()
+    plain = plain if plain is not None else plain_reinit_opts()
+    pb = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+    pb.set_velocity(F.ccw_rotation())
+    ic = F.zalesak_disk()
+    pb.project(ic)
+    area0 = pb.reduce(abi.RED_MASS_SHARP)
+    lo = default_learned_opts(max_residual=max_residual)
+    lo.fallback = abi.ReinitOpts.from_buffer_copy(plain)
+    lo.fallback.narrow_band = 1
+    lo.fallback.band_cells = lo.band_cells
+    nit = C.c_int(0)
+    steps = reinits = n_band = n_fb = 0
+    check(L.flsp_sync(pb.h))
+    t0 = time.perf_counter()
+    if method == "plain" and use_graph:
+        # fixed-count reinit replayed from captured CUDA graphs; the step
+        # count is that of the host-driven run to T (CFL-limited, same for all)
+        nsteps = zalesak_run.steps_to_T.get((n, T))
+        ctl = abi.default_ls_opts(reinit_frequency=every, reinit=plain)
+        check(L.flsp_ls_run_steps(pb.h, C.byref(ctl), int(nsteps)))
+        check(L.flsp_sync(pb.h))
+        steps, reinits = nsteps, nsteps // every
+    else:
+        while pb.get_time() < T - 1e-12:
+            check(L.flsp_advance_steps(pb.h, int(every), float(T)))
+            steps += every
+            if method == "plain":
+                check(L.flsp_reinit(pb.h, C.byref(plain), C.byref(nit)))
+            elif method == "learned":
+                st = net.reinit(pb, lo)
+                n_band += st["n_band"]
+                n_fb += st["n_fallback"]
+            reinits += 1
+        check(L.flsp_sync(pb.h))
+        zalesak_run.steps_to_T[(n, T)] = steps
+    wall = time.perf_counter() - t0
+    out = {"method": method, "mesh": f"{n}x{n}", "steps": steps, "reinits": reinits, "wall_s": wall,
+           "dof_steps_per_s": pb.n_dofs * steps / wall,
+           "l1_interface_error": pb.reduce(abi.RED_L1_INTERFACE_IC, ic),
+           "area_change": (pb.reduce(abi.RED_MASS_SHARP) - area0) / area0,
+           "grad_deviation": pb.reduce(abi.RED_GRAD_DEVIATION)}
+    if method == "learned":
+        out["fallback_fraction"] = n_fb / n_band if n_band else 0.0
+        out["max_residual"] = max_residual
+    if method == "plain":
+        out["graph_replay"] = bool(use_graph)
+    pb.close()
+    return out
+
+
+zalesak_run.steps_to_T = {}
+
+
+def learned_vs_plain(n=128, instances=24, train_steps=8000, seed=7):
+    """Train the network on the plain sweep's pairs (on the GPU), then run
+    the slotted-disk revolution with no reinit, the plain sweep (host loop
+    and graph replay) and the learned reinit with and without the residual
+    fallback."""
+    import time
+    net = MLP(device=0, seed=seed)
+    t0 = time.perf_counter()
+    n_pairs = collect_training_pairs(net, n=n, instances=instances)
+    t1 = time.perf_counter()
+    loss0 = net.eval()
+    last = net.train(steps=train_steps, batch=8192, lr=1e-3, seed=1)
+    t2 = time.perf_counter()
+    loss1 = net.eval()
+    runs = [zalesak_run("none", n=n), zalesak_run("plain", n=n), zalesak_run("plain", n=n, use_graph=True),
+            zalesak_run("learned", net, n=n), zalesak_run("learned", net, n=n, max_residual=1e9)]
+    net.close()
+    return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
+                         "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},
+            "runs": runs}
