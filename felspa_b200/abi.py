@@ -137,6 +137,19 @@ class LearnedStats(C.Structure):
     ]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [
+        ("adv_tile", C.c_int * 2),
+        ("hj_tile", C.c_int * 2),
+        ("n_adv", C.c_int),
+        ("n_hj", C.c_int),
+        ("adv_cand", (C.c_int * 2) * 8),
+        ("hj_cand", (C.c_int * 2) * 8),
+        ("adv_ms", C.c_double * 8),
+        ("hj_ms", C.c_double * 8),
+    ]
+
+
 MLP_IN, MLP_HIDDEN, MLP_OUT = 82, 256, 9
 
 

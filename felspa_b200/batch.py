@@ -1,0 +1,98 @@
+"""Batched problems: many independent 2D level-set problems advanced by one
+persistent launch per RK stage / reinit pseudo-step, periods replayed from
+captured CUDA graphs, tile shapes from the batch autotuner
+(flsp_batch_* in include/flsp_dg.h).  Not in the reference, where a
+simulator object holds one problem."""
+import ctypes as C
+
+import numpy as np
+
+from . import abi, fields as F
+from .level_set import Mesh, Problem
+from .lib import check, load
+
+
+class Batch:
+    def __init__(self, meshes, degrees, precision=abi.FP32, cfl_max=0.1, rk_order=3, device=0):
+        L = load()
+        n = len(meshes)
+        md = (abi.MeshDesc * n)(*[m.desc() for m in meshes])
+        od = (abi.DGOpts * n)()
+        for i, p in enumerate(degrees):
+            L.flsp_default_dg_opts(C.byref(od[i]))
+            od[i].degree = int(p)
+            od[i].basis = abi.BASIS_Q
+            od[i].precision = precision
+            od[i].rk_order = rk_order
+            od[i].cfl_max = cfl_max
+            od[i].device = device
+        self._md, self._od = md, od
+        b = C.c_void_p()
+        check(L.flsp_batch_create(n, md, od, C.byref(b)))
+        self.h = b
+        self.problems = []
+        for i in range(n):
+            ph = C.c_void_p()
+            check(L.flsp_batch_problem(b, i, C.byref(ph)))
+            self.problems.append(Problem.wrap(ph, meshes[i], int(degrees[i]), abi.BASIS_Q, precision))
+        self.n_dofs = sum(p.n_dofs for p in self.problems)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for p in self.problems:
+                p.h = None
+            load().flsp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self):
+        t = abi.BatchTuning()
+        check(load().flsp_batch_autotune(self.h, C.byref(t)))
+        return {"adv_tile": tuple(t.adv_tile), "hj_tile": tuple(t.hj_tile),
+                "adv_ms": {f"{t.adv_cand[i][0]}x{t.adv_cand[i][1]}": t.adv_ms[i] for i in range(t.n_adv)},
+                "hj_ms": {f"{t.hj_cand[i][0]}x{t.hj_cand[i][1]}": t.hj_ms[i] for i in range(t.n_hj)}}
+
+    def run_steps(self, n_steps, control=None, sync=True):
+        ctl = control if control is not None else abi.default_ls_opts(
+            reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=5))
+        check(load().flsp_batch_run_steps(self.h, C.byref(ctl), int(n_steps)))
+        if sync:
+            self.sync()
+
+    def sync(self):
+        check(load().flsp_batch_sync(self.h))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(load().flsp_batch_stream(self.h, C.byref(s)))
+        return s.value
+
+
+def config3_instances(n_problems=256, seed_base=1000, n_min=32, n_max=256):
+    """The batched configuration: problem i draws from default_rng(seed_base + i)
+    a mesh size N = round(32 * 8^U) (log-uniform 32..256), a degree in {1,2,3};
+    its IC is a union of 1-4 circles (centres U[0.2,0.8]^2, radii U[0.05,0.2])
+    and its velocity the 8-mode Fourier stream-function field scaled to
+    max|u| = 1, both seeded with seed_base + i."""
+    out = []
+    for i in range(n_problems):
+        rng = np.random.default_rng(seed_base + i)
+        n = int(round(n_min * (n_max / n_min) ** rng.uniform()))
+        p = int(rng.integers(1, 4))
+        out.append({"n": n, "degree": p, "ic": F.circles_union(seed_base + i),
+                    "velocity": F.fourier_stream_2d(seed=seed_base + i)})
+    return out
+
+
+def make_batch(instances, precision=abi.FP32, cfl_max=0.1):
+    b = Batch([Mesh(2, (d["n"], d["n"])) for d in instances], [d["degree"] for d in instances],
+              precision=precision, cfl_max=cfl_max)
+    for pb, d in zip(b.problems, instances):
+        pb.set_velocity(d["velocity"])
+        pb.project(d["ic"])
+    return b

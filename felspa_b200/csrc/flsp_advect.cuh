@@ -181,8 +181,9 @@ __device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T c
 
 // General velocity: a runtime sum of separable terms per component.  (A
 // velocity whose components are single terms takes adv_sep_kernel.)
+// one tile of a stage (launch slot `slot`); a plain launch serves slot blockIdx.x
 template <int DIM, int P, typename T>
-__global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
+__device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* box = reinterpret_cast<T*>(smem_raw);
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
   T* vt = box + (size_t)nboxc * NM;
   T* fl = vt + (size_t)max(nterm, 1) * span * NPT;   // [DIM][NF][nt]
   const Tab1D<T>& tb = tab<T>(P);
-  const TileCoord tc = tile_coord(m, DIM);
+  const TileCoord tc = tile_coord(m, DIM, slot);
 
   // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
   {
@@ -442,6 +443,11 @@ __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
   }
   __syncthreads();
   store_tile<DIM, NM>(m, stage_buf, a.out, tc.ox, tc.oy, tc.oz);
+}
+
+template <int DIM, int P, typename T>
+__global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
+  adv_stage_tile<DIM, P, T>(a, (int)blockIdx.x);
 }
 
 }  // namespace flsp

@@ -92,6 +92,7 @@ int upload_tables(int dev) {
   ST(upload_tables_misc());
   ST(upload_tables_sep2());
   ST(upload_tables_sep3());
+  ST(upload_tables_batch());
   if (dev >= 0 && dev < 64) g_tables_ready[dev] = true;
   return FLSP_OK;
 }
@@ -1279,6 +1280,397 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   }
   h->n_since_reinit = 0;
   if (stats) *stats = stl;
+  return FLSP_OK;
+}
+
+// ---- batched problems (no counterpart in the reference: one problem per
+// simulator object there).  Many independent 2D problems advance in one
+// persistent launch per RK stage and per reinit pseudo-step, periods
+// replayed from captured CUDA graphs, tile shapes from the autotuner.
+}  // extern "C"
+
+struct flsp_batch {
+  int dev = 0, prec = 0, rk = 3;
+  cudaStream_t stream = nullptr;
+  std::vector<flsp_handle*> h;
+  int cur = 0;             // common buffer role of every problem
+  int n_since_reinit = 0;
+  bool tuned = false;
+  int adv_tile[3] = {16, 16, 1}, hj_tile[3] = {16, 8, 1};
+  flsp_batch_tuning tuning;
+  // device descriptors and work lists for the current tiles
+  BatchProb* probs = nullptr;
+  int2* items_adv = nullptr;
+  int2* items_hj = nullptr;
+  int2* items_weno = nullptr;
+  int n_adv = 0, n_hj = 0, n_weno = 0;
+  size_t smem_adv = 0, smem_hj = 0, smem_weno = 0;
+  int grid_adv = 1, grid_hj = 1, grid_weno = 1;
+  bool built = false;
+  std::map<unsigned long long, GraphEntry> graphs;
+};
+
+namespace {
+
+void batch_free_plan(flsp_batch* b) {
+  if (b->probs) cudaFree(b->probs);
+  if (b->items_adv) cudaFree(b->items_adv);
+  if (b->items_hj) cudaFree(b->items_hj);
+  if (b->items_weno) cudaFree(b->items_weno);
+  b->probs = nullptr;
+  b->items_adv = b->items_hj = b->items_weno = nullptr;
+  b->built = false;
+  for (auto& kv : b->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  b->graphs.clear();
+}
+
+// descriptors and work lists of every problem for tiles (adv, hj)
+int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
+  batch_free_plan(b);
+  const int n = (int)b->h.size();
+  std::vector<BatchProb> pr((size_t)n);
+  std::vector<int2> ia, ih, iw;
+  size_t sa = 0, sh = 0, sw = 0;
+  for (int i = 0; i < n; ++i) {
+    flsp_handle* h = b->h[i];
+    BatchProb& q = pr[(size_t)i];
+    std::memset(&q, 0, sizeof(q));
+    q.m_adv = h->m;
+    q.m_adv.tiles = nullptr;
+    q.m_adv.n_tiles = nullptr;
+    q.m_hj = q.m_adv;
+    q.m_weno = q.m_adv;
+    set_tile(q.m_adv, 2, adv_tile);
+    set_tile(q.m_hj, 2, hj_tile);
+    set_tile(q.m_weno, 2, kWenoTile);
+    for (int k = 0; k < 3; ++k) q.buf[k] = h->buf[k];
+    q.clk = h->clk;
+    VelDev v = h->veldev();
+    q.vtab = v.vtab;
+    q.n_terms = v.n_terms;
+    q.nmax = v.nmax;
+    q.npt = v.npt;
+    for (int k = 0; k < kMaxTerms; ++k) q.comp[k] = v.comp[k];
+    q.p = h->p;
+    q.ca.cfl_max = h->cfl_max;
+    q.ca.scale = adv_cfl_scaling(h->p);
+    q.ca.tkind = h->vel.time_kind;
+    q.ca.ta = h->vel.ta;
+    q.ca.tb = h->vel.tb;
+    q.ca.rk = h->rk;
+    q.adv_scale = adv_cfl_scaling(h->p);
+    auto add = [&](const MeshArgs& m, std::vector<int2>& it) {
+      const long long nt = nblocks(m);
+      for (long long t = 0; t < nt; ++t) it.push_back(make_int2(i, (int)t));
+    };
+    add(q.m_adv, ia);
+    add(q.m_hj, ih);
+    add(q.m_weno, iw);
+    size_t x = 0;
+    ST(batch_smem(kBatchKindAdv, h->p, b->prec, adv_tile, v.n_terms, &x));
+    sa = std::max(sa, x);
+    ST(batch_smem(kBatchKindHJ, h->p, b->prec, hj_tile, 0, &x));
+    sh = std::max(sh, x);
+    ST(batch_smem(kBatchKindWeno, h->p, b->prec, kWenoTile, 0, &x));
+    sw = std::max(sw, x);
+  }
+  CU(cudaMalloc(&b->probs, sizeof(BatchProb) * (size_t)n));
+  CU(cudaMalloc(&b->items_adv, sizeof(int2) * ia.size()));
+  CU(cudaMalloc(&b->items_hj, sizeof(int2) * ih.size()));
+  CU(cudaMalloc(&b->items_weno, sizeof(int2) * iw.size()));
+  CU(cudaMemcpy(b->probs, pr.data(), sizeof(BatchProb) * (size_t)n, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->items_adv, ia.data(), sizeof(int2) * ia.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->items_hj, ih.data(), sizeof(int2) * ih.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(b->items_weno, iw.data(), sizeof(int2) * iw.size(), cudaMemcpyHostToDevice));
+  b->n_adv = (int)ia.size();
+  b->n_hj = (int)ih.size();
+  b->n_weno = (int)iw.size();
+  b->smem_adv = sa;
+  b->smem_hj = sh;
+  b->smem_weno = sw;
+  ST(batch_prepare(kBatchKindAdv, b->prec, sa, adv_tile[0] * adv_tile[1], b->n_adv, &b->grid_adv));
+  ST(batch_prepare(kBatchKindHJ, b->prec, sh, hj_tile[0] * hj_tile[1], b->n_hj, &b->grid_hj));
+  ST(batch_prepare(kBatchKindWeno, b->prec, sw, kWenoTile[0] * kWenoTile[1], b->n_weno, &b->grid_weno));
+  for (int d = 0; d < 3; ++d) {
+    b->adv_tile[d] = adv_tile[d];
+    b->hj_tile[d] = hj_tile[d];
+  }
+  b->built = true;
+  return FLSP_OK;
+}
+
+int batch_sync_problems(flsp_batch* b) {
+  for (flsp_handle* h : b->h) CU(cudaStreamSynchronize(h->stream));
+  // a common buffer role: move a problem's state where the others' is
+  for (flsp_handle* h : b->h)
+    if (h->cur != b->cur) {
+      CU(cudaMemcpy(h->buf[b->cur], h->buf[h->cur], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice));
+      h->cur = b->cur;
+    }
+  return FLSP_OK;
+}
+
+int batch_enqueue_step(flsp_batch* b) {
+  ST(launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvBegin, 0.0));
+  const int x = b->cur, y = (x + 1) % 3, z = (x + 2) % 3;
+  const int thr = b->adv_tile[0] * b->adv_tile[1];
+  auto st = [&](int in, int pn, int out, int k, int comb) {
+    return launch_batch_adv(b->stream, b->prec, b->probs, b->items_adv, b->n_adv, b->grid_adv, thr, b->smem_adv, in,
+                            pn, out, k, comb);
+  };
+  if (b->rk == 1) {
+    ST(st(x, x, y, 0, kRK1));
+    b->cur = y;
+  } else if (b->rk == 2) {
+    ST(st(x, x, y, 0, kRK2a));
+    ST(st(y, x, z, 1, kRK2b));
+    b->cur = z;
+  } else {
+    ST(st(x, x, y, 0, kRK3a));
+    ST(st(y, x, z, 1, kRK3b));
+    ST(st(z, x, y, 2, kRK3c));
+    b->cur = y;
+  }
+  return launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvEnd, 0.0);
+}
+
+int batch_enqueue_reinit(flsp_batch* b, const flsp_reinit_opts* o, bool limiter) {
+  const int n = (int)b->h.size();
+  const int phi0 = b->cur;
+  const int thr = b->hj_tile[0] * b->hj_tile[1];
+  ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjReset, 0.0));
+  ST(launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, thr, b->smem_hj, phi0, phi0, -1,
+                     kHJCflOnly, o->rk_order));
+  for (int k = 0; k < o->n_pseudo_steps; ++k) {
+    ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjBegin, o->cfl_max));
+    const int src = b->cur;
+    const int dst = (src == phi0) ? (phi0 + 1) % 3 : other(src, phi0);
+    ST(launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, thr, b->smem_hj, src, phi0,
+                       dst, kHJStep, o->rk_order));
+    int res = dst;
+    if (limiter) {
+      const int lim = other(dst, phi0);
+      ST(launch_batch_weno(b->stream, b->prec, b->probs, b->items_weno, b->n_weno, b->grid_weno,
+                           kWenoTile[0] * kWenoTile[1], b->smem_weno, dst, lim));
+      res = lim;
+    }
+    b->cur = res;
+    ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjEnd, 0.0));
+  }
+  return FLSP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void flsp_batch_destroy(flsp_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_free_plan(b);
+  for (flsp_handle* h : b->h) flsp_destroy(h);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int flsp_batch_create(int n, const flsp_mesh_desc* meshes, const flsp_dg_opts* opts, flsp_batch** out) {
+  if (!out || !meshes || !opts) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *out = nullptr;
+  if (n < 1 || n > (1 << 20)) return fail(FLSP_ERR_BAD_ARG, "bad batch size");
+  for (int i = 0; i < n; ++i) {
+    if (meshes[i].dim != 2) return fail(FLSP_ERR_UNSUPPORTED, "batched problems are 2D");
+    if (opts[i].basis != FLSP_BASIS_Q) return fail(FLSP_ERR_UNSUPPORTED, "batched problems use the Q basis");
+    if (opts[i].precision != opts[0].precision || opts[i].rk_order != opts[0].rk_order ||
+        opts[i].device != opts[0].device)
+      return fail(FLSP_ERR_BAD_ARG, "batched problems share precision, RK order and device");
+  }
+  flsp_batch* b = new flsp_batch();
+  std::memset(&b->tuning, 0, sizeof(b->tuning));
+  b->dev = opts[0].device;
+  b->prec = opts[0].precision;
+  b->rk = opts[0].rk_order;
+  for (int i = 0; i < n; ++i) {
+    flsp_handle* h = nullptr;
+    const int st = flsp_create(&meshes[i], &opts[i], &h);
+    if (st) {
+      flsp_batch_destroy(b);
+      return st;
+    }
+    b->h.push_back(h);
+  }
+  if (cudaSetDevice(b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    flsp_batch_destroy(b);
+    return fail(FLSP_ERR_CUDA, "batch stream creation failed");
+  }
+  *out = b;
+  return FLSP_OK;
+}
+
+int flsp_batch_size(const flsp_batch* b, int* n) {
+  if (!b || !n) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *n = (int)b->h.size();
+  return FLSP_OK;
+}
+
+int flsp_batch_problem(flsp_batch* b, int i, flsp_handle** h) {
+  if (!b || !h) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (i < 0 || i >= (int)b->h.size()) return fail(FLSP_ERR_BAD_ARG, "problem index out of range");
+  *h = b->h[(size_t)i];
+  return FLSP_OK;
+}
+
+int flsp_batch_autotune(flsp_batch* b, flsp_batch_tuning* out) {
+  if (!b) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  CU(cudaSetDevice(b->dev));
+  for (flsp_handle* h : b->h)
+    if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set for every problem");
+  ST(batch_sync_problems(b));
+  static const int ca[][3] = {{32, 8, 1}, {16, 16, 1}, {16, 8, 1}, {8, 8, 1}};
+  static const int ch[][3] = {{16, 8, 1}, {8, 16, 1}, {8, 8, 1}};
+  flsp_batch_tuning t;
+  std::memset(&t, 0, sizeof(t));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  auto time_it = [&](auto&& launch, double* ms) -> int {
+    for (int r = 0; r < 2; ++r) ST(launch());
+    CU(cudaEventRecord(e0, b->stream));
+    const int reps = 5;
+    for (int r = 0; r < reps; ++r) ST(launch());
+    CU(cudaEventRecord(e1, b->stream));
+    CU(cudaEventSynchronize(e1));
+    float f = 0.0f;
+    CU(cudaEventElapsedTime(&f, e0, e1));
+    *ms = f / reps;
+    return FLSP_OK;
+  };
+  // the stage: clock set-up at the current time (harmless: the step's own
+  // set-up recomputes it), the first RK stage into a free buffer
+  double best = 1e300;
+  int bi = 0;
+  for (int c = 0; c < 4; ++c) {
+    ST(batch_build(b, ca[c], ch[0]));
+    ST(launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvBegin, 0.0));
+    const int x = b->cur, y = (x + 1) % 3;
+    double ms = 0.0;
+    ST(time_it([&]() {
+      return launch_batch_adv(b->stream, b->prec, b->probs, b->items_adv, b->n_adv, b->grid_adv, ca[c][0] * ca[c][1],
+                              b->smem_adv, x, x, y, 0, kRK3a);
+    }, &ms));
+    t.adv_cand[c][0] = ca[c][0];
+    t.adv_cand[c][1] = ca[c][1];
+    t.adv_ms[c] = ms;
+    if (ms < best) { best = ms; bi = c; }
+  }
+  t.n_adv = 4;
+  // the reinit step: the CFL pass (reads the state, writes only the clock's
+  // CFL slot, which every reinit resets)
+  best = 1e300;
+  int bj = 0;
+  for (int c = 0; c < 3; ++c) {
+    ST(batch_build(b, ca[bi], ch[c]));
+    const int x = b->cur;
+    double ms = 0.0;
+    ST(time_it([&]() {
+      return launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, ch[c][0] * ch[c][1],
+                             b->smem_hj, x, x, -1, kHJCflOnly, 1);
+    }, &ms));
+    t.hj_cand[c][0] = ch[c][0];
+    t.hj_cand[c][1] = ch[c][1];
+    t.hj_ms[c] = ms;
+    if (ms < best) { best = ms; bj = c; }
+  }
+  t.n_hj = 3;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ST(batch_build(b, ca[bi], ch[bj]));
+  t.adv_tile[0] = ca[bi][0];
+  t.adv_tile[1] = ca[bi][1];
+  t.hj_tile[0] = ch[bj][0];
+  t.hj_tile[1] = ch[bj][1];
+  b->tuning = t;
+  b->tuned = true;
+  if (out) *out = t;
+  return FLSP_OK;
+}
+
+int flsp_batch_run_steps(flsp_batch* b, const flsp_ls_opts* o, int n_steps) {
+  if (!b || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n_steps < 0 || o->reinit_frequency < 1) return fail(FLSP_ERR_BAD_ARG, "bad step counts");
+  const flsp_reinit_opts ro = o->reinit;
+  if (o->execute_reinit) {
+    if (ro.mode != FLSP_REINIT_FIXED) return fail(FLSP_ERR_BAD_ARG, "batched reinit is fixed-count (FLSP_REINIT_FIXED)");
+    if (ro.viscosity != 0.0 || ro.narrow_band) return fail(FLSP_ERR_UNSUPPORTED, "batched reinit: no viscosity, no narrow band");
+    ST(validate_reinit(b->h[0], &ro));
+  }
+  CU(cudaSetDevice(b->dev));
+  if (!b->tuned) ST(flsp_batch_autotune(b, nullptr));
+  ST(batch_sync_problems(b));
+  const bool limiter = ro.limiter != 0;   // 2D: on unless switched off (reinit.cc:475-478)
+  const int n = (int)b->h.size();
+  ST(launch_batch_clock(b->stream, b->probs, n, kBatchAdvHorizon, 0.0));
+  int done = 0;
+  while (done < n_steps) {
+    const int to_reinit = o->execute_reinit ? o->reinit_frequency - b->n_since_reinit : n_steps - done;
+    if (to_reinit <= 0) { b->n_since_reinit = 0; continue; }
+    if (done + to_reinit <= n_steps && o->execute_reinit) {
+      unsigned long long key = 1469598103934665603ull;
+      auto mix = [&](const void* p, size_t nb) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < nb; ++i) { key ^= c[i]; key *= 1099511628211ull; }
+      };
+      mix(&b->cur, sizeof(b->cur));
+      mix(&to_reinit, sizeof(to_reinit));
+      mix(&ro, sizeof(ro));
+      auto it = b->graphs.find(key);
+      if (it == b->graphs.end()) {
+        const int cur0 = b->cur;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int st = FLSP_OK;
+        for (int s2 = 0; s2 < to_reinit && st == FLSP_OK; ++s2) st = batch_enqueue_step(b);
+        if (st == FLSP_OK) st = batch_enqueue_reinit(b, &ro, limiter);
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); b->cur = cur0; return st; }
+        if (ce != cudaSuccess) return fail(FLSP_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+        GraphEntry ge;
+        ge.cur_after = b->cur;
+        b->cur = cur0;
+        CU(cudaGraphInstantiate(&ge.exec, g, 0));
+        cudaGraphDestroy(g);
+        it = b->graphs.emplace(key, ge).first;
+      }
+      CU(cudaGraphLaunch(it->second.exec, b->stream));
+      b->cur = it->second.cur_after;
+      b->n_since_reinit = 0;
+      done += to_reinit;
+    } else {
+      const int k = std::min(to_reinit, n_steps - done);
+      for (int s2 = 0; s2 < k; ++s2) ST(batch_enqueue_step(b));
+      b->n_since_reinit += k;
+      done += k;
+    }
+  }
+  for (flsp_handle* h : b->h) {
+    h->cur = b->cur;
+    h->n_since_reinit = b->n_since_reinit;
+  }
+  return FLSP_OK;
+}
+
+int flsp_batch_sync(flsp_batch* b) {
+  if (!b) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  CU(cudaSetDevice(b->dev));
+  CU(cudaStreamSynchronize(b->stream));
+  for (flsp_handle* h : b->h) ST(sync_clock(h));
+  return FLSP_OK;
+}
+
+int flsp_batch_stream(const flsp_batch* b, void** stream) {
+  if (!b || !stream) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *stream = (void*)b->stream;
   return FLSP_OK;
 }
 

@@ -190,14 +190,16 @@ struct TileCoord {
   int ox, oy, oz;     // tile origin
 };
 
-// a block of a narrow-band launch with no tile to serve (uniform per block)
-__device__ __forceinline__ bool tile_inactive(const MeshArgs& m) {
-  return m.tiles != nullptr && (int)blockIdx.x >= *m.n_tiles;
+// a launch slot (the block index of a plain launch, a work item of a
+// persistent one) with no tile to serve in a narrow-band launch (uniform per block)
+__device__ __forceinline__ bool tile_inactive(const MeshArgs& m, int slot) {
+  return m.tiles != nullptr && slot >= *m.n_tiles;
 }
 
-__device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim) {
+// tile of launch slot `slot` and this thread's cell in it
+__device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim, int slot) {
   TileCoord c;
-  int b = m.tiles ? m.tiles[blockIdx.x] : (int)blockIdx.x;
+  int b = m.tiles ? m.tiles[slot] : slot;
   const int bx = b % m.ntile[0];
   b /= m.ntile[0];
   const int by = dim > 1 ? b % m.ntile[1] : 0;
@@ -217,6 +219,9 @@ __device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim) {
             c.gy < m.n[1] && c.gz < m.n[2];
   return c;
 }
+
+__device__ __forceinline__ bool tile_inactive(const MeshArgs& m) { return tile_inactive(m, (int)blockIdx.x); }
+__device__ __forceinline__ TileCoord tile_coord(const MeshArgs& m, int dim) { return tile_coord(m, dim, (int)blockIdx.x); }
 
 // padded smem box (tile + 1 halo layer per axis, edge/corner slots unused)
 __device__ __forceinline__ int box_index(const MeshArgs& m, int dim, int lx, int ly, int lz) {

@@ -103,7 +103,7 @@ __device__ __forceinline__ void vertex_eval(const T* c, const T* x0, const T* x1
 }
 
 template <int DIM, int P, typename T>
-__global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
+__device__ __forceinline__ void hjq_tile(const HJArgs<T>& a, int slot) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NV = 1 << DIM;
   constexpr int NF = ipow(N1, DIM - 1), NQF = ipow(NQ, DIM - 1), NC = 1 << (DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
   T* jn = c0s + (size_t)ntp * NM;           // [2*DIM*NQF][nt]
   double* red = align16<double>(jn + (size_t)nt * 2 * DIM * NQF);
   const Tab1D<T>& tb = tab<T>(P);
-  if (tile_inactive(m)) return;
-  const TileCoord tc = tile_coord(m, DIM);
+  if (tile_inactive(m, slot)) return;
+  const TileCoord tc = tile_coord(m, DIM, slot);
 
   load_box<DIM, NM>(m, a.phi, box, tc.ox, tc.oy, tc.oz, true);
   load_tile<DIM, NM>(m, a.phi0, c0s, tc.ox, tc.oy, tc.oz, true, ntp);
@@ -451,6 +451,11 @@ __global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
   }
   __syncthreads();
   store_tile<DIM, NM>(m, sb, a.out, tc.ox, tc.oy, tc.oz);
+}
+
+template <int DIM, int P, typename T>
+__global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
+  hjq_tile<DIM, P, T>(a, (int)blockIdx.x);
 }
 
 }  // namespace flsp

@@ -1,0 +1,226 @@
+// flsp_k_batch.cu — batched problems: many independent 2D level-set
+// problems (their own meshes, degrees 1..3, velocities and clocks) advance
+// in ONE persistent launch per RK stage (and one per reinit pseudo-step and
+// limiter pass).  A block walks a list of work items (problem, tile) and
+// runs the same per-tile bodies as the single-problem kernels
+// (adv_stage_tile, hjq_tile, weno_tile), switching on the item's degree.
+// The tile shapes are launch parameters picked by the batch autotuner.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "flsp_advect.cuh"
+#include "flsp_clock.cuh"
+#include "flsp_hjq.cuh"
+#include "flsp_launch.h"
+#include "flsp_tables.h"
+#include "flsp_weno.cuh"
+
+namespace flsp {
+
+int upload_tables_batch() {
+  cudaError_t e = upload_tables_here();
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
+  return FLSP_OK;
+}
+
+namespace {
+
+// per-item argument structs are assembled in local memory from the
+// problem's descriptor and the launch's buffer roles
+template <typename T>
+__device__ __forceinline__ void make_adv_args(const BatchProb& pr, int ix, int in_n, int iout, int stage, int combine,
+                                              AdvArgs<T>& a) {
+  a.m = pr.m_adv;
+  a.v.vtab = reinterpret_cast<const T*>(pr.vtab);
+  a.v.n_terms = pr.n_terms;
+  a.v.nmax = pr.nmax;
+  a.v.npt = pr.npt;
+#pragma unroll 1
+  for (int k = 0; k < kMaxTerms; ++k) a.v.comp[k] = pr.comp[k];
+  a.phi_s = reinterpret_cast<const T*>(pr.buf[ix]);
+  a.phi_n = reinterpret_cast<const T*>(pr.buf[in_n]);
+  a.out = reinterpret_cast<T*>(pr.buf[iout]);
+  a.clk = pr.clk;
+  a.stage = stage;
+  a.combine = combine;
+  a.ct_explicit = 0.0;
+  a.dt_explicit = 0.0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2)
+    batch_adv_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int ix,
+                     int in_n, int iout, int stage, int combine) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int2 w = items[it];
+    AdvArgs<T> a;
+    make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
+    switch (probs[w.x].p) {
+      case 1: adv_stage_tile<2, 1, T>(a, w.y); break;
+      case 2: adv_stage_tile<2, 2, T>(a, w.y); break;
+      default: adv_stage_tile<2, 3, T>(a, w.y); break;
+    }
+    __syncthreads();   // shared memory is reused by the next item
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+    batch_hj_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int isrc,
+                    int iphi0, int idst, int mode, int rk) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int2 w = items[it];
+    const BatchProb& pr = probs[w.x];
+    HJArgs<T> a;
+    a.m = pr.m_hj;
+    a.phi = reinterpret_cast<const T*>(pr.buf[isrc]);
+    a.phi0 = reinterpret_cast<const T*>(pr.buf[iphi0]);
+    a.out = idst >= 0 ? reinterpret_cast<T*>(pr.buf[idst]) : nullptr;
+    a.clk = pr.clk;
+    a.mode = mode;
+    a.rk = rk;
+    a.dt_explicit = 0.0;
+    a.block = pr.m_hj.ncell * pr.m_hj.nb;
+    a.rdiff = nullptr;
+    switch (pr.p) {
+      case 1: hjq_tile<2, 1, T>(a, w.y); break;
+      case 2: hjq_tile<2, 2, T>(a, w.y); break;
+      default: hjq_tile<2, 3, T>(a, w.y); break;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    batch_weno_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int iin,
+                      int iout) {
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int2 w = items[it];
+    const BatchProb& pr = probs[w.x];
+    WenoArgs<T> a;
+    a.m = pr.m_weno;
+    a.in = reinterpret_cast<const T*>(pr.buf[iin]);
+    a.out = reinterpret_cast<T*>(pr.buf[iout]);
+    a.count = nullptr;
+    switch (pr.p) {
+      case 1: weno_tile<1, T>(a, w.y); break;
+      case 2: weno_tile<2, T>(a, w.y); break;
+      default: weno_tile<3, T>(a, w.y); break;
+    }
+    __syncthreads();
+  }
+}
+
+// clocks: one thread per problem
+__global__ void batch_clock_kernel(const BatchProb* __restrict__ probs, int n, int what, double cfl_max) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BatchProb& pr = probs[i];
+  switch (what) {
+    case kBatchAdvBegin: adv_clock_begin_body(pr.clk, pr.ca); break;
+    case kBatchAdvEnd: adv_clock_end_body(pr.clk); break;
+    case kBatchAdvHorizon: adv_clock_horizon_body(pr.clk, __longlong_as_double(0x7ff0000000000000LL)); break;
+    case kBatchHjReset: hj_clock_reset_body(pr.clk); break;
+    case kBatchHjBegin: hj_clock_begin_body(pr.clk, cfl_max, pr.p, 0.0, pr.m_hj.min_diam, pr.adv_scale); break;
+    default: hj_clock_end_body(pr.clk); break;
+  }
+}
+
+template <typename K>
+int persistent_grid(K kern, int threads, size_t smem, int n_items) {
+  int per_sm = 0, dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return std::max(1, std::min(n_items, nsm * per_sm));
+}
+
+}  // namespace
+
+int batch_smem(int kind, int p, int prec, const int* tile, int n_terms, size_t* bytes) {
+  auto go = [&](auto tz) -> size_t {
+    using T = decltype(tz);
+    if (kind == kBatchKindAdv) {
+      switch (p) {
+        case 1: return adv_smem_bytes<2, 1, T>(tile, std::max(n_terms, 1));
+        case 2: return adv_smem_bytes<2, 2, T>(tile, std::max(n_terms, 1));
+        default: return adv_smem_bytes<2, 3, T>(tile, std::max(n_terms, 1));
+      }
+    } else if (kind == kBatchKindHJ) {
+      switch (p) {
+        case 1: return hjq_smem_bytes<2, 1, T>(tile);
+        case 2: return hjq_smem_bytes<2, 2, T>(tile);
+        default: return hjq_smem_bytes<2, 3, T>(tile);
+      }
+    }
+    switch (p) {
+      case 1: return weno_smem_bytes<1, T>(tile);
+      case 2: return weno_smem_bytes<2, T>(tile);
+      default: return weno_smem_bytes<3, T>(tile);
+    }
+  };
+  *bytes = prec == FLSP_FP64 ? go((double)0) : go((float)0);
+  return FLSP_OK;
+}
+
+int launch_batch_clock(cudaStream_t s, const BatchProb* probs, int n, int what, double cfl_max) {
+  batch_clock_kernel<<<(n + 127) / 128, 128, 0, s>>>(probs, n, what, cfl_max);
+  return launch_status("batch_clock_kernel");
+}
+
+template <typename T>
+static int batch_attr(int kind, size_t smem) {
+  cudaError_t e = cudaSuccess;
+  const int s = (int)smem;
+  if (kind == kBatchKindAdv) e = cudaFuncSetAttribute(batch_adv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  else if (kind == kBatchKindHJ) e = cudaFuncSetAttribute(batch_hj_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  else e = cudaFuncSetAttribute(batch_weno_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("batch attr: ") + cudaGetErrorString(e));
+  return FLSP_OK;
+}
+
+int batch_prepare(int kind, int prec, size_t smem, int threads, int n_items, int* grid) {
+  if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "batch tile too large for shared memory");
+  int st = prec == FLSP_FP64 ? batch_attr<double>(kind, smem) : batch_attr<float>(kind, smem);
+  if (st) return st;
+  auto g = [&](auto tz) -> int {
+    using T = decltype(tz);
+    if (kind == kBatchKindAdv) return persistent_grid(batch_adv_kernel<T>, threads, smem, n_items);
+    if (kind == kBatchKindHJ) return persistent_grid(batch_hj_kernel<T>, threads, smem, n_items);
+    return persistent_grid(batch_weno_kernel<T>, threads, smem, n_items);
+  };
+  *grid = prec == FLSP_FP64 ? g((double)0) : g((float)0);
+  return FLSP_OK;
+}
+
+int launch_batch_adv(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                     int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine) {
+  if (prec == FLSP_FP64)
+    batch_adv_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
+  else
+    batch_adv_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
+  return launch_status("batch_adv_kernel");
+}
+
+int launch_batch_hj(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                    int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk) {
+  if (prec == FLSP_FP64)
+    batch_hj_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
+  else
+    batch_hj_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
+  return launch_status("batch_hj_kernel");
+}
+
+int launch_batch_weno(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                      int threads, size_t smem, int iin, int iout) {
+  if (prec == FLSP_FP64)
+    batch_weno_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
+  else
+    batch_weno_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
+  return launch_status("batch_weno_kernel");
+}
+
+}  // namespace flsp

@@ -39,6 +39,36 @@ int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margi
 // out[c] = phi0[c] for cells with flags[c] == 0
 int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags);
 
+// ---------------- batched problems (flsp_k_batch.cu) ----------------
+// one problem of a batch, as the batched kernels see it (2D, Q basis)
+struct BatchProb {
+  MeshArgs m_adv, m_hj, m_weno;   // the batch's tile shapes, no narrow band
+  void* buf[3];                   // state buffers (roles are launch parameters)
+  DevClock* clk;
+  const void* vtab;               // velocity table (state precision)
+  int n_terms, nmax, npt;
+  int comp[kMaxTerms];
+  int p;                          // degree 1..3
+  AdvClockArgs ca;                // advection clock parameters
+  double adv_scale;               // advection CFL scaling of the degree
+};
+enum BatchKernelKind : int { kBatchKindAdv = 0, kBatchKindHJ = 1, kBatchKindWeno = 2 };
+enum BatchClockOp : int {
+  kBatchAdvBegin = 0, kBatchAdvEnd = 1, kBatchAdvHorizon = 2, kBatchHjReset = 3, kBatchHjBegin = 4, kBatchHjEnd = 5
+};
+int upload_tables_batch();
+// shared memory one problem needs for a tile of the given kind
+int batch_smem(int kind, int p, int prec, const int* tile, int n_terms, size_t* bytes);
+// kernel attributes for `smem` and the persistent grid for n_items
+int batch_prepare(int kind, int prec, size_t smem, int threads, int n_items, int* grid);
+int launch_batch_clock(cudaStream_t s, const BatchProb* probs, int n, int what, double cfl_max);
+int launch_batch_adv(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                     int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine);
+int launch_batch_hj(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                    int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk);
+int launch_batch_weno(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
+                      int threads, size_t smem, int iin, int iout);
+
 // restrict a launch's MeshArgs to the narrow-band tile list of `kind`
 inline void apply_band(const Ctx& c, int kind, MeshArgs& m) {
   m.tiles = c.nb_tiles[kind];

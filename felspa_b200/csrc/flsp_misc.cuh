@@ -2,6 +2,7 @@
 // clocks, host<->device DoF order, initial-condition projection, FP64
 // diagnostics reductions, the static part of the advection CFL.
 #pragma once
+#include "flsp_clock.cuh"
 #include "flsp_device.cuh"
 #include "flsp_dg.h"
 
@@ -14,69 +15,30 @@ constexpr double kEpsD = 2.220446049250313e-16;
 // clocks
 // ---------------------------------------------------------------------
 
-// AdvectSimulator::advance_time substep set-up (advection.cc:396-404):
-// CFL estimate at the current time (running maximum, the estimator never
-// resets), substep = min(cfl_max / estimate, remaining), stage time factors.
+// clock kernels: one thread (the updates are in flsp_clock.cuh)
 __global__ void adv_clock_begin(DevClock* c, const AdvClockArgs a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const double ctn = time_factor(a.tkind, a.ta, a.tb, c->t);
-  const double vd = fabs(ctn) * c->vd_static;
-  c->vd_run = fmax(c->vd_run, vd);
-  const double suggest = a.cfl_max / (c->vd_run * a.scale);
-  const double remaining = c->scratch[0] - c->scratch[1];   // time_step - cumulative
-  const double dt = fmin(suggest, remaining);
-  c->dt = dt;
-  c->active = fabs(dt) <= kEpsD ? 0 : 1;   // TempoIntegrator skips zero steps
-  c->ct[0] = ctn;
-  c->ct[1] = time_factor(a.tkind, a.ta, a.tb, c->t + dt);
-  c->ct[2] = time_factor(a.tkind, a.ta, a.tb, c->t + 0.5 * dt);
+  adv_clock_begin_body(c, a);
 }
-
 __global__ void adv_clock_end(DevClock* c) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (c->active) {
-    c->t += c->dt;
-    c->n_substeps += 1;
-  }
-  c->scratch[1] += c->dt;   // cumulative time of this advance call
+  adv_clock_end_body(c);
 }
-
-// start an advance call of length time_step (scratch[0]); +inf = unclamped
 __global__ void adv_clock_horizon(DevClock* c, double time_step) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  c->scratch[0] = time_step;
-  c->scratch[1] = 0.0;
+  adv_clock_horizon_body(c, time_step);
 }
-
 __global__ void hj_clock_reset(DevClock* c) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  c->hj_vd_run = 0.0;
-  c->hj_dt = 0.0;
-  c->hj_cum = 0.0;
-  c->hj_vd_bits = 0ull;
-  c->hj_iter = 0;
+  hj_clock_reset_body(c);
 }
-
-// ReinitSimulatorLDG::advance_time step size (reinit.cc:396-408) with
-// HJSimulator::cfl_scaling (hamilton_jacobi.cc:554-580)
-__global__ void hj_clock_begin(DevClock* c, double cfl_max, int p, double nu, double min_diam,
-                               double adv_scale) {
+__global__ void hj_clock_begin(DevClock* c, double cfl_max, int p, double nu, double min_diam, double adv_scale) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const double vd = __longlong_as_double((long long)c->hj_vd_bits);
-  c->hj_vd_bits = 0ull;
-  c->hj_vd_run = fmax(c->hj_vd_run, vd);
-  double scale;
-  if (nu > 0.0)
-    scale = pow((double)(p + 1), 2.0) * c->hj_vd_run + nu * pow((double)(p + 1), 4.0) / pow(min_diam, 2.0);
-  else
-    scale = adv_scale * c->hj_vd_run;
-  c->hj_dt = cfl_max / scale;
+  hj_clock_begin_body(c, cfl_max, p, nu, min_diam, adv_scale);
 }
-
 __global__ void hj_clock_end(DevClock* c) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  c->hj_cum += c->hj_dt;
-  c->hj_iter += 1;
+  hj_clock_end_body(c);
 }
 
 // ---------------------------------------------------------------------

@@ -54,14 +54,14 @@ __device__ __forceinline__ void legendre_at(T x, T* v, T* d, T* dd) {
 }
 
 template <int P, typename T>
-__global__ void __launch_bounds__(256) weno_kernel(const WenoArgs<T> a) {
+__device__ __forceinline__ void weno_tile(const WenoArgs<T>& a, int slot) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = N1 * N1, NQV = NQ * NQ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* box = reinterpret_cast<T*>(smem_raw);
   const MeshArgs& m = a.m;
   const Tab1D<T>& tb = tab<T>(P);
-  if (tile_inactive(m)) return;
-  const TileCoord tc = tile_coord(m, 2);
+  if (tile_inactive(m, slot)) return;
+  const TileCoord tc = tile_coord(m, 2, slot);
   load_box<2, NM>(m, a.in, box, tc.ox, tc.oy, 0, true);
   cp_async_wait_all();
   __syncthreads();
@@ -245,6 +245,11 @@ __global__ void __launch_bounds__(256) weno_kernel(const WenoArgs<T> a) {
     }
   }
   for (int k = 0; k < m.nb; ++k) a.out[cell * m.nb + k] = outc[m.g2q[k]];
+}
+
+template <int P, typename T>
+__global__ void __launch_bounds__(256) weno_kernel(const WenoArgs<T> a) {
+  weno_tile<P, T>(a, (int)blockIdx.x);
 }
 
 }  // namespace flsp

@@ -108,9 +108,29 @@ class Problem:
         check(L.flsp_dofs_per_cell(h, C.byref(nb)))
         self.dofs_per_cell = nb.value
 
+    @classmethod
+    def wrap(cls, handle, mesh, fe_degree, basis, precision):
+        """A Problem view of a handle owned elsewhere (a batch member)."""
+        self = cls.__new__(cls)
+        self.mesh = mesh
+        self.fe_degree = fe_degree
+        self.basis = basis
+        self.precision = precision
+        self._mdesc = mesh.desc()
+        self.h = handle
+        self._owned = False
+        n = C.c_int64(0)
+        check(load().flsp_n_dofs(handle, C.byref(n)))
+        self.n_dofs = n.value
+        nb = C.c_int(0)
+        check(load().flsp_dofs_per_cell(handle, C.byref(nb)))
+        self.dofs_per_cell = nb.value
+        return self
+
     def close(self):
         if getattr(self, "h", None):
-            load().flsp_destroy(self.h)
+            if getattr(self, "_owned", True):
+                load().flsp_destroy(self.h)
             self.h = None
 
     def __del__(self):

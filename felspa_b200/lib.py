@@ -68,6 +68,14 @@ PROTOTYPES = {
     "flsp_reinit_learned": (C.c_int, [_vp, _vp, C.POINTER(abi.LearnedOpts), C.POINTER(abi.LearnedStats)]),
     "flsp_default_train_opts": (None, [C.POINTER(abi.TrainOpts)]),
     "flsp_default_learned_opts": (None, [C.POINTER(abi.LearnedOpts)]),
+    "flsp_batch_create": (C.c_int, [C.c_int, C.POINTER(abi.MeshDesc), C.POINTER(abi.DGOpts), C.POINTER(_vp)]),
+    "flsp_batch_destroy": (None, [_vp]),
+    "flsp_batch_size": (C.c_int, [_vp, _ip]),
+    "flsp_batch_problem": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "flsp_batch_autotune": (C.c_int, [_vp, C.POINTER(abi.BatchTuning)]),
+    "flsp_batch_run_steps": (C.c_int, [_vp, C.POINTER(abi.LSOpts), C.c_int]),
+    "flsp_batch_sync": (C.c_int, [_vp]),
+    "flsp_batch_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
 }
 
 

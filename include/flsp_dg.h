@@ -382,6 +382,42 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
 void flsp_default_train_opts(flsp_train_opts* o);
 void flsp_default_learned_opts(flsp_learned_opts* o);
 
+/* ------------------------------------------------------------------
+   Batched problems (no counterpart in the reference, where one simulator
+   object holds one problem).  Many independent 2D Q-basis problems (own
+   meshes, degrees 1..3, velocities, ICs and clocks; one precision and RK
+   order) advance together: one persistent launch per RK stage and per
+   reinit pseudo-step covers every problem, a reinit period is replayed from
+   a captured CUDA graph, and the tile shapes come from flsp_batch_autotune
+   (run on first use if not called).  Problem i is a regular handle
+   (flsp_batch_problem) for set-up, state exchange and reductions; the
+   batch owns it.
+   ------------------------------------------------------------------ */
+typedef struct flsp_batch flsp_batch;
+
+typedef struct flsp_batch_tuning {
+  int adv_tile[2];          /* chosen advection-stage tile (cells x, y)    */
+  int hj_tile[2];           /* chosen reinit-step tile                     */
+  int n_adv, n_hj;          /* candidates timed                            */
+  int adv_cand[8][2];
+  int hj_cand[8][2];
+  double adv_ms[8];         /* ms per batched launch of each candidate     */
+  double hj_ms[8];
+} flsp_batch_tuning;
+
+int flsp_batch_create(int n, const flsp_mesh_desc* meshes, const flsp_dg_opts* opts,
+                      flsp_batch** out);
+void flsp_batch_destroy(flsp_batch* b);
+int flsp_batch_size(const flsp_batch* b, int* n);
+int flsp_batch_problem(flsp_batch* b, int i, flsp_handle** h);
+int flsp_batch_autotune(flsp_batch* b, flsp_batch_tuning* out);
+/* n_steps substeps of every problem with a fixed-count reinit every
+   reinit_frequency steps (no viscosity, no narrow band); enqueued, returns
+   without waiting */
+int flsp_batch_run_steps(flsp_batch* b, const flsp_ls_opts* o, int n_steps);
+int flsp_batch_sync(flsp_batch* b);
+int flsp_batch_stream(const flsp_batch* b, void** stream);
+
 /* default option structs (reference defaults) */
 void flsp_default_dg_opts(flsp_dg_opts* o);
 void flsp_default_reinit_opts(flsp_reinit_opts* o);

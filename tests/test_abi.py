@@ -42,11 +42,12 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "flsp_dg.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(flsp_mesh_desc),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(flsp_mesh_desc),
          sizeof(flsp_dg_opts), sizeof(flsp_factor), sizeof(flsp_vel_term), sizeof(flsp_velocity_desc),
          sizeof(flsp_ic_node), sizeof(flsp_ic_desc), sizeof(flsp_reinit_opts), sizeof(flsp_ls_opts),
          offsetof(flsp_ic_desc, waves), sizeof(flsp_train_opts), sizeof(flsp_learned_opts),
-         offsetof(flsp_learned_opts, fallback), sizeof(flsp_learned_stats));
+         offsetof(flsp_learned_opts, fallback), sizeof(flsp_learned_stats), sizeof(flsp_batch_tuning),
+         offsetof(flsp_batch_tuning, adv_ms));
   return 0;
 }
 """
@@ -60,7 +61,8 @@ int main(void) {
     mine = [C.sizeof(abi.MeshDesc), C.sizeof(abi.DGOpts), C.sizeof(abi.Factor), C.sizeof(abi.VelTerm),
             C.sizeof(abi.VelocityDesc), C.sizeof(abi.ICNode), C.sizeof(abi.ICDesc), C.sizeof(abi.ReinitOpts),
             C.sizeof(abi.LSOpts), abi.ICDesc.waves.offset, C.sizeof(abi.TrainOpts), C.sizeof(abi.LearnedOpts),
-            abi.LearnedOpts.fallback.offset, C.sizeof(abi.LearnedStats)]
+            abi.LearnedOpts.fallback.offset, C.sizeof(abi.LearnedStats), C.sizeof(abi.BatchTuning),
+            abi.BatchTuning.adv_ms.offset]
     assert vals == mine
 
 
