@@ -96,3 +96,68 @@ def make_batch(instances, precision=abi.FP32, cfl_max=0.1):
         pb.set_velocity(d["velocity"])
         pb.project(d["ic"])
     return b
+
+
+def config3_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, compare_problems=32, compare_steps=50):
+    """Batched configuration: DoF-steps/s of the whole batch (device time of
+    `steps` steps with a reinit every `reinit_every`, CUDA events on the batch
+    stream) and the autotuner's report; on a subset, for comparison, the same
+    problems issued one after the other, each in its own graph-replayed run
+    on its own stream (so that they overlap on the GPU)."""
+    import time
+    import torch
+    from .lib import check, load
+    ctl = abi.default_ls_opts(reinit_frequency=reinit_every,
+                              reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=n_pseudo))
+    inst = config3_instances(n_problems)
+    b = make_batch(inst, precision=abi.FP32)
+    t0 = time.perf_counter()
+    tune = b.autotune()
+    t_tune = time.perf_counter() - t0
+    b.run_steps(reinit_every, ctl)          # warm-up period (captures the graph)
+    s = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    b.run_steps(steps, ctl, sync=False)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    b.sync()
+    finite = all(np.all(np.isfinite(p.get_state())) for p in b.problems[:16])
+    n_dofs = b.n_dofs
+    b.close()
+    # the same problems one by one (subset), each its own graph-replayed run
+    sub = inst[:compare_problems]
+    singles = []
+    for d in sub:
+        pb = Problem(Mesh(2, (d["n"], d["n"])), d["degree"], basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+        pb.set_velocity(d["velocity"])
+        pb.project(d["ic"])
+        check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), reinit_every))
+        pb.sync()
+        singles.append(pb)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for pb in singles:
+        check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), compare_steps))
+    for pb in singles:
+        pb.sync()
+    t_single = time.perf_counter() - t0
+    sub_dofs = sum(pb.n_dofs for pb in singles)
+    for pb in singles:
+        pb.close()
+    bs = make_batch(sub, precision=abi.FP32)
+    bs.run_steps(reinit_every, ctl)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bs.run_steps(compare_steps, ctl)
+    t_batch_sub = time.perf_counter() - t0
+    bs.close()
+    return {"problems": n_problems, "n_dofs": n_dofs, "steps": steps, "reinit_every": reinit_every,
+            "pseudo_steps": n_pseudo, "device_ms": ms, "dof_steps_per_s": n_dofs * steps / (ms * 1e-3),
+            "autotune": tune, "autotune_s": t_tune, "finite": bool(finite),
+            "subset_one_by_one": {"problems": compare_problems, "steps": compare_steps,
+                                  "one_by_one_s": t_single, "batched_s": t_batch_sub,
+                                  "one_by_one_dof_steps_per_s": sub_dofs * compare_steps / t_single,
+                                  "batched_dof_steps_per_s": sub_dofs * compare_steps / t_batch_sub}}

@@ -246,8 +246,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   // velocity component `comp` (times the time factor) at table columns
   auto vel = [&](int comp, int jx, int jy, int jz) -> T {
     T u = T(0);
-    for (int k = 0; k < nterm; ++k) {
-      if (a.v.comp[k] != comp) continue;
+    for (int k = a.v.cstart[comp]; k < a.v.cstart[comp + 1]; ++k) {
       T v = vrow(k, 0)[jx] * vrow(k, 1)[jy];
       if constexpr (DIM == 3) v = v * vrow(k, 2)[jz];
       u += v;

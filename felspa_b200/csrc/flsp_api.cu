@@ -467,7 +467,13 @@ void layout_velocity(flsp_handle* h) {
   bool sep = true;
   for (int d = 0; d < h->dim; ++d) sep = sep && count[d] <= 1;
   h->vel_dev = v;
-  if (!sep) return;
+  if (!sep) {
+    // terms grouped by component (stable: each component keeps its own
+    // order, so its sum is formed in the same order)
+    std::stable_sort(h->vel_dev.terms, h->vel_dev.terms + h->vel_dev.n_terms,
+                     [](const flsp_vel_term& x, const flsp_vel_term& y) { return x.comp < y.comp; });
+    return;
+  }
   flsp_velocity_desc r = v;
   r.n_terms = h->dim;
   for (int d = 0; d < h->dim; ++d) {
@@ -1375,6 +1381,19 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
     ST(batch_smem(kBatchKindWeno, h->p, b->prec, kWenoTile, 0, &x));
     sw = std::max(sw, x);
   }
+  // most expensive items first (higher degree, more velocity terms): blocks
+  // take items round-robin, so the long ones spread over the whole grid and
+  // the short ones fill in at the end
+  auto by_cost = [&](std::vector<int2>& it) {
+    std::stable_sort(it.begin(), it.end(), [&](const int2& x, const int2& y) {
+      const long long cx = (long long)pr[(size_t)x.x].p * 64 + pr[(size_t)x.x].n_terms;
+      const long long cy = (long long)pr[(size_t)y.x].p * 64 + pr[(size_t)y.x].n_terms;
+      return cx > cy;
+    });
+  };
+  by_cost(ia);
+  by_cost(ih);
+  by_cost(iw);
   CU(cudaMalloc(&b->probs, sizeof(BatchProb) * (size_t)n));
   CU(cudaMalloc(&b->items_adv, sizeof(int2) * ia.size()));
   CU(cudaMalloc(&b->items_hj, sizeof(int2) * ih.size()));

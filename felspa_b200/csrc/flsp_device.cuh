@@ -174,7 +174,17 @@ struct VelArgs {
   int nmax;
   int npt;
   int comp[kMaxTerms];
+  int cstart[4];   // terms of component c: [cstart[c], cstart[c+1]) (terms sorted by component)
 };
+
+// first term of each component in a component-sorted term list
+__host__ __device__ inline void term_ranges(const int* comp, int n_terms, int* cstart) {
+  for (int c = 0; c < 4; ++c) {
+    int k = 0;
+    while (k < n_terms && comp[k] < c) ++k;
+    cstart[c] = k;
+  }
+}
 
 // next 16-byte aligned address at or after p (shared-memory sub-buffers)
 template <typename U>

@@ -98,6 +98,7 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     a.v.nmax = v.nmax;
     a.v.npt = v.npt;
     for (int k = 0; k < v.n_terms; ++k) a.v.comp[k] = v.comp[k];
+    term_ranges(a.v.comp, v.n_terms, a.v.cstart);
     a.phi_s = reinterpret_cast<const T*>(in);
     a.phi_n = reinterpret_cast<const T*>(phin);
     a.out = reinterpret_cast<T*>(out);

@@ -26,8 +26,8 @@ int upload_tables_batch() {
 
 namespace {
 
-// per-item argument structs are assembled in local memory from the
-// problem's descriptor and the launch's buffer roles
+// per-item argument structs are assembled (in shared memory, by one
+// thread) from the problem's descriptor and the launch's buffer roles
 template <typename T>
 __device__ __forceinline__ void make_adv_args(const BatchProb& pr, int ix, int in_n, int iout, int stage, int combine,
                                               AdvArgs<T>& a) {
@@ -38,6 +38,7 @@ __device__ __forceinline__ void make_adv_args(const BatchProb& pr, int ix, int i
   a.v.npt = pr.npt;
 #pragma unroll 1
   for (int k = 0; k < kMaxTerms; ++k) a.v.comp[k] = pr.comp[k];
+  term_ranges(pr.comp, pr.n_terms, a.v.cstart);
   a.phi_s = reinterpret_cast<const T*>(pr.buf[ix]);
   a.phi_n = reinterpret_cast<const T*>(pr.buf[in_n]);
   a.out = reinterpret_cast<T*>(pr.buf[iout]);
@@ -52,11 +53,18 @@ template <typename T>
 __global__ void __launch_bounds__(256, 2)
     batch_adv_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int ix,
                      int in_n, int iout, int stage, int combine) {
+  // the item's arguments are assembled once per block in shared memory
+  // (every thread reads them, like a plain launch's kernel parameters)
+  __shared__ AdvArgs<T> a;
+  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
-    AdvArgs<T> a;
-    make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
-    switch (probs[w.x].p) {
+    if (threadIdx.x == 0) {
+      make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
+      pdeg = probs[w.x].p;
+    }
+    __syncthreads();
+    switch (pdeg) {
       case 1: adv_stage_tile<2, 1, T>(a, w.y); break;
       case 2: adv_stage_tile<2, 2, T>(a, w.y); break;
       default: adv_stage_tile<2, 3, T>(a, w.y); break;
@@ -69,21 +77,26 @@ template <typename T>
 __global__ void __launch_bounds__(128)
     batch_hj_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int isrc,
                     int iphi0, int idst, int mode, int rk) {
+  __shared__ HJArgs<T> a;
+  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
-    const BatchProb& pr = probs[w.x];
-    HJArgs<T> a;
-    a.m = pr.m_hj;
-    a.phi = reinterpret_cast<const T*>(pr.buf[isrc]);
-    a.phi0 = reinterpret_cast<const T*>(pr.buf[iphi0]);
-    a.out = idst >= 0 ? reinterpret_cast<T*>(pr.buf[idst]) : nullptr;
-    a.clk = pr.clk;
-    a.mode = mode;
-    a.rk = rk;
-    a.dt_explicit = 0.0;
-    a.block = pr.m_hj.ncell * pr.m_hj.nb;
-    a.rdiff = nullptr;
-    switch (pr.p) {
+    if (threadIdx.x == 0) {
+      const BatchProb& pr = probs[w.x];
+      a.m = pr.m_hj;
+      a.phi = reinterpret_cast<const T*>(pr.buf[isrc]);
+      a.phi0 = reinterpret_cast<const T*>(pr.buf[iphi0]);
+      a.out = idst >= 0 ? reinterpret_cast<T*>(pr.buf[idst]) : nullptr;
+      a.clk = pr.clk;
+      a.mode = mode;
+      a.rk = rk;
+      a.dt_explicit = 0.0;
+      a.block = pr.m_hj.ncell * pr.m_hj.nb;
+      a.rdiff = nullptr;
+      pdeg = pr.p;
+    }
+    __syncthreads();
+    switch (pdeg) {
       case 1: hjq_tile<2, 1, T>(a, w.y); break;
       case 2: hjq_tile<2, 2, T>(a, w.y); break;
       default: hjq_tile<2, 3, T>(a, w.y); break;
@@ -96,15 +109,20 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     batch_weno_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int iin,
                       int iout) {
+  __shared__ WenoArgs<T> a;
+  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
-    const BatchProb& pr = probs[w.x];
-    WenoArgs<T> a;
-    a.m = pr.m_weno;
-    a.in = reinterpret_cast<const T*>(pr.buf[iin]);
-    a.out = reinterpret_cast<T*>(pr.buf[iout]);
-    a.count = nullptr;
-    switch (pr.p) {
+    if (threadIdx.x == 0) {
+      const BatchProb& pr = probs[w.x];
+      a.m = pr.m_weno;
+      a.in = reinterpret_cast<const T*>(pr.buf[iin]);
+      a.out = reinterpret_cast<T*>(pr.buf[iout]);
+      a.count = nullptr;
+      pdeg = pr.p;
+    }
+    __syncthreads();
+    switch (pdeg) {
       case 1: weno_tile<1, T>(a, w.y); break;
       case 2: weno_tile<2, T>(a, w.y); break;
       default: weno_tile<3, T>(a, w.y); break;
