@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="short run for ncu: set-up, 2 reinit periods, no timing loops")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched configuration (256 2D problems, ~30 s)")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-vs-plain reinitialisation comparison (2D, ~1 min)")
     return ap.parse_args()
@@ -333,6 +335,15 @@ def run_ours(args):
     }
     if world == 1 and not args.no_learned:
         line["learned_vs_plain"] = learned_comparison()
+    if world == 1 and not args.no_batched:
+        from felspa_b200.batch import config3_benchmark
+        r = config3_benchmark()
+        line["batched"] = {
+            "workload": "256 independent 2D Q problems, meshes log-uniform 32^2..256^2, degree U{1,2,3}, union of 1-4 "
+                        "circles, 8-mode Fourier stream-function velocity (seeds default_rng(1000+i)), 500 SSP-RK3 "
+                        "steps, fixed 5-pseudo-step reinit every 10, FP32; one persistent launch per RK stage / "
+                        "pseudo-step, periods replayed from CUDA graphs, tiles from the autotuner",
+            **{k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()}}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
