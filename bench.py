@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="short run for ncu: set-up, 2 reinit periods, no timing loops")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the FP64 run of the same periods (accuracy of the FP32 mode)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched configuration (256 2D problems, ~30 s)")
     ap.add_argument("--no-learned", action="store_true",
@@ -275,6 +277,25 @@ def run_ours(args):
         e2e_ms.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
 
+    # FP32 production mode against FP64 on the same periods: L1 interface
+    # difference and area (FP64 device reductions of the FP64 handle)
+    acc64 = None
+    if not args.no_fp64_check:
+        periods = args.warmup + 2 * args.steps
+        s32 = pb.get_state()
+        mass32 = ls.integrate_mass()
+        ls64 = make_problem(abi.FP64, local)
+        ls64.run_steps(periods * REINIT_EVERY)
+        s64 = ls64.problem.get_state()
+        mass64 = ls64.integrate_mass()
+        ls64.problem.set_state(s32)
+        ls64.problem.snapshot()
+        ls64.problem.set_state(s64)
+        acc64 = {"periods": periods, "l1_interface_fp32_vs_fp64": ls64.problem.reduce(abi.RED_L1_INTERFACE),
+                 "area_fp32_vs_fp64_rel": (mass32 - mass64) / mass64,
+                 "max_coeff_diff_rel": float(abs(s32 - s64).max() / abs(s64).max())}
+        ls64.problem.close()
+
     # roofline of the dominant kernel (advection stage), events on the library stream
     ms_stage = pb.time_kernel(0, reps=20)
     ms_hj = pb.time_kernel(1, reps=10)
@@ -331,7 +352,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": 8 * n_dofs, "ms_per_step": e2e_total / args.steps},
         "gpu_launches": per_step_launches * args.steps,
         "clocks": clocks,
-        "accuracy": {"area_rel_change": (area1 - area0) / area0},
+        "accuracy": {"area_rel_change": (area1 - area0) / area0, "fp32_vs_fp64": acc64},
     }
     if world == 1 and not args.no_learned:
         line["learned_vs_plain"] = learned_comparison()
