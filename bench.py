@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP64 run of the same periods (accuracy of the FP32 mode)")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the narrow-band and 128^3 variants of the 3D workload")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched configuration (256 2D problems, ~30 s)")
     ap.add_argument("--no-learned", action="store_true",
@@ -356,6 +358,19 @@ def run_ours(args):
     }
     if world == 1 and not args.no_learned:
         line["learned_vs_plain"] = learned_comparison()
+    if world == 1 and not args.no_variants:
+        from felspa_b200 import fields as F
+        line["variants"] = {
+            "narrow_band_64cubed": {
+                "what": "the headline workload with the compute-restricted narrow band (6 cells) in the reinit",
+                **variant_rate(abi.FP32, local, N_CELLS, F.deformation_3d(), F.sphere((0.35, 0.35, 0.35), 0.15), 10,
+                               narrow_band=1)},
+            "large_128cubed": {
+                "what": "config-5 scale: 128^3 Q2 FP32 (56.6 M DoFs), plume rolls u = curl(0, psi, 0), "
+                        "psi = 0.5 sin(pi x) sin(pi y) sin(pi z)(1 - exp(-t)), perturbed plane z = 0.5 + 0.02 sum of "
+                        "16 cosine modes; plain full-sweep reinit",
+                **variant_rate(abi.FP32, local, 128, F.plume_3d(), F.perturbed_plane(seed=5), 4)},
+        }
     if world == 1 and not args.no_batched:
         from felspa_b200.batch import config3_benchmark
         r = config3_benchmark()
@@ -369,6 +384,39 @@ def run_ours(args):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=0, band_cells=6.0):
+    """DoF-steps/s (device time, CUDA events on the library stream) of `periods`
+    reinit periods (10 SSP-RK3 steps + 5 fixed pseudo-steps) of a 3D Q2 problem."""
+    import torch
+    from felspa_b200 import abi
+    from felspa_b200.level_set import LevelSetSurface, Mesh
+    ro = abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=N_PSEUDO, narrow_band=narrow_band,
+                                 band_cells=band_cells)
+    ctl = abi.default_ls_opts(reinit_frequency=REINIT_EVERY, reinit=ro)
+    ls = LevelSetSurface(Mesh(3, (n_cells,) * 3), DEGREE, basis=abi.BASIS_Q, precision=precision, cfl_max=CFL,
+                         device=device, control=ctl)
+    # projection only: the reference's initial global sweep (for ICs that are
+    # not exact distance functions) diverges on fine 3D meshes without
+    # artificial viscosity
+    ls.problem.set_velocity(velocity)
+    ls.problem.project(ic)
+    a0 = ls.integrate_mass()
+    ls.run_steps(REINIT_EVERY)   # warm-up, graph capture
+    s = torch.cuda.ExternalStream(ls.problem.stream(), device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    ls.run_steps(periods * REINIT_EVERY, sync=False)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"n_dofs": ls.problem.n_dofs, "periods": periods, "device_ms": ms,
+           "dof_steps_per_s": ls.problem.n_dofs * periods * REINIT_EVERY / (ms * 1e-3),
+           "area_rel_change": (ls.integrate_mass() - a0) / a0}
+    ls.problem.close()
+    return out
 
 
 def learned_comparison():
