@@ -118,3 +118,28 @@ def test_product_does_not_reference_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in text.lower(), f
+
+
+def test_learned_and_batch_entry_points_without_gpu(flsp):
+    """the network and batch entry points report a missing device or bad
+    arguments instead of falling back to the CPU"""
+    L = flsp.load()
+    n = C.c_int64(0)
+    assert L.flsp_mlp_n_params(C.byref(n)) == abi.FLSP_OK
+    assert n.value == 256 * 82 + 256 + 3 * (256 * 256 + 256) + 9 * 256 + 9
+    h = C.c_void_p()
+    assert L.flsp_mlp_create(0, 1, C.byref(h)) == abi.FLSP_ERR_NO_DEVICE
+    m = (abi.MeshDesc * 2)(abi.mesh_desc(2, (8, 8)), abi.mesh_desc(3, (8, 8, 8)))
+    o = (abi.DGOpts * 2)()
+    for i in range(2):
+        L.flsp_default_dg_opts(C.byref(o[i]))
+        o[i].basis = abi.BASIS_Q
+    b = C.c_void_p()
+    assert L.flsp_batch_create(2, m, o, C.byref(b)) == abi.FLSP_ERR_UNSUPPORTED   # a 3D member
+    assert L.flsp_batch_create(0, m, o, C.byref(b)) == abi.FLSP_ERR_BAD_ARG
+    t = abi.TrainOpts()
+    L.flsp_default_train_opts(C.byref(t))
+    assert (t.batch, t.lr, t.beta1, t.beta2) == (8192, 1e-3, 0.9, 0.999)
+    lo = abi.LearnedOpts()
+    L.flsp_default_learned_opts(C.byref(lo))
+    assert (lo.band_cells, lo.max_residual, lo.fallback.mode, lo.fallback.narrow_band) == (6.0, 0.05, abi.REINIT_FIXED, 1)
