@@ -34,11 +34,14 @@
 
 namespace flsp {
 
-// row layout: two (P+1)^2 blocks, each padded to a multiple of 4 elements
-// so that every block starts on a 16-byte boundary (FP32 and FP64)
+// row layout: two (P+1)^2 blocks, each with one spare element and padded to
+// a multiple of 4 elements so that every block starts on a 16-byte boundary
+// (FP32 and FP64).  The spare element of the A block of a row with e != d
+// holds the sign of g_de over the cell's Gauss points (+1 / -1 if it keeps
+// one sign, 0 if it changes sign).
 template <int P>
 __host__ __device__ constexpr int sep_boff() {
-  return (((P + 1) * (P + 1) + 3) / 4) * 4;
+  return (((P + 1) * (P + 1) + 1 + 3) / 4) * 4;
 }
 template <int P>
 __host__ __device__ constexpr int sep_opw() {
@@ -381,6 +384,21 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
         face_trace<DIM, N1, E, T>(src, Ls, tr);
       }
     };
+    const T s1 = ct * fe;
+    const T* r0 = rowp(E, t0, lc[t0]);
+    const T* r1 = DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr;
+    // tangential factors of one sign over the face: |u_E| = sigma u_E, so
+    // B = sigma A and the flux is u_E times the upwind trace alone
+    const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
+    if (sigma != T(0)) {
+      // upwind side: the lower cell where u_E > 0; a missing side takes the
+      // other (domain boundary: own trace)
+      const bool up_m = (s1 * sigma > T(0)) ? has_m : !has_p;
+      T W[NF];
+      trace(up_m ? cm : cp, up_m ? tb.L1 : tb.L0, W);
+      face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
+      return;
+    }
     T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
     if (has_m) trace(cm, tb.L1, S);
     if (has_p) trace(cp, tb.L0, D);
@@ -390,9 +408,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
       S[mf] = T(0.5) * (tm + tp);
       D[mf] = T(0.5) * (tm - tp);
     }
-    const T s1 = ct * fe;
-    face_apply<DIM, N1, BOFF, T>(rowp(E, t0, lc[t0]), DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr, S, D, s1,
-                                 s1 < T(0) ? -s1 : s1, has_m && has_p, F);
+    face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, has_m && has_p, F);
   };
 
   T R[NM];

@@ -492,7 +492,8 @@ void layout_velocity(flsp_handle* h) {
 // For component d, axis e and cell index i along e, with g = the term's
 // axis-e factor at the cell's QGauss(p+2) points:
 //   A[a][b] = sum_q w_q g(x_q) L_b(x_q) (e == d ? L_a'(x_q) : L_a(x_q))
-//   e != d: B[a][b] = sum_q w_q |g(x_q)| L_a(x_q) L_b(x_q)  (at element boff)
+//   e != d: B[a][b] = sum_q w_q |g(x_q)| L_a(x_q) L_b(x_q)  (at element boff),
+//           and at element (p+1)^2 the sign of g over the points (0: mixed)
 //   e == d: g(0), g(1)                                      (at element boff)
 // All in FP64 (long double sums) from the same factor values as the
 // point-wise tables, stored in the state precision.
@@ -502,7 +503,7 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
   VelDev vd = h->veldev();
   if (!vd.sep1) return FLSP_OK;
   const int n1 = h->p + 1, nq = h->p + 2, nn = n1 * n1;
-  const int boff = ((nn + 3) / 4) * 4, opw = 2 * boff;
+  const int boff = ((nn + 1 + 3) / 4) * 4, opw = 2 * boff;   // spare element nn: sign of g
   // a tile copies its rows in one piece: pad each (d, e) block past the mesh
   const int stride = h->nmax + kOpRowPad;
   const size_t nrow = (size_t)h->dim * 3 * stride;
@@ -530,6 +531,14 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
             row[al * n1 + be] = (double)sa;
             if (e != d) row[boff + al * n1 + be] = (double)sb;
           }
+        if (e != d) {   // sign of g over the Gauss points (0: changes sign)
+          bool pos = true, neg = true;
+          for (int q = 0; q < nq; ++q) {
+            pos = pos && gq[q] >= 0.0;
+            neg = neg && gq[q] <= 0.0;
+          }
+          row[nn] = pos ? 1.0 : (neg ? -1.0 : 0.0);
+        }
         if (e == d) {
           row[boff] = gq[nq];          // xi = 0
           row[boff + 1] = gq[nq + 1];  // xi = 1
