@@ -35,6 +35,7 @@ struct HJArgs {
   double dt_explicit;           // used when clk == nullptr
   long long block;              // gradient block stride (ncell * nb)
   const T* __restrict__ rdiff;  // LDG diffusion RHS per unit volume (nu > 0) or null
+  T* stab;                      // smooth-sign table of the tensor-product kernel (hjs_kernel)
 };
 
 // add the cell's LDG diffusion RHS (HBM layout) to R (Q layout)

@@ -453,9 +453,4 @@ __device__ __forceinline__ void hjq_tile(const HJArgs<T>& a, int slot) {
   store_tile<DIM, NM>(m, sb, a.out, tc.ox, tc.oy, tc.oz);
 }
 
-template <int DIM, int P, typename T>
-__global__ void __launch_bounds__(128) hjq_kernel(const HJArgs<T> a) {
-  hjq_tile<DIM, P, T>(a, (int)blockIdx.x);
-}
-
 }  // namespace flsp

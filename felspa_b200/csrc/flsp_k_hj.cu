@@ -3,7 +3,7 @@
 #include <cstring>
 
 #include "flsp_hj.cuh"
-#include "flsp_hjq.cuh"
+#include "flsp_hjs.cuh"
 #include "flsp_ldg.cuh"
 #include "flsp_launch.h"
 #include "flsp_tables.h"
@@ -22,16 +22,16 @@ int hj_default_tile(const Ctx& c, int* tile) {
     using T = decltype(tz);
     static const int c2[][3] = {{16, 16, 1}, {16, 8, 1}, {8, 8, 1}, {8, 4, 1}};
     static const int c3[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}};
-    // the tensor-product kernel runs 128-thread CTAs
-    static const int q2[][3] = {{16, 8, 1}, {8, 8, 1}, {8, 4, 1}, {4, 4, 1}};
-    static const int q3[][3] = {{8, 4, 4}, {4, 4, 4}, {4, 4, 2}, {4, 2, 2}};
-    const bool tq = c.basis == FLSP_BASIS_Q;
-    const int(*cand)[3] = DIM == 2 ? (tq ? q2 : c2) : (tq ? q3 : c3);
-    int i = 0;
-    for (; i < 3; ++i) {
-      const size_t b = tq ? hjq_smem_bytes<DIM, P, T>(cand[i]) : hj_smem_bytes<DIM, P, T>(cand[i]);
-      if (b <= 200 * 1024) break;
+    if (c.basis == FLSP_BASIS_Q) {   // the tensor-product kernel's fixed tile
+      tile[0] = HjsTile<DIM>::X;
+      tile[1] = HjsTile<DIM>::Y;
+      tile[2] = HjsTile<DIM>::Z;
+      return FLSP_OK;
     }
+    const int(*cand)[3] = DIM == 2 ? c2 : c3;
+    int i = 0;
+    for (; i < 3; ++i)
+      if (hj_smem_bytes<DIM, P, T>(cand[i]) <= 200 * 1024) break;
     tile[0] = cand[i][0];
     tile[1] = cand[i][1];
     tile[2] = cand[i][2];
@@ -44,18 +44,31 @@ int hj_prepare(const Ctx& c, const int* tile) {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
     const bool tq = c.basis == FLSP_BASIS_Q;
-    const size_t smem = tq ? hjq_smem_bytes<DIM, P, T>(tile) : hj_smem_bytes<DIM, P, T>(tile);
+    const size_t smem = tq ? hjs_smem_bytes<DIM, P, T>(tile) : hj_smem_bytes<DIM, P, T>(tile);
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "reinit tile too large for shared memory");
-    cudaError_t e = cudaFuncSetAttribute(tq ? hjq_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
+    if (tq && (tile[0] != HjsTile<DIM>::X || tile[1] != HjsTile<DIM>::Y || (DIM > 2 && tile[2] != HjsTile<DIM>::Z)))
+      return set_error(FLSP_ERR_BAD_ARG, "the tensor-product reinit kernel has a fixed tile");
+    cudaError_t e = cudaFuncSetAttribute(tq ? hjs_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(tq ? hjq_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
+      e = cudaFuncSetAttribute(tq ? hjs_kernel<DIM, P, T> : hj_kernel<DIM, P, T>,
                                cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("hj attr: ") + cudaGetErrorString(e));
     return FLSP_OK;
   });
 }
 
+int hj_table_bytes(const Ctx& c, const int* tile, size_t* bytes) {
+  return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
+    constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
+    using T = decltype(tz);
+    MeshArgs m = c.m;
+    set_tile(m, DIM, tile);
+    const long long nt = (long long)m.tile[0] * m.tile[1] * m.tile[2];
+    *bytes = (size_t)nblocks(m) * hjs_ns<DIM, P>() * nt * sizeof(T);
+    return FLSP_OK;
+  });
+}
 
 int ldg_prepare(const Ctx& c) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
@@ -113,9 +126,18 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
     // the gradient export mode uses the modal kernel for both bases
     if (mode != kHJGradients) apply_band(c, kNbHJ, a.m);   // the gradient export uses no band
     if (c.basis == FLSP_BASIS_Q && mode != kHJGradients) {
-      const size_t smem = hjq_smem_bytes<DIM, P, T>(a.m.tile);
-      hjq_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
-      return launch_status("hjq_kernel");
+      // the smooth-sign table is filled by the sweep's kHJCflOnly launch,
+      // which evaluates phi0 as phi
+      if (!c.hj_stab) return set_error(FLSP_ERR_BAD_ARG, "reinit sign table not allocated");
+      if (mode == kHJCflOnly && phi != phi0)
+        return set_error(FLSP_ERR_BAD_ARG, "the sign-table launch needs phi == phi0");
+      if (a.m.tile[0] != HjsTile<DIM>::X || a.m.tile[1] != HjsTile<DIM>::Y || a.m.tile[2] != HjsTile<DIM>::Z)
+        return set_error(FLSP_ERR_BAD_ARG, "the tensor-product reinit kernel has a fixed tile");
+      a.stab = reinterpret_cast<T*>(c.hj_stab);
+      const size_t smem = hjs_smem_bytes<DIM, P, T>(a.m.tile);
+      const int threads = HjsTile<DIM>::N * (P + 2);
+      hjs_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), threads, smem, c.stream>>>(a);
+      return launch_status("hjs_kernel");
     }
     int tm[3];
     if (c.basis == FLSP_BASIS_Q) {  // modal kernel with its own tile

@@ -23,6 +23,7 @@ struct Ctx {
   cudaStream_t stream;
   const int* nb_tiles[3];   // active tile lists (null: every tile)
   const int* nb_count[3];   // device counts of the lists
+  void* hj_stab;            // smooth-sign table of the tensor-product reinit kernel
 };
 
 // tile shapes of the LDG viscosity and WENO limiter kernels
@@ -148,6 +149,8 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
 // ---------------- reinitialisation (flsp_k_hj.cu) ----------------
 int hj_default_tile(const Ctx& c, int* tile);
 int hj_prepare(const Ctx& c, const int* tile);
+// bytes of the tensor-product reinit kernel's smooth-sign table for `tile`
+int hj_table_bytes(const Ctx& c, const int* tile, size_t* bytes);
 int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClock* clk, int mode,
               int rk, double dt_explicit, long long block, const int* tile,
               const void* rdiff = nullptr);
