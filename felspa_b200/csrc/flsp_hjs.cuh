@@ -178,17 +178,19 @@ __device__ __forceinline__ void hjs_face(const MeshArgs& m, const T* box, T* jn,
   }
 }
 
-// value and gradient (reference-cell derivatives) of the modal field c at
-// the vertex with corner bits (vx, vy, vz)
+// values and gradients (reference-cell derivatives) of the modal field c
+// at the two vertices (vx = 0, 1) of the x-line with corner bits (vy, vz):
+// the y/z reductions are shared by both ends of the line
 template <int DIM, int N1, typename T>
-__device__ __forceinline__ void hjs_vertex(const T* c, const Tab1D<T>& tb, int vx, int vy, int vz, T& val,
-                                           T* gr) {
-  const T* X = vx ? tb.L1 : tb.L0;
-  const T* Xd = vx ? tb.D1 : tb.D0;
-  const T* Y = vy ? tb.L1 : tb.L0;
-  const T* Yd = vy ? tb.D1 : tb.D0;
+__device__ __forceinline__ void hjs_line(const T* c, const Tab1D<T>& tb, int vy, int vz, T* val, T (*gr)[3]) {
+  T Y[N1], Yd[N1];
+#pragma unroll
+  for (int b = 0; b < N1; ++b) {
+    Y[b] = vy ? tb.L1[b] : tb.L0[b];
+    Yd[b] = vy ? tb.D1[b] : tb.D0[b];
+  }
+  T V[N1], Vy[N1], Vz[N1];
   if constexpr (DIM == 2) {
-    T W[N1], Wd[N1];
 #pragma unroll
     for (int a = 0; a < N1; ++a) {
       T s0 = T(0), s1 = T(0);
@@ -197,23 +199,17 @@ __device__ __forceinline__ void hjs_vertex(const T* c, const Tab1D<T>& tb, int v
         s0 += c[a + N1 * b] * Y[b];
         s1 += c[a + N1 * b] * Yd[b];
       }
-      W[a] = s0;
-      Wd[a] = s1;
+      V[a] = s0;
+      Vy[a] = s1;
+      Vz[a] = T(0);
     }
-    T v = T(0), gx = T(0), gy = T(0);
-#pragma unroll
-    for (int a = 0; a < N1; ++a) {
-      v += W[a] * X[a];
-      gx += W[a] * Xd[a];
-      gy += Wd[a] * X[a];
-    }
-    val = v;
-    gr[0] = gx;
-    gr[1] = gy;
   } else {
-    const T* Z = vz ? tb.L1 : tb.L0;
-    const T* Zd = vz ? tb.D1 : tb.D0;
-    T V[N1], Vy[N1], Vz[N1];
+    T Z[N1], Zd[N1];
+#pragma unroll
+    for (int b = 0; b < N1; ++b) {
+      Z[b] = vz ? tb.L1[b] : tb.L0[b];
+      Zd[b] = vz ? tb.D1[b] : tb.D0[b];
+    }
 #pragma unroll
     for (int a = 0; a < N1; ++a) {
       T W[N1], Wd[N1];
@@ -239,6 +235,11 @@ __device__ __forceinline__ void hjs_vertex(const T* c, const Tab1D<T>& tb, int v
       Vy[a] = s1;
       Vz[a] = s2;
     }
+  }
+#pragma unroll
+  for (int vx = 0; vx < 2; ++vx) {
+    const T* X = vx ? tb.L1 : tb.L0;
+    const T* Xd = vx ? tb.D1 : tb.D0;
     T v = T(0), gx = T(0), gy = T(0), gz = T(0);
 #pragma unroll
     for (int a = 0; a < N1; ++a) {
@@ -247,10 +248,10 @@ __device__ __forceinline__ void hjs_vertex(const T* c, const Tab1D<T>& tb, int v
       gy += Vy[a] * X[a];
       gz += Vz[a] * X[a];
     }
-    val = v;
-    gr[0] = gx;
-    gr[1] = gy;
-    gr[2] = gz;
+    val[vx] = v;
+    gr[vx][0] = gx;
+    gr[vx][1] = gy;
+    gr[vx][2] = gz;
   }
 }
 
@@ -410,14 +411,18 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
       }
     }
 
-    // -------- vertex CFL estimate for the next pseudo-step (vertices v with
-    // v % NQ == k)
+    // -------- vertex CFL estimate for the next pseudo-step: x-lines of
+    // vertices ln = k, k + NQ, ... (corner bits vy = ln & 1, vz = ln >> 1)
+#pragma unroll 1
+    for (int ln = k; ln < NV / 2; ln += NQ) {
+      T vals[2], grs[2][3];
+      hjs_line<DIM, N1, T>(cr, tb, ln & 1, ln >> 1, vals, grs);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      if (v % NQ != k) continue;
-      const int vb[3] = {v & 1, (v >> 1) & 1, (v >> 2) & 1};
-      T val, dphi[3];
-      hjs_vertex<DIM, N1, T>(cr, tb, vb[0], vb[1], vb[2], val, dphi);
+      for (int vx = 0; vx < 2; ++vx) {
+      const int v = vx + 2 * ln;
+      const int vb[3] = {vx, ln & 1, ln >> 1};
+      const T val = vals[vx];
+      const T* dphi = grs[vx];
       T S;
       if (fill) {
         T g2 = T(0);
@@ -460,6 +465,7 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
 #pragma unroll
       for (int d = 0; d < DIM; ++d) s2 += gs[d] * gs[d];
       vmax = fmax(vmax, (double)sqrt(s2));
+      }
     }
     vmax = vmax / m.diam;
   }
@@ -598,13 +604,12 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
   }
   __syncthreads();   // planes done: the face-jump area becomes the store staging
 
-  // -------- modes q with q % NQ == k: sum over the planes, update, stage
+  // -------- modes q = k, k + NQ, ...: sum over the planes, update, stage
   T* sb = jn;   // [NT][NM]
   if (valid) {
     const long long cell = (long long)g[0] + (long long)m.n[0] * (g[1] + (long long)m.n[1] * g[2]);
-#pragma unroll
-    for (int q = 0; q < NM; ++q) {
-      if (q % NQ != k) continue;
+#pragma unroll 1
+    for (int q = k; q < NM; q += NQ) {
       const int u = q % NU, cz = q / NU;   // (aa, b) of the plane projection, last-axis mode
       T R = T(0);
 #pragma unroll
