@@ -36,6 +36,7 @@ struct HJArgs {
   long long block;              // gradient block stride (ncell * nb)
   const T* __restrict__ rdiff;  // LDG diffusion RHS per unit volume (nu > 0) or null
   T* stab;                      // smooth-sign table of the tensor-product kernel (hjs_kernel)
+  int* err;                     // device error word (DevClock::err) or null
 };
 
 // add the cell's LDG diffusion RHS (HBM layout) to R (Q layout)

@@ -43,17 +43,29 @@ __host__ __device__ constexpr int hjs_ns() {
   return ipow(P + 2, DIM) + (1 << DIM);
 }
 
+// shared-memory plan: the halo box as rows of cells along x, each row a
+// bulk copy from a 16-byte aligned global address (the row's data starts at
+// its slot + the address phase), then the face jumps, the corner jumps,
+// the plane projections and the block reduction
 template <int DIM, int P, typename T>
-__host__ __device__ inline size_t hjs_smem_bytes(const int* tile) {
-  constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NQF = ipow(NQ, DIM - 1), NC = 1 << (DIM - 1);
-  constexpr int NU = ipow(N1, DIM - 1);
-  const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
-  const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
-  const size_t box = (size_t)bx * by * bz * NM;
-  const size_t jn = (size_t)2 * DIM * NQF * nt;
-  const size_t jv = (size_t)2 * DIM * NC * nt;
-  const size_t ub = (size_t)NQ * NU * nt;
-  return (box + jn + jv + ub) * sizeof(T) + 64 * sizeof(double) + 16;
+struct HjsPlan {
+  using TL = HjsTile<DIM>;
+  static constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NQF = ipow(NQ, DIM - 1);
+  static constexpr int NC = 1 << (DIM - 1), NU = ipow(N1, DIM - 1);
+  static constexpr int BY = TL::Y + 2, BZ = DIM > 2 ? TL::Z + 2 : 1, NROWS = BY * BZ;
+  static constexpr int NMB = NM * (int)sizeof(T);   // bytes per cell
+  static constexpr int SLOT = (((TL::X + 2) * NMB + 30) + 15) / 16 * 16;
+  static constexpr size_t OFF_BOX = 16;
+  static constexpr size_t OFF_JN = OFF_BOX + (size_t)NROWS * SLOT;
+  static constexpr size_t OFF_JV = OFF_JN + (size_t)2 * DIM * NQF * TL::N * sizeof(T);
+  static constexpr size_t OFF_UB = OFF_JV + (size_t)2 * DIM * NC * TL::N * sizeof(T);
+  static constexpr size_t OFF_RED = (OFF_UB + (size_t)NQ * NU * TL::N * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t BYTES = OFF_RED + 64 * sizeof(double);
+};
+
+template <int DIM, int P, typename T>
+__host__ __device__ inline size_t hjs_smem_bytes(const int*) {
+  return HjsPlan<DIM, P, T>::BYTES;
 }
 
 // smooth sign from phi0's value and (scaled) gradient at a point, with the
@@ -68,20 +80,13 @@ __device__ __forceinline__ T hjs_sign(T p0, T g2, T hmin) {
   }
 }
 
-// slot of local cell (lx, ly, lz) in the halo box (tile + one layer)
-template <int DIM>
-__device__ __forceinline__ int hjs_box_index(int lx, int ly, int lz) {
-  using TL = HjsTile<DIM>;
-  constexpr int bx = TL::X + 2, by = TL::Y + 2;
-  return (lx + 1) + bx * ((ly + 1) + by * (DIM > 2 ? lz + 1 : 0));
-}
-
 // the jump phi_upper - phi_lower on the faces normal to E (one face per
 // call, lower cell at local lc with lc[E] = f - 1), times 1/h_E, written
 // nodal at the face Gauss points and at the face corners for both adjacent
 // tile cells
-template <int DIM, int P, int E, typename T>
-__device__ __forceinline__ void hjs_face(const MeshArgs& m, const T* box, T* jn, T* jv, const int* o, int r) {
+template <int DIM, int P, int E, typename T, typename CellP>
+__device__ __forceinline__ void hjs_face(const MeshArgs& m, const CellP& cellp, T* jn, T* jv, const int* o,
+                                         int r) {
   constexpr int N1 = P + 1, NQ = P + 2, NF = ipow(N1, DIM - 1), NQF = ipow(NQ, DIM - 1), NC = 1 << (DIM - 1);
   constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
   constexpr int st[3] = {1, N1, N1 * N1};
@@ -100,8 +105,8 @@ __device__ __forceinline__ void hjs_face(const MeshArgs& m, const T* box, T* jn,
   const bool inside = o[E] + f - 1 >= 0 && o[E] + f < m.n[E];
   T J[NF];
   if (inside) {
-    const T* cu = box + (size_t)hjs_box_index<DIM>(lu[0], lu[1], lu[2]) * (ipow(N1, DIM));
-    const T* cd = box + (size_t)hjs_box_index<DIM>(ll[0], ll[1], ll[2]) * (ipow(N1, DIM));
+    const T* cu = cellp(lu[0], lu[1], lu[2]);
+    const T* cd = cellp(ll[0], ll[1], ll[2]);
 #pragma unroll
     for (int mf = 0; mf < NF; ++mf) {
       const int m0 = mf % N1, m1 = mf / N1;
@@ -255,65 +260,76 @@ __device__ __forceinline__ void hjs_line(const T* c, const Tab1D<T>& tb, int vy,
   }
 }
 
-// One launch serves one HjsTile of cells with NQ threads per cell
-// (blockDim = cells * NQ).  Modes: kHJCflOnly (phi == phi0: fills the sign
+// One block serves one HjsTile of cells (launch slot blockIdx.x) with NQ
+// threads per cell (blockDim = cells * NQ); its halo box arrives by bulk
+// copies on one mbarrier.  Modes: kHJCflOnly (phi == phi0: fills the sign
 // table, CFL estimate of the first pseudo-step) and kHJStep (one pseudo-
 // step from the table, CFL estimate of the next).
 template <int DIM, int P, typename T>
 __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJArgs<T> a) {
+  using PL = HjsPlan<DIM, P, T>;
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NV = 1 << DIM;
   constexpr int NQF = ipow(NQ, DIM - 1), NC = 1 << (DIM - 1);
   constexpr int NU = ipow(N1, DIM - 1), NQV = ipow(NQ, DIM), NS = NQV + NV;
   using TL = HjsTile<DIM>;
-  constexpr int TX = TL::X, TY = TL::Y, TZ = TL::Z, NT = TL::N;
-  constexpr int NBOX = (TX + 2) * (TY + 2) * (DIM > 2 ? TZ + 2 : 1);
+  constexpr int TX = TL::X, TY = TL::Y, TZ = TL::Z, NT = TL::N, NMB = PL::NMB;
   static_assert(NM <= 2 * DIM * NQF, "the store staging reuses the face-jump area");
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
+  unsigned char* boxb = smem_raw + PL::OFF_BOX;
+  T* jn = reinterpret_cast<T*>(smem_raw + PL::OFF_JN);   // [2*DIM*NQF][NT]
+  T* jv = reinterpret_cast<T*>(smem_raw + PL::OFF_JV);   // [2*DIM*NC][NT]
+  T* ub = reinterpret_cast<T*>(smem_raw + PL::OFF_UB);   // [NQ][NU][NT]
+  double* red = reinterpret_cast<double*>(smem_raw + PL::OFF_RED);
   const MeshArgs& m = a.m;
+  const Tab1D<T>& tb = tab<T>(P);
   const int slot = (int)blockIdx.x;
   if (tile_inactive(m, slot)) return;
-  T* box = reinterpret_cast<T*>(smem_raw);
-  T* jn = box + (size_t)NBOX * NM;         // [2*DIM*NQF][NT]
-  T* jv = jn + (size_t)2 * DIM * NQF * NT;  // [2*DIM*NC][NT]
-  T* ub = jv + (size_t)2 * DIM * NC * NT;   // [NQ][NU][NT]
-  double* red = align16<double>(ub + (size_t)NQ * NU * NT);
-  const Tab1D<T>& tb = tab<T>(P);
 
-  const int tile = m.tiles ? m.tiles[slot] : slot;
-  int o[3];
-  {
-    int b = tile;
+  auto origin = [&](int slot, int* o) {
+    int b = m.tiles ? m.tiles[slot] : slot;
     o[0] = (b % m.ntile[0]) * TX;
     b /= m.ntile[0];
     o[1] = DIM > 1 ? (b % m.ntile[1]) * TY : 0;
     o[2] = DIM > 2 ? (b / m.ntile[1]) * TZ : 0;
-  }
+  };
+  // halo box of the tile in launch slot `slot`: rows (ly, lz) of cells
+  // [max(ox - 1, 0), min(ox + TX + 1, n)) by bulk copies (warp 0)
+  auto issue = [&](int slot) {
+    int so[3];
+    origin(slot, so);
+    const int hx0 = max(so[0] - 1, 0), hx1 = min(so[0] + TX + 1, m.n[0]);
+    const int lane = threadIdx.x;
+    const char* gsrc = reinterpret_cast<const char*>(a.phi);
+    unsigned bytes = 0;
+    // pass 0 counts the bytes, pass 1 issues the copies
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1) {
+#pragma unroll
+        for (int w = 16; w > 0; w >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, w);
+        if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+        __syncwarp();
+      }
+      for (int rr = lane; rr < PL::NROWS; rr += 32) {
+        const int ly = rr % PL::BY - 1, lz = DIM > 2 ? rr / PL::BY - 1 : 0;
+        const bool yout = ly < 0 || ly >= TY, zout = DIM > 2 && (lz < 0 || lz >= TZ);
+        if (yout && zout) continue;
+        const int gy = so[1] + ly, gz = so[2] + lz;
+        if (gy < 0 || gy >= m.n[1] || (DIM > 2 && (gz < 0 || gz >= m.n[2]))) continue;
+        const long long rowcell = (long long)m.n[0] * (gy + (long long)m.n[1] * (DIM > 2 ? gz : 0));
+        const long long s0 = (rowcell + hx0) * NMB, s1 = (rowcell + hx1) * NMB;
+        const long long a0 = s0 & ~15LL, a1 = (s1 + 15) & ~15LL;
+        if (pass == 0) bytes += (unsigned)(a1 - a0);
+        else bulk_g2s(boxb + (size_t)rr * PL::SLOT, gsrc + a0, (unsigned)(a1 - a0), bar);
+      }
+    }
+  };
+
   const int cl = (int)threadIdx.x % NT, k = (int)threadIdx.x / NT;   // cell, Gauss plane
   const int l[3] = {cl % TX, (cl / TX) % TY, DIM > 2 ? cl / (TX * TY) : 0};
-  const int g[3] = {o[0] + l[0], o[1] + l[1], o[2] + l[2]};
-  const bool valid = g[0] < m.n[0] && g[1] < m.n[1] && (DIM < 3 || g[2] < m.n[2]);
-
-  load_box<DIM, NM>(m, a.phi, box, o[0], o[1], o[2], true);
-  cp_async_wait_all();
-  __syncthreads();
-
-  // -------- face jumps, one work item per face of the tile
-  {
-    constexpr int C0 = (TX + 1) * (NT / TX), C1 = (TY + 1) * (NT / TY);
-    constexpr int C2 = DIM > 2 ? (TZ + 1) * (NT / TZ) : 0;
-    for (int i = threadIdx.x; i < C0 + C1 + C2; i += NT * NQ) {
-      if (i < C0) hjs_face<DIM, P, 0, T>(m, box, jn, jv, o, i);
-      else if (i < C0 + C1) hjs_face<DIM, P, 1, T>(m, box, jn, jv, o, i - C0);
-      else if constexpr (DIM > 2) hjs_face<DIM, P, 2, T>(m, box, jn, jv, o, i - C0 - C1);
-    }
-  }
-  __syncthreads();
-
   const T ih[3] = {T(1.0 / m.h[0]), T(1.0 / m.h[1]), T(DIM > 2 ? 1.0 / m.h[2] : 1.0)};
   const T hmin = T(m.min_diam);
   const bool fill = a.mode == kHJCflOnly;
-  T* srow = a.stab + (size_t)tile * NS * NT + cl;   // this cell's table column, stride NT
-  const T* c = box + (size_t)hjs_box_index<DIM>(l[0], l[1], l[2]) * NM;
   // this thread's Gauss plane (uniform per warp): its 1D table entries
   T Lk[N1], Dk[N1];
 #pragma unroll
@@ -321,10 +337,49 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
     Lk[b] = tb.Lq[b][k];
     Dk[b] = tb.Dq[b][k];
   }
+  const T dt = a.clk ? T(a.clk->hj_dt) : T(a.dt_explicit);
   double vmax = 0.0;
 
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x < 32) issue(slot);
+
+  int o[3];
+  origin(slot, o);
+  const int tile = m.tiles ? m.tiles[slot] : slot;
+  const int g[3] = {o[0] + l[0], o[1] + l[1], o[2] + l[2]};
+  const bool valid = g[0] < m.n[0] && g[1] < m.n[1] && (DIM < 3 || g[2] < m.n[2]);
+  const int gx0 = max(o[0] - 1, 0);
+  // box copy of the cell at local coordinates (lx, ly, lz)
+  auto cellp = [&](int lx, int ly, int lz) -> const T* {
+    const int rr = (ly + 1) + PL::BY * (DIM > 2 ? lz + 1 : 0);
+    const unsigned rowcell = (unsigned)m.n[0] * (unsigned)((o[1] + ly) + m.n[1] * (DIM > 2 ? o[2] + lz : 0));
+    const unsigned phase = ((rowcell + (unsigned)gx0) * (unsigned)NMB) & 15u;
+    return reinterpret_cast<const T*>(boxb + (size_t)rr * PL::SLOT + phase + (o[0] + lx - gx0) * NMB);
+  };
+  if (!mbar_wait(bar, 0u, 1 << 22)) {
+    if (threadIdx.x == 0 && a.err) atomicOr(a.err, kErrCopyTimeout);
+  }
+
+  // -------- face jumps, one work item per face of the tile
+  {
+    constexpr int C0 = (TX + 1) * (NT / TX), C1 = (TY + 1) * (NT / TY);
+    constexpr int C2 = DIM > 2 ? (TZ + 1) * (NT / TZ) : 0;
+    for (int i = threadIdx.x; i < C0 + C1 + C2; i += NT * NQ) {
+      if (i < C0) hjs_face<DIM, P, 0, T>(m, cellp, jn, jv, o, i);
+      else if (i < C0 + C1) hjs_face<DIM, P, 1, T>(m, cellp, jn, jv, o, i - C0);
+      else if constexpr (DIM > 2) hjs_face<DIM, P, 2, T>(m, cellp, jn, jv, o, i - C0 - C1);
+    }
+  }
+  __syncthreads();
+
+  T* srow = a.stab + (size_t)tile * NS * NT + cl;   // this cell's table column, stride NT
+  // the cell's modes projected on this thread's Gauss plane of the last
+  // axis: value (PL0) and derivative (PL1) tables, in the modes of the others
+  T PL0[NU], PL1[NU];
+  const T* c = cellp(l[0], l[1], l[2]);   // the cell's modes (box copy)
   if (valid) {
-    T cr[NM];   // the cell's modes, read once for the sign table and the vertices
+    T cr[NM];
 #pragma unroll
     for (int q = 0; q < NM; ++q) cr[q] = c[q];
     // -------- sign table of this cell's Gauss plane (phi == phi0)
@@ -467,16 +522,28 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
       vmax = fmax(vmax, (double)sqrt(s2));
       }
     }
-    vmax = vmax / m.diam;
+    if (!fill) {
+#pragma unroll
+      for (int u = 0; u < NU; ++u) {
+        T s1 = T(0), s2 = T(0);
+#pragma unroll
+        for (int cc = 0; cc < N1; ++cc) {
+          const T cv = cr[u + NU * cc];
+          s1 += cv * Lk[cc];
+          s2 += cv * Dk[cc];
+        }
+        PL0[u] = s1;
+        PL1[u] = s2;
+      }
+    }
   }
-
+  vmax = vmax / m.diam;
   const double bm = block_max(vmax, red);
   if (threadIdx.x == 0 && a.clk) atomic_max_pos(&a.clk->hj_vd_bits, bm);
   if (a.mode != kHJStep) return;
 
   // -------- pseudo-step: H at this plane's Gauss points, projected onto
   // the modes of the other axes
-  const T dt = a.clk ? T(a.clk->hj_dt) : T(a.dt_explicit);
   auto jnv = [&](int d, int side, int qf) -> T { return jn[(size_t)((2 * d + side) * NQF + qf) * NT + cl]; };
   auto hfun = [&](T S, const T* lft, const T* rgt) -> T {
     T avg2 = T(0);
@@ -497,19 +564,8 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
     const T K0k = tb.K0q[k], K1k = tb.K1q[k];
     if constexpr (DIM == 2) {
       const int qy = k;
-      T Py[N1], Pdy[N1];
-#pragma unroll
-      for (int aa = 0; aa < N1; ++aa) {
-        T s1 = T(0), s2 = T(0);
-#pragma unroll
-        for (int b = 0; b < N1; ++b) {
-          const T cv = c[aa + N1 * b];
-          s1 += cv * Lk[b];
-          s2 += cv * Dk[b];
-        }
-        Py[aa] = s1;
-        Pdy[aa] = s2;
-      }
+      const T* Py = PL0;
+      const T* Pdy = PL1;
       const T jlx = jnv(0, 0, qy), jhx = jnv(0, 1, qy);
       T X[N1];
 #pragma unroll
@@ -534,21 +590,6 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
 #pragma unroll
       for (int aa = 0; aa < N1; ++aa) ub[(size_t)(k * NU + aa) * NT + cl] = X[aa];
     } else {
-      T Pz[N1][N1], Dz[N1][N1];
-#pragma unroll
-      for (int aa = 0; aa < N1; ++aa)
-#pragma unroll
-        for (int b = 0; b < N1; ++b) {
-          T s1 = T(0), s2 = T(0);
-#pragma unroll
-          for (int cc = 0; cc < N1; ++cc) {
-            const T cv = c[aa + N1 * (b + N1 * cc)];
-            s1 += cv * Lk[cc];
-            s2 += cv * Dk[cc];
-          }
-          Pz[aa][b] = s1;
-          Dz[aa][b] = s2;
-        }
       T U[N1][N1];
 #pragma unroll
       for (int aa = 0; aa < N1; ++aa)
@@ -562,9 +603,9 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
           T s1 = T(0), s2 = T(0), s3 = T(0);
 #pragma unroll
           for (int b = 0; b < N1; ++b) {
-            s1 += Pz[aa][b] * tb.Lq[b][qy];
-            s2 += Pz[aa][b] * tb.Dq[b][qy];
-            s3 += Dz[aa][b] * tb.Lq[b][qy];
+            s1 += PL0[aa + N1 * b] * tb.Lq[b][qy];
+            s2 += PL0[aa + N1 * b] * tb.Dq[b][qy];
+            s3 += PL1[aa + N1 * b] * tb.Lq[b][qy];
           }
           Py[aa] = s1 * ih[0];
           Pdy[aa] = s2 * ih[1];
@@ -605,6 +646,7 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
   __syncthreads();   // planes done: the face-jump area becomes the store staging
 
   // -------- modes q = k, k + NQ, ...: sum over the planes, update, stage
+  {
   T* sb = jn;   // [NT][NM]
   if (valid) {
     const long long cell = (long long)g[0] + (long long)m.n[0] * (g[1] + (long long)m.n[1] * g[2]);
@@ -620,6 +662,7 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
   }
   __syncthreads();
   store_tile<DIM, NM>(m, sb, a.out, o[0], o[1], o[2]);
+  }
 }
 
 }  // namespace flsp

@@ -134,6 +134,7 @@ int launch_hj(const Ctx& c, const void* phi, const void* phi0, void* out, DevClo
       if (a.m.tile[0] != HjsTile<DIM>::X || a.m.tile[1] != HjsTile<DIM>::Y || a.m.tile[2] != HjsTile<DIM>::Z)
         return set_error(FLSP_ERR_BAD_ARG, "the tensor-product reinit kernel has a fixed tile");
       a.stab = reinterpret_cast<T*>(c.hj_stab);
+      a.err = clk ? &clk->err : nullptr;
       const size_t smem = hjs_smem_bytes<DIM, P, T>(a.m.tile);
       const int threads = HjsTile<DIM>::N * (P + 2);
       hjs_kernel<DIM, P, T><<<(unsigned)nblocks(a.m), threads, smem, c.stream>>>(a);
