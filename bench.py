@@ -371,6 +371,13 @@ def run_ours(args):
                         "16 cosine modes; plain full-sweep reinit",
                 **variant_rate(abi.FP32, local, 128, F.plume_3d(), F.perturbed_plane(seed=5), 4)},
         }
+        from felspa_b200.batch import config5_group
+        line["variants"]["config5_group"] = {
+            "what": "config-5 structure: the 128^3 Q2 FP32 plume problem and 8 side 64^3 problems (perturbed "
+                    "planes, seeds 5..13) advanced together, each reinit period (5 SSP-RK3 substeps + a fixed "
+                    "5-pseudo-step plain reinit) of all 9 problems replayed from ONE CUDA graph (one branch per "
+                    "problem); compared with the same periods replayed problem by problem",
+            **config5_group(periods=4)}
     if world == 1 and not args.no_batched:
         from felspa_b200.batch import config3_benchmark
         r = config3_benchmark()

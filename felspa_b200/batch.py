@@ -161,3 +161,95 @@ def config3_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, co
                                   "one_by_one_s": t_single, "batched_s": t_batch_sub,
                                   "one_by_one_dof_steps_per_s": sub_dofs * compare_steps / t_single,
                                   "batched_dof_steps_per_s": sub_dofs * compare_steps / t_batch_sub}}
+
+
+class Group:
+    """Several independent problems (any dimension, size or degree) whose
+    reinit periods run from ONE captured CUDA graph, one branch per problem
+    (flsp_group_* in include/flsp_dg.h).  The problems stay the caller's:
+    the group only orders and replays their periods."""
+
+    def __init__(self, problems):
+        L = load()
+        self.problems = list(problems)
+        hs = (C.c_void_p * len(self.problems))(*[p.h for p in self.problems])
+        g = C.c_void_p()
+        check(L.flsp_group_create(hs, len(self.problems), C.byref(g)))
+        self.h = g
+        self.n_dofs = sum(p.n_dofs for p in self.problems)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().flsp_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_periods(self, n_periods, control, sync=True):
+        check(load().flsp_group_run_periods(self.h, C.byref(control), int(n_periods)))
+        if sync:
+            self.sync()
+
+    def sync(self):
+        check(load().flsp_group_sync(self.h))
+
+    def stream(self):
+        s = C.c_void_p()
+        check(load().flsp_group_stream(self.h, C.byref(s)))
+        return s.value
+
+
+def config5_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_pseudo=5, degree=2):
+    """The large 3D configuration's structure: a main n_main^3 Q2 FP32 problem
+    and n_sides n_side^3 side problems (plume rolls u = curl(0, psi, 0),
+    perturbed-plane ICs with seeds 5, 6, ...), one graph per reinit period
+    (reinit_every SSP-RK3 substeps + a fixed n_pseudo-step reinit) covering
+    every problem.  Returns DoF-steps/s over all problems (device time, CUDA
+    events on the group's stream) and the same periods with each problem
+    replayed alone, one after the other."""
+    import torch
+    ctl = abi.default_ls_opts(reinit_frequency=reinit_every,
+                              reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=n_pseudo))
+    sizes = [n_main] + [n_side] * n_sides
+    probs = []
+    for i, n in enumerate(sizes):
+        pb = Problem(Mesh(3, (n, n, n)), degree, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+        pb.set_velocity(F.plume_3d())
+        pb.project(F.perturbed_plane(seed=5 + i))
+        probs.append(pb)
+    g = Group(probs)
+    g.run_periods(1, ctl)            # warm-up period (captures the graph)
+    s = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    g.run_periods(periods, ctl, sync=False)
+    e1.record(s)
+    e1.synchronize()
+    ms_group = e0.elapsed_time(e1)
+    g.sync()
+    finite = all(bool(np.all(np.isfinite(p.get_state()))) for p in probs)
+    n_dofs = g.n_dofs
+    g.close()
+    # the same periods, each problem alone (its own graph), one after the other
+    ms_alone = 0.0
+    for pb in probs:
+        check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), reinit_every))   # warm-up / capture
+        pb.sync()
+        st = torch.cuda.ExternalStream(pb.stream())
+        torch.cuda.synchronize()
+        e0.record(st)
+        check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), periods * reinit_every))
+        e1.record(st)
+        e1.synchronize()
+        ms_alone += e0.elapsed_time(e1)
+    for pb in probs:
+        pb.close()
+    steps = periods * reinit_every
+    return {"n_dofs": n_dofs, "problems": len(sizes), "periods": periods, "device_ms": ms_group,
+            "dof_steps_per_s": n_dofs * steps / (ms_group * 1e-3),
+            "one_after_another_dof_steps_per_s": n_dofs * steps / (ms_alone * 1e-3), "finite": finite}

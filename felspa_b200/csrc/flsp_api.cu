@@ -1049,6 +1049,31 @@ int flsp_ls_advance(flsp_handle* h, const flsp_ls_opts* o, double time_step, int
 
 // n_steps advection substeps, fixed-count reinit every reinit_frequency
 // steps; one reinit period is captured into a CUDA graph and replayed
+// one reinit period on the handle's stream: `steps` advection substeps, then
+// the fixed-count reinit (graph-capturable; band buffers allocated before)
+int enqueue_period(flsp_handle* h, const flsp_reinit_opts* ro, int steps) {
+  for (int s = 0; s < steps; ++s) ST(enqueue_adv_step(h));
+  const bool limiter = reinit_limiter(h, ro);
+  const int phi0 = h->cur;
+  if (ro->narrow_band) {
+    const int stb = band_begin(h, ro, phi0, limiter);
+    if (stb) {
+      for (int k = 0; k < 3; ++k) h->nb_use[k] = false;
+      return stb;
+    }
+  }
+  int st = launch_hj_clock_reset(h->stream, h->clk);
+  if (st == FLSP_OK)
+    st = launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, ro->rk_order, 0.0,
+                   h->ndofs, h->hj_tile);
+  for (int k = 0; k < ro->n_pseudo_steps && st == FLSP_OK; ++k) st = enqueue_hj_step(h, ro, phi0, limiter);
+  if (ro->narrow_band) {
+    const int st2 = band_end(h, phi0);
+    if (st == FLSP_OK) st = st2;
+  }
+  return st;
+}
+
 int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
   if (!h || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
   if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
@@ -1084,22 +1109,7 @@ int flsp_ls_run_steps(flsp_handle* h, const flsp_ls_opts* o, int n_steps) {
         if (ro.narrow_band) ST(ensure_band_buffers(h));
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        int st = FLSP_OK;
-        for (int s = 0; s < to_reinit && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
-        if (st == FLSP_OK) {
-          const bool limiter = reinit_limiter(h, &ro);
-          const int phi0 = h->cur;
-          if (ro.narrow_band) st = band_begin(h, &ro, phi0, limiter);
-          if (st == FLSP_OK) st = launch_hj_clock_reset(h->stream, h->clk);
-          if (st == FLSP_OK)
-            st = launch_hj(h->ctx(), h->buf[phi0], h->buf[phi0], nullptr, h->clk, kHJCflOnly, ro.rk_order, 0.0,
-                           h->ndofs, h->hj_tile);
-          for (int k = 0; k < ro.n_pseudo_steps && st == FLSP_OK; ++k) st = enqueue_hj_step(h, &ro, phi0, limiter);
-          if (ro.narrow_band) {
-            const int st2 = band_end(h, phi0);
-            if (st == FLSP_OK) st = st2;
-          }
-        }
+        const int st = enqueue_period(h, &ro, to_reinit);
         cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
         if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); h->cur = cur0; return st; }
         if (ce != cudaSuccess) return fail(FLSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
@@ -1716,6 +1726,153 @@ int flsp_batch_sync(flsp_batch* b) {
 int flsp_batch_stream(const flsp_batch* b, void** stream) {
   if (!b || !stream) return fail(FLSP_ERR_BAD_ARG, "null argument");
   *stream = (void*)b->stream;
+  return FLSP_OK;
+}
+
+
+// ---------------------------------------------------------------------
+// Groups: several independent problems (any dimension, size or degree)
+// whose reinit periods are captured into ONE CUDA graph, one branch per
+// problem, so that their kernels run side by side on the device.
+// ---------------------------------------------------------------------
+}  // extern "C"
+
+struct GroupGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int> cur_after;
+};
+
+struct flsp_group {
+  int dev = 0;
+  std::vector<flsp_handle*> h;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  std::map<unsigned long long, GroupGraph> graphs;
+};
+
+extern "C" {
+
+int flsp_group_create(flsp_handle* const* handles, int n, flsp_group** out) {
+  if (!handles || n < 1 || !out) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!handles[i]) return fail(FLSP_ERR_BAD_ARG, "null handle");
+    if (handles[i]->dev != handles[0]->dev) return fail(FLSP_ERR_BAD_ARG, "group members on different devices");
+    for (int j = 0; j < i; ++j)
+      if (handles[j] == handles[i]) return fail(FLSP_ERR_BAD_ARG, "a handle appears twice in the group");
+  }
+  flsp_group* g = new flsp_group();
+  g->dev = handles[0]->dev;
+  g->h.assign(handles, handles + n);
+  g->join.assign(n, nullptr);
+  cudaError_t e = cudaSetDevice(g->dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    flsp_group_destroy(g);
+    return fail(FLSP_ERR_CUDA, std::string("group: ") + cudaGetErrorString(e));
+  }
+  *out = g;
+  return FLSP_OK;
+}
+
+void flsp_group_destroy(flsp_group* g) {
+  if (!g) return;
+  cudaSetDevice(g->dev);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  for (auto& kv : g->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  for (cudaEvent_t ev : g->join)
+    if (ev) cudaEventDestroy(ev);
+  if (g->fork) cudaEventDestroy(g->fork);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) {
+  if (!g || !o || n_periods < 0) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  if (o->reinit_frequency < 1 || !o->execute_reinit || o->reinit.mode != FLSP_REINIT_FIXED)
+    return fail(FLSP_ERR_BAD_ARG, "group periods need a fixed-count reinit (FLSP_REINIT_FIXED)");
+  const flsp_reinit_opts ro = o->reinit;
+  const int n = (int)g->h.size();
+  CU(cudaSetDevice(g->dev));
+  for (flsp_handle* h : g->h) {
+    if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+    if (h->n_since_reinit != 0) return fail(FLSP_ERR_BAD_ARG, "a group member is inside a reinit period");
+    ST(validate_reinit(h, &ro));
+    if (ro.viscosity > 0.0) ST(ensure_ldg_buffers(h));
+    if (ro.narrow_band) ST(ensure_band_buffers(h));
+  }
+  // the group's stream waits for every member's earlier work
+  for (int i = 0; i < n; ++i) {
+    CU(cudaEventRecord(g->join[i], g->h[i]->stream));
+    CU(cudaStreamWaitEvent(g->stream, g->join[i], 0));
+  }
+  for (int it = 0; it < n_periods; ++it) {
+    unsigned long long key = 1469598103934665603ull;
+    auto mix = [&key](const void* p, size_t nb) {
+      const unsigned char* b = (const unsigned char*)p;
+      for (size_t i = 0; i < nb; ++i) { key ^= b[i]; key *= 1099511628211ull; }
+    };
+    for (flsp_handle* h : g->h) mix(&h->cur, sizeof(h->cur));
+    mix(&o->reinit_frequency, sizeof(o->reinit_frequency));
+    mix(&ro, sizeof(ro));
+    auto gi = g->graphs.find(key);
+    if (gi == g->graphs.end()) {
+      std::vector<int> cur0(n);
+      for (int i = 0; i < n; ++i) cur0[i] = g->h[i]->cur;
+      cudaGraph_t graph = nullptr;
+      CU(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+      int st = FLSP_OK;
+      cudaError_t ce = cudaEventRecord(g->fork, g->stream);
+      for (int i = 0; i < n && st == FLSP_OK && ce == cudaSuccess; ++i) {
+        flsp_handle* h = g->h[i];
+        ce = cudaStreamWaitEvent(h->stream, g->fork, 0);   // the member's stream joins the capture
+        if (ce == cudaSuccess) st = launch_adv_clock_horizon(h->stream, h->clk, INFINITY);
+        if (ce == cudaSuccess && st == FLSP_OK) st = enqueue_period(h, &ro, o->reinit_frequency);
+        if (ce == cudaSuccess) ce = cudaEventRecord(g->join[i], h->stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(g->stream, g->join[i], 0);
+      }
+      const cudaError_t ce2 = cudaStreamEndCapture(g->stream, &graph);
+      if (st != FLSP_OK || ce != cudaSuccess || ce2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        for (int i = 0; i < n; ++i) g->h[i]->cur = cur0[i];
+        if (st != FLSP_OK) return st;
+        return fail(FLSP_ERR_CUDA, std::string("group capture: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
+      }
+      GroupGraph gg;
+      gg.cur_after.resize(n);
+      for (int i = 0; i < n; ++i) {
+        gg.cur_after[i] = g->h[i]->cur;
+        g->h[i]->cur = cur0[i];
+      }
+      const cudaError_t ci = cudaGraphInstantiate(&gg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ci != cudaSuccess) return fail(FLSP_ERR_CUDA, std::string("group graph: ") + cudaGetErrorString(ci));
+      gi = g->graphs.emplace(key, gg).first;
+    }
+    CU(cudaGraphLaunch(gi->second.exec, g->stream));
+    for (int i = 0; i < n; ++i) g->h[i]->cur = gi->second.cur_after[i];
+  }
+  // every member's stream waits for the group's work
+  CU(cudaEventRecord(g->fork, g->stream));
+  for (flsp_handle* h : g->h) CU(cudaStreamWaitEvent(h->stream, g->fork, 0));
+  return FLSP_OK;
+}
+
+int flsp_group_sync(flsp_group* g) {
+  if (!g) return fail(FLSP_ERR_BAD_ARG, "null group");
+  CU(cudaSetDevice(g->dev));
+  CU(cudaStreamSynchronize(g->stream));
+  for (flsp_handle* h : g->h) ST(sync_clock(h));
+  return FLSP_OK;
+}
+
+int flsp_group_stream(const flsp_group* g, void** stream) {
+  if (!g || !stream) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  *stream = (void*)g->stream;
   return FLSP_OK;
 }
 

@@ -418,6 +418,25 @@ int flsp_batch_run_steps(flsp_batch* b, const flsp_ls_opts* o, int n_steps);
 int flsp_batch_sync(flsp_batch* b);
 int flsp_batch_stream(const flsp_batch* b, void** stream);
 
+/* ------------------------------------------------------------------
+   Groups.  No counterpart in the reference (FELSPA advances one problem
+   per simulator object).  A group holds several independent problems of
+   any dimension, mesh size or degree (regular handles, still owned by the
+   caller); a reinit period of every member (reinit_frequency substeps and
+   a fixed-count reinit) is captured into ONE CUDA graph with one branch
+   per member, so that small members fill the device beside a large one.
+   Every member must be at the start of a reinit period.  Work is enqueued
+   on the group's stream, ordered after the members' earlier work and
+   before their later work; flsp_group_sync waits for it.
+   ------------------------------------------------------------------ */
+typedef struct flsp_group flsp_group;
+
+int flsp_group_create(flsp_handle* const* handles, int n, flsp_group** out);
+void flsp_group_destroy(flsp_group* g);
+int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods);
+int flsp_group_sync(flsp_group* g);
+int flsp_group_stream(const flsp_group* g, void** stream);
+
 /* default option structs (reference defaults) */
 void flsp_default_dg_opts(flsp_dg_opts* o);
 void flsp_default_reinit_opts(flsp_reinit_opts* o);

@@ -143,3 +143,16 @@ def test_learned_and_batch_entry_points_without_gpu(flsp):
     lo = abi.LearnedOpts()
     L.flsp_default_learned_opts(C.byref(lo))
     assert (lo.band_cells, lo.max_residual, lo.fallback.mode, lo.fallback.narrow_band) == (6.0, 0.05, abi.REINIT_FIXED, 1)
+
+
+def test_group_entry_points_without_gpu(flsp):
+    """the group entry points reject bad arguments before touching a device"""
+    L = flsp.load()
+    g = C.c_void_p()
+    hs = (C.c_void_p * 1)(None)
+    assert L.flsp_group_create(hs, 0, C.byref(g)) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_group_create(hs, 1, C.byref(g)) == abi.FLSP_ERR_BAD_ARG   # a null member
+    ctl = abi.default_ls_opts()
+    assert L.flsp_group_run_periods(None, C.byref(ctl), 1) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_group_sync(None) == abi.FLSP_ERR_BAD_ARG
+    L.flsp_group_destroy(None)
