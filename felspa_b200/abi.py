@@ -151,6 +151,8 @@ class BatchTuning(C.Structure):
 
 
 MLP_IN, MLP_HIDDEN, MLP_OUT = 82, 256, 9
+MLP3_IN, MLP3_OUT = 730, 27
+PATCH_2D_Q2, PATCH_3D_Q2 = 0, 1
 
 
 class LSOpts(C.Structure):

@@ -626,13 +626,19 @@ int build_vtab(flsp_handle* h) {
 
 // ---- learned reinitialisation helpers
 int learned_check(const flsp_handle* h, const flsp_mlp* net) {
-  if (h->dim != 2 || h->p != 2 || h->basis != FLSP_BASIS_Q)
-    return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: 2D, degree 2, Q basis only");
-  if (std::fabs(h->m.h[0] - h->m.h[1]) > 1e-12 * h->m.h[0])
-    return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: square cells only");
+  if (h->p != 2 || h->basis != FLSP_BASIS_Q)
+    return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: degree 2, Q basis only");
+  for (int d = 1; d < h->dim; ++d)
+    if (std::fabs(h->m.h[0] - h->m.h[d]) > 1e-12 * h->m.h[0])
+      return fail(FLSP_ERR_UNSUPPORTED, "learned reinitialisation: square / cubic cells only");
   if (net && net->dev != h->dev) return fail(FLSP_ERR_BAD_ARG, "network and problem on different devices");
+  if (net && (h->dim == 3) != (net->patch == FLSP_PATCH_3D_Q2))
+    return fail(FLSP_ERR_BAD_ARG, "the network's patch is not of the problem's dimension");
   return FLSP_OK;
 }
+
+// network input width for the handle's dimension
+int learned_n_in(const flsp_handle* h) { return h->dim == 3 ? FLSP_MLP3_IN : FLSP_MLP_IN; }
 
 int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
   const int64_t ncell = h->m.ncell;
@@ -648,7 +654,7 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
   if (h->lrn_feat_cap < nfeat) {
     if (h->lrn_feat) cudaFree(h->lrn_feat);
     h->lrn_feat = nullptr;
-    CU(cudaMalloc(&h->lrn_feat, (size_t)nfeat * FLSP_MLP_IN * sizeof(float)));
+    CU(cudaMalloc(&h->lrn_feat, (size_t)nfeat * learned_n_in(h) * sizeof(float)));
     h->lrn_feat_cap = nfeat;
   }
   return FLSP_OK;
@@ -657,8 +663,8 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
 // band cells of the current state: |mean phi| <= band_cells * h; returns the count
 int select_band(flsp_handle* h, double band_cells, int64_t* n) {
   ST(ensure_learned_buffers(h, 0));
-  ST(launch_band_select(h->stream, h->prec, h->buf[h->cur], h->m.ncell, band_cells * h->m.h[0], h->lrn_flags,
-                        h->lrn_work, h->lrn_cells, h->lrn_count));
+  ST(launch_band_select(h->stream, h->prec, h->m.nb, h->buf[h->cur], h->m.ncell, band_cells * h->m.h[0],
+                        h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count));
   CU(cudaMemcpyAsync(h->lrn_count_host, h->lrn_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
   *n = h->lrn_count_host[0];
@@ -1235,13 +1241,13 @@ int flsp_mlp_collect(flsp_mlp* net, flsp_handle* h, double band_cells, const fls
   ST(select_band(h, band_cells, &n));
   ST(mlp_ensure_pairs(net, net->n_pairs + n));
   const double hh = h->m.h[0];
-  ST(launch_patch_features(h->stream, h->prec, h->buf[h->cur], h->m.n[0], h->m.n[1], hh, h->lrn_cells, n, nullptr,
-                           net->feat + net->n_pairs * FLSP_MLP_IN));
+  ST(launch_patch_features(h->stream, h->prec, h->dim, h->buf[h->cur], h->m.n, hh, h->lrn_cells, n, nullptr,
+                           net->feat + net->n_pairs * net->n_in));
   CU(cudaMemcpyAsync(h->lrn_save, h->buf[h->cur], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
   int nit = 0;
   ST(run_reinit(h, target, &nit));
-  ST(launch_patch_targets(h->stream, h->prec, h->lrn_save, h->buf[h->cur], hh, h->lrn_cells, n,
-                          net->targ + net->n_pairs * FLSP_MLP_OUT));
+  ST(launch_patch_targets(h->stream, h->prec, h->m.nb, h->lrn_save, h->buf[h->cur], hh, h->lrn_cells, n,
+                          net->targ + net->n_pairs * net->n_out));
   CU(cudaStreamSynchronize(h->stream));
   net->n_pairs += n;
   if (n_added) *n_added = n;
@@ -1275,9 +1281,9 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   const int pre = h->cur;
   const int out = other(pre, -1);
   const int* nband = h->lrn_count;
-  ST(launch_band_select(h->stream, h->prec, h->buf[pre], ncell, o->band_cells * hh, h->lrn_flags, h->lrn_work,
-                        h->lrn_cells, h->lrn_count));
-  ST(launch_patch_features(h->stream, h->prec, h->buf[pre], h->m.n[0], h->m.n[1], hh, h->lrn_cells, ncell, nband,
+  ST(launch_band_select(h->stream, h->prec, h->m.nb, h->buf[pre], ncell, o->band_cells * hh, h->lrn_flags,
+                        h->lrn_work, h->lrn_cells, h->lrn_count));
+  ST(launch_patch_features(h->stream, h->prec, h->dim, h->buf[pre], h->m.n, hh, h->lrn_cells, ncell, nband,
                            h->lrn_feat));
   {
     // the network runs on its own stream: order it after the features and back
@@ -1292,10 +1298,10 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
     cudaEventDestroy(ev);
     ST(st);
   }
-  ST(launch_apply_delta(h->stream, h->prec, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, ncell, nband,
-                        net->y, 16));
+  ST(launch_apply_delta(h->stream, h->prec, h->m.nb, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, ncell,
+                        nband, net->y, net->y_ld));
   // band cells whose result is not distance-like enough take the HJ sweep
-  ST(launch_residual_flags(h->stream, h->prec, h->buf[out], h->m.n[0], hh, h->lrn_cells, ncell, nband,
+  ST(launch_residual_flags(h->stream, h->prec, h->dim, h->buf[out], hh, h->lrn_cells, ncell, nband,
                            o->max_residual, h->lrn_flags, h->lrn_count + 1));
   CU(cudaMemcpyAsync(h->lrn_count_host, h->lrn_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(h->lrn_count_host + 2, net->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1312,8 +1318,8 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
     const int hj = h->cur;
     const int res = other(hj, -1);
     CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
-    ST(launch_merge_cells(h->stream, h->prec, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, stl.n_band,
-                          nullptr));
+    ST(launch_merge_cells(h->stream, h->prec, h->m.nb, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags,
+                          stl.n_band, nullptr));
     h->cur = res;
     stl.hj_ran = 1;
     CU(cudaStreamSynchronize(h->stream));

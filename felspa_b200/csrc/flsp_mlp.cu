@@ -79,11 +79,15 @@ __global__ void k_transpose_packed(const __nv_bfloat16* __restrict__ src, int R,
 }
 
 // output-layer gradient, packed R x 64: g = dy[r][n] (given) or
-// 2 (y - t) / (B * 9) (MSE of the batch); per-block loss and column sums
+// 2 (y - t) / (B * OUT) (MSE of the batch); per-block loss and column sums
+// (col_part row stride ldy)
+template <int OUT>
 __global__ void k_out_grad(const float* __restrict__ y, int ldy, const float* __restrict__ dy,
                            const float* __restrict__ targ, const int* __restrict__ idx, int B, int R,
                            __nv_bfloat16* __restrict__ gout, double* __restrict__ loss_part,
                            float* __restrict__ col_part) {
+  constexpr int kMlpOut = OUT;
+  static_assert(OUT <= 64, "output gradient rows are 64 wide");
   __shared__ double sl[256];
   __shared__ float sc[256][kMlpOut];
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -120,10 +124,10 @@ __global__ void k_out_grad(const float* __restrict__ y, int ldy, const float* __
   for (int n = 0; n < kMlpOut; ++n) sc[threadIdx.x][n] = gv[n];
   __syncthreads();
   if (threadIdx.x < kMlpOut + 1) {
-    // fixed-order sums: thread n < 9 sums column n, thread 9 the loss
+    // fixed-order sums: thread n < OUT sums column n, thread OUT the loss
     double s = 0.0;
     for (int i = 0; i < (int)blockDim.x; ++i) s += threadIdx.x < kMlpOut ? (double)sc[i][threadIdx.x] : sl[i];
-    if (threadIdx.x < kMlpOut) col_part[(long long)blockIdx.x * 16 + threadIdx.x] = (float)s;
+    if (threadIdx.x < kMlpOut) col_part[(long long)blockIdx.x * ldy + threadIdx.x] = (float)s;
     else loss_part[blockIdx.x] = s;
   }
 }
@@ -157,47 +161,53 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __re
   }
 }
 
-// ---- level-set patch kernels (2D, degree 2, Q basis: 9 coefficients / cell)
-template <typename T>
-__global__ void k_patch_features(const T* __restrict__ s, int nx, int ny, float ih, float hfeat,
+// ---- level-set patch kernels (degree 2, Q basis: NB = 3^dim coefficients
+// per cell, lexicographic cells)
+// one thread per (listed cell, patch cell): the patch cell's coefficients
+// over h; the centre cell also writes 64 h at the end of the row.  Patch
+// cells outside the domain repeat the nearest inside cell.
+template <int DIM, typename T>
+__global__ void k_patch_features(const T* __restrict__ s, int nx, int ny, int nz, float ih, float hfeat,
                                  const int* __restrict__ cells, long long n, const int* __restrict__ n_dev,
                                  float* __restrict__ feat) {
+  constexpr int NB = DIM == 2 ? 9 : 27, NP = DIM == 2 ? 9 : 27, NIN = NP * NB + 1;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n_dev) n = min(n, (long long)*n_dev);
-  if (t >= n * 9) return;
-  const long long i = t / 9;
-  const int j = (int)(t % 9);   // patch cell: dy outer, dx inner
-  const int c = cells[i];
-  const int cx = c % nx, cy = c / nx;
-  const int px = min(max(cx + j % 3 - 1, 0), nx - 1), py = min(max(cy + j / 3 - 1, 0), ny - 1);
-  const T* src = s + ((long long)py * nx + px) * 9;
-  float* dst = feat + i * kMlpIn + j * 9;
+  if (t >= n * NP) return;
+  const long long i = t / NP;
+  const int j = (int)(t % NP);   // patch cell: z outer, y, x inner
+  const long long c = cells[i];
+  const int cx = (int)(c % nx), cy = (int)((c / nx) % ny), cz = DIM > 2 ? (int)(c / ((long long)nx * ny)) : 0;
+  const int px = min(max(cx + j % 3 - 1, 0), nx - 1), py = min(max(cy + (j / 3) % 3 - 1, 0), ny - 1);
+  const int pz = DIM > 2 ? min(max(cz + j / 9 - 1, 0), nz - 1) : 0;
+  const T* src = s + (((long long)pz * ny + py) * nx + px) * NB;
+  float* dst = feat + i * NIN + j * NB;
 #pragma unroll
-  for (int q = 0; q < 9; ++q) dst[q] = (float)src[q] * ih;
-  if (j == 4) feat[i * kMlpIn + 81] = hfeat;
+  for (int q = 0; q < NB; ++q) dst[q] = (float)src[q] * ih;
+  if (j == NP / 2) feat[i * NIN + NIN - 1] = hfeat;
 }
 
 template <typename T>
-__global__ void k_patch_targets(const T* __restrict__ pre, const T* __restrict__ post, float ih,
+__global__ void k_patch_targets(const T* __restrict__ pre, const T* __restrict__ post, int nb, float ih,
                                 const int* __restrict__ cells, long long n, float* __restrict__ targ) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= n * 9) return;
-  const long long i = t / 9;
-  const int q = (int)(t % 9);
+  if (t >= n * nb) return;
+  const long long i = t / nb;
+  const int q = (int)(t % nb);
   const long long c = cells[i];
-  targ[i * 9 + q] = (float)((double)post[c * 9 + q] - (double)pre[c * 9 + q]) * ih;
+  targ[i * nb + q] = (float)((double)post[c * nb + q] - (double)pre[c * nb + q]) * ih;
 }
 
 template <typename T>
-__global__ void k_apply_delta(T* __restrict__ out, double h, const int* __restrict__ cells, long long n,
+__global__ void k_apply_delta(T* __restrict__ out, int nb, double h, const int* __restrict__ cells, long long n,
                               const int* __restrict__ n_dev, const float* __restrict__ y, int ldy) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n_dev) n = min(n, (long long)*n_dev);
-  if (t >= n * 9) return;
-  const long long i = t / 9;
-  const int q = (int)(t % 9);
+  if (t >= n * nb) return;
+  const long long i = t / nb;
+  const int q = (int)(t % nb);
   const long long c = cells[i];
-  out[c * 9 + q] = (T)((double)out[c * 9 + q] + h * (double)y[i * ldy + q]);
+  out[c * nb + q] = (T)((double)out[c * nb + q] + h * (double)y[i * ldy + q]);
 }
 
 // band flags and per-block counts (256 cells per block)
@@ -235,48 +245,63 @@ __global__ void k_band_compact(const int* __restrict__ flags, long long ncell, c
 }
 
 // mean of ||grad phi| - 1| over the 3 x 3 Gauss points of each listed cell
-template <typename T>
+// mean over the cell's 3^dim Gauss points of ||grad phi| - 1| (degree-2
+// Legendre modes on [0,1] per axis, Q layout a + 3 b (+ 9 c))
+template <int DIM, typename T>
 __global__ void k_residual(const T* __restrict__ s, double ih, const int* __restrict__ cells, long long n,
                            const int* __restrict__ n_dev, double thr, int* __restrict__ flags, int* __restrict__ count) {
+  constexpr int NB = DIM == 2 ? 9 : 27;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n_dev) n = min(n, (long long)*n_dev);
   if (i >= n) return;
-  const T* c = s + (long long)cells[i] * 9;
+  const T* c = s + (long long)cells[i] * NB;
   const double g[3] = {0.5 - 0.5 * 0.7745966692414834, 0.5, 0.5 + 0.5 * 0.7745966692414834};
   const double w[3] = {5.0 / 18.0, 8.0 / 18.0, 5.0 / 18.0};
   const double r3 = 1.7320508075688772, r5 = 2.23606797749979;
+  double Lv[3][3], Dv[3][3];   // [point][mode]
+  for (int k = 0; k < 3; ++k) {
+    const double x = g[k];
+    Lv[k][0] = 1.0;
+    Lv[k][1] = r3 * (2 * x - 1);
+    Lv[k][2] = r5 * (6 * x * x - 6 * x + 1);
+    Dv[k][0] = 0.0;
+    Dv[k][1] = 2 * r3;
+    Dv[k][2] = r5 * (12 * x - 6);
+  }
   double acc = 0.0;
-  for (int qy = 0; qy < 3; ++qy)
-    for (int qx = 0; qx < 3; ++qx) {
-      const double x = g[qx], y = g[qy];
-      const double Lx[3] = {1.0, r3 * (2 * x - 1), r5 * (6 * x * x - 6 * x + 1)};
-      const double Ly[3] = {1.0, r3 * (2 * y - 1), r5 * (6 * y * y - 6 * y + 1)};
-      const double Dx[3] = {0.0, 2 * r3, r5 * (12 * x - 6)};
-      const double Dy[3] = {0.0, 2 * r3, r5 * (12 * y - 6)};
-      double gx = 0.0, gy = 0.0;
-      for (int b = 0; b < 3; ++b)
-        for (int a = 0; a < 3; ++a) {
-          gx += (double)c[a + 3 * b] * Dx[a] * Ly[b];
-          gy += (double)c[a + 3 * b] * Lx[a] * Dy[b];
+  for (int qz = 0; qz < (DIM > 2 ? 3 : 1); ++qz)
+    for (int qy = 0; qy < 3; ++qy)
+      for (int qx = 0; qx < 3; ++qx) {
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+        for (int cc = 0; cc < (DIM > 2 ? 3 : 1); ++cc) {
+          const double lz = DIM > 2 ? Lv[qz][cc] : 1.0, dz = DIM > 2 ? Dv[qz][cc] : 0.0;
+          for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+              const double v = (double)c[a + 3 * b + 9 * cc];
+              gx += v * Dv[qx][a] * Lv[qy][b] * lz;
+              gy += v * Lv[qx][a] * Dv[qy][b] * lz;
+              gz += v * Lv[qx][a] * Lv[qy][b] * dz;
+            }
         }
-      acc += w[qx] * w[qy] * fabs(sqrt(gx * gx + gy * gy) * ih - 1.0);
-    }
+        const double wq = w[qx] * w[qy] * (DIM > 2 ? w[qz] : 1.0);
+        acc += wq * fabs(sqrt(gx * gx + gy * gy + gz * gz) * ih - 1.0);
+      }
   const int f = acc > thr ? 1 : 0;
   flags[i] = f;
   if (f) atomicAdd(count, 1);
 }
 
 template <typename T>
-__global__ void k_merge(const T* __restrict__ src, T* __restrict__ out, const int* __restrict__ cells,
+__global__ void k_merge(const T* __restrict__ src, T* __restrict__ out, int nb, const int* __restrict__ cells,
                         const int* __restrict__ flags, long long n, const int* __restrict__ n_dev) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (n_dev) n = min(n, (long long)*n_dev);
-  if (t >= n * 9) return;
-  const long long i = t / 9;
+  if (t >= n * nb) return;
+  const long long i = t / nb;
   if (!flags[i]) return;
   const long long c = cells[i];
-  const int q = (int)(t % 9);
-  out[c * 9 + q] = src[c * 9 + q];
+  const int q = (int)(t % nb);
+  out[c * nb + q] = src[c * nb + q];
 }
 
 // ------------------------------------------------------------------ GEMM launch
@@ -316,18 +341,18 @@ int mlp_ensure_cap(flsp_mlp* net, int64_t rows) {
   fr(net->colsum); fr(net->loss_part);
   net->cap = 0;
   const size_t c = (size_t)need;
-  MCU(cudaMalloc(&net->x, c * 128 * 2));
+  MCU(cudaMalloc(&net->x, c * net->k_in * 2));
   for (int i = 0; i < 4; ++i) {
     MCU(cudaMalloc(&net->act[i], c * 256 * 2));
     MCU(cudaMalloc(&net->gd[i], c * 256 * 4));
   }
-  MCU(cudaMalloc(&net->y, c * 16 * 4));
+  MCU(cudaMalloc(&net->y, c * net->y_ld * 4));
   MCU(cudaMalloc(&net->gout, c * 64 * 2));
   MCU(cudaMalloc(&net->gh[0], c * 256 * 2));
   MCU(cudaMalloc(&net->gh[1], c * 256 * 2));
-  MCU(cudaMalloc(&net->tA, c * 256 * 2));
+  MCU(cudaMalloc(&net->tA, c * std::max(256, net->k_in) * 2));
   MCU(cudaMalloc(&net->tG, c * 256 * 2));
-  MCU(cudaMalloc(&net->colsum, (c / 32) * 256 * 4));
+  MCU(cudaMalloc(&net->colsum, (c / 32 + 1) * 256 * 4));
   MCU(cudaMalloc(&net->loss_part, (c / 256 + 1) * 8));
   net->cap = need;
   return FLSP_OK;
@@ -337,11 +362,12 @@ int mlp_ensure_pairs(flsp_mlp* net, int64_t n) {
   if (net->pair_cap >= n) return FLSP_OK;
   const int64_t cap = std::max<int64_t>(n, std::max<int64_t>(2 * net->pair_cap, 1 << 16));
   float *f = nullptr, *t = nullptr;
-  MCU(cudaMalloc(&f, (size_t)cap * kMlpIn * 4));
-  MCU(cudaMalloc(&t, (size_t)cap * kMlpOut * 4));
+  MCU(cudaMalloc(&f, (size_t)cap * net->n_in * 4));
+  MCU(cudaMalloc(&t, (size_t)cap * net->n_out * 4));
   if (net->n_pairs) {
-    MCU(cudaMemcpyAsync(f, net->feat, (size_t)net->n_pairs * kMlpIn * 4, cudaMemcpyDeviceToDevice, net->stream));
-    MCU(cudaMemcpyAsync(t, net->targ, (size_t)net->n_pairs * kMlpOut * 4, cudaMemcpyDeviceToDevice, net->stream));
+    MCU(cudaMemcpyAsync(f, net->feat, (size_t)net->n_pairs * net->n_in * 4, cudaMemcpyDeviceToDevice, net->stream));
+    MCU(cudaMemcpyAsync(t, net->targ, (size_t)net->n_pairs * net->n_out * 4, cudaMemcpyDeviceToDevice,
+                        net->stream));
     MCU(cudaStreamSynchronize(net->stream));
   }
   if (net->feat) cudaFree(net->feat);
@@ -376,7 +402,8 @@ static int repack(flsp_mlp* net) {
 
 int mlp_pack_input(flsp_mlp* net, const float* feat, const int* idx, int64_t n, const int* rows_dev) {
   const long long R = round128(n);
-  k_pack<<<grid_of(R * 128), 256, 0, net->stream>>>(feat, idx, kMlpIn, 1, (int)n, kMlpIn, 1.0f, net->x, (int)R, 128,
+  k_pack<<<grid_of(R * net->k_in), 256, 0, net->stream>>>(feat, idx, net->n_in, 1, (int)n, net->n_in, 1.0f, net->x,
+                                                          (int)R, net->k_in,
                                                     rows_dev);
   return launch_status("k_pack");
 }
@@ -410,8 +437,8 @@ int mlp_forward_dev(flsp_mlp* net, int64_t n, bool train, const int* rows_dev) {
   a.K = net->L[4].k_pad;
   a.bias = net->bp[4];
   a.y = net->y;
-  a.ldy = 16;
-  a.n_valid = 16;
+  a.ldy = net->y_ld;
+  a.n_valid = net->y_ld;
   a.m_valid = R;
   a.err = net->err;
   a.rows_dev = rows_dev;
@@ -432,21 +459,27 @@ static int mlp_backward_dev(flsp_mlp* net, int64_t n) {
     const int grows = l == kMlpLayers - 1 ? 128 : 256;   // padded output rows (M of the GEMM)
     MST(transpose(st, G, R, l == kMlpLayers - 1 ? 64 : 256, net->tG, grows));
     const __nv_bfloat16* Ain = l == 0 ? net->x : net->act[l - 1];
-    const int ain_k = l == 0 ? 128 : 256;
+    const int ain_k = l == 0 ? net->k_in : 256;
     MST(transpose(st, Ain, R, ain_k, net->tA, ain_k));
-    TcGemmArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.A = net->tG;
-    a.B = net->tA;
-    a.M = grows;
-    a.N = ain_k;
-    a.K = R;
-    a.y = net->g + L.w_off;
-    a.ldy = L.n_in;
-    a.n_valid = L.n_in;
-    a.m_valid = L.n_out;
-    a.err = net->err;
-    MST(gemm<kEpiStoreF32>(st, a));
+    // wide inputs (the 3D patch): column blocks of at most 256 inputs, each
+    // a row block of the transposed input
+    for (int c0 = 0; c0 < ain_k; c0 += 256) {
+      TcGemmArgs a;
+      std::memset(&a, 0, sizeof(a));
+      a.A = net->tG;
+      a.B = net->tA;
+      a.b_rows = ain_k;
+      a.b_row0 = c0;
+      a.M = grows;
+      a.N = std::min(256, ain_k - c0);
+      a.K = R;
+      a.y = net->g + L.w_off + c0;
+      a.ldy = L.n_in;
+      a.n_valid = std::min(a.N, L.n_in - c0);
+      a.m_valid = L.n_out;
+      a.err = net->err;
+      if (a.n_valid > 0) MST(gemm<kEpiStoreF32>(st, a));
+    }
     if (l == 0) break;
     // G_{l-1} = (G W_l) * GELU'(z_{l-1}), with its column sums -> db_{l-1}
     TcGemmArgs b;
@@ -471,13 +504,23 @@ static int mlp_backward_dev(flsp_mlp* net, int64_t n) {
   return FLSP_OK;
 }
 
+// the output-layer gradient kernel for the network's width
+static void out_grad_launch(flsp_mlp* net, int nblk, const float* dy, const float* targ, const int* idx, int n,
+                            int R) {
+  if (net->n_out == FLSP_MLP3_OUT)
+    k_out_grad<FLSP_MLP3_OUT><<<nblk, 256, 0, net->stream>>>(net->y, net->y_ld, dy, targ, idx, n, R, net->gout,
+                                                             net->loss_part, net->colsum);
+  else
+    k_out_grad<kMlpOut><<<nblk, 256, 0, net->stream>>>(net->y, net->y_ld, dy, targ, idx, n, R, net->gout,
+                                                       net->loss_part, net->colsum);
+}
+
 static int output_grad(flsp_mlp* net, int64_t n, const float* dy_dev, const int* idx) {
   const int R = (int)round128(n);
   const int nblk = R / 256 + 1;
-  k_out_grad<<<nblk, 256, 0, net->stream>>>(net->y, 16, dy_dev, net->targ, idx, (int)n, R, net->gout,
-                                            net->loss_part, net->colsum);
+  out_grad_launch(net, nblk, dy_dev, net->targ, idx, (int)n, R);
   MST(launch_status("k_out_grad"));
-  k_colsum<<<1, 32, 0, net->stream>>>(net->colsum, nblk, 16, kMlpOut, net->g + net->L[4].b_off);
+  k_colsum<<<1, 32, 0, net->stream>>>(net->colsum, nblk, net->y_ld, net->n_out, net->g + net->L[4].b_off);
   MST(launch_status("k_colsum"));
   k_sum_double<<<1, 1, 0, net->stream>>>(net->loss_part, nblk, net->loss_dev);
   return launch_status("k_sum_double");
@@ -536,8 +579,21 @@ void flsp_mlp_destroy(flsp_mlp* net) {
 }
 
 int flsp_mlp_create(int device, uint64_t seed, flsp_mlp** out) {
+  return flsp_mlp_create_patch(FLSP_PATCH_2D_Q2, device, seed, out);
+}
+
+int flsp_mlp_info(const flsp_mlp* net, int* n_in, int* n_out, int64_t* n_params) {
+  if (!net) return set_error(FLSP_ERR_BAD_ARG, "null argument");
+  if (n_in) *n_in = net->n_in;
+  if (n_out) *n_out = net->n_out;
+  if (n_params) *n_params = net->n_params;
+  return FLSP_OK;
+}
+
+int flsp_mlp_create_patch(int patch, int device, uint64_t seed, flsp_mlp** out) {
   if (!out) return set_error(FLSP_ERR_BAD_ARG, "null argument");
   *out = nullptr;
+  if (patch != FLSP_PATCH_2D_Q2 && patch != FLSP_PATCH_3D_Q2) return set_error(FLSP_ERR_BAD_ARG, "bad patch kind");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(FLSP_ERR_NO_DEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return set_error(FLSP_ERR_BAD_ARG, "bad device ordinal");
@@ -547,11 +603,16 @@ int flsp_mlp_create(int device, uint64_t seed, flsp_mlp** out) {
   MCU(cudaSetDevice(device));
   flsp_mlp* net = new flsp_mlp();
   net->dev = device;
+  net->patch = patch;
+  net->n_in = patch == FLSP_PATCH_3D_Q2 ? FLSP_MLP3_IN : kMlpIn;
+  net->n_out = patch == FLSP_PATCH_3D_Q2 ? FLSP_MLP3_OUT : kMlpOut;
+  net->k_in = ((net->n_in + 63) / 64) * 64;
+  net->y_ld = ((net->n_out + 15) / 16) * 16;
   auto fail_destroy = [&](int code) { flsp_mlp_destroy(net); return code; };
   if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail_destroy(set_error(FLSP_ERR_CUDA, "stream creation failed"));
-  const int nin[kMlpLayers] = {kMlpIn, kMlpHidden, kMlpHidden, kMlpHidden, kMlpHidden};
-  const int nout[kMlpLayers] = {kMlpHidden, kMlpHidden, kMlpHidden, kMlpHidden, kMlpOut};
+  const int nin[kMlpLayers] = {net->n_in, kMlpHidden, kMlpHidden, kMlpHidden, kMlpHidden};
+  const int nout[kMlpLayers] = {kMlpHidden, kMlpHidden, kMlpHidden, kMlpHidden, net->n_out};
   size_t off = 0;
   for (int l = 0; l < kMlpLayers; ++l) {
     MlpLayer& L = net->L[l];
@@ -630,17 +691,18 @@ int flsp_mlp_forward(flsp_mlp* net, const float* x, int64_t batch, float* y) {
   if (batch <= 0 || batch > (1LL << 24)) return set_error(FLSP_ERR_BAD_ARG, "bad batch size");
   MCU(cudaSetDevice(net->dev));
   MST(mlp_ensure_cap(net, batch));
-  MST(ensure_hbuf(net, (size_t)batch * kMlpIn * 4));
+  const size_t xb = (size_t)batch * net->n_in * 4;
+  MST(ensure_hbuf(net, xb));
   float* fdev = nullptr;
-  MCU(cudaMallocAsync(&fdev, (size_t)batch * kMlpIn * 4, net->stream));
-  std::memcpy(net->hbuf, x, (size_t)batch * kMlpIn * 4);
-  cudaMemcpyAsync(fdev, net->hbuf, (size_t)batch * kMlpIn * 4, cudaMemcpyHostToDevice, net->stream);
+  MCU(cudaMallocAsync(&fdev, xb, net->stream));
+  std::memcpy(net->hbuf, x, xb);
+  cudaMemcpyAsync(fdev, net->hbuf, xb, cudaMemcpyHostToDevice, net->stream);
   int st = mlp_pack_input(net, fdev, nullptr, batch, nullptr);
   if (st == FLSP_OK) st = mlp_forward_dev(net, batch, false, nullptr);
   cudaFreeAsync(fdev, net->stream);
   MST(st);
   MST(check_err(net));
-  MCU(cudaMemcpy2DAsync(y, kMlpOut * 4, net->y, 16 * 4, kMlpOut * 4, (size_t)batch, cudaMemcpyDeviceToHost,
+  MCU(cudaMemcpy2DAsync(y, net->n_out * 4, net->y, net->y_ld * 4, net->n_out * 4, (size_t)batch, cudaMemcpyDeviceToHost,
                         net->stream));
   MCU(cudaStreamSynchronize(net->stream));
   return FLSP_OK;
@@ -652,10 +714,10 @@ int flsp_mlp_backward(flsp_mlp* net, const float* x, const float* dy, int64_t ba
   MCU(cudaSetDevice(net->dev));
   MST(mlp_ensure_cap(net, batch));
   float *fdev = nullptr, *dydev = nullptr;
-  MCU(cudaMallocAsync(&fdev, (size_t)batch * kMlpIn * 4, net->stream));
-  MCU(cudaMallocAsync(&dydev, (size_t)batch * kMlpOut * 4, net->stream));
-  MCU(cudaMemcpyAsync(fdev, x, (size_t)batch * kMlpIn * 4, cudaMemcpyHostToDevice, net->stream));
-  MCU(cudaMemcpyAsync(dydev, dy, (size_t)batch * kMlpOut * 4, cudaMemcpyHostToDevice, net->stream));
+  MCU(cudaMallocAsync(&fdev, (size_t)batch * net->n_in * 4, net->stream));
+  MCU(cudaMallocAsync(&dydev, (size_t)batch * net->n_out * 4, net->stream));
+  MCU(cudaMemcpyAsync(fdev, x, (size_t)batch * net->n_in * 4, cudaMemcpyHostToDevice, net->stream));
+  MCU(cudaMemcpyAsync(dydev, dy, (size_t)batch * net->n_out * 4, cudaMemcpyHostToDevice, net->stream));
   int st = mlp_pack_input(net, fdev, nullptr, batch, nullptr);
   if (st == FLSP_OK) st = mlp_forward_dev(net, batch, true, nullptr);
   if (st == FLSP_OK) st = output_grad(net, batch, dydev, nullptr);
@@ -742,7 +804,7 @@ int flsp_mlp_train(flsp_mlp* net, const flsp_train_opts* o, double* loss) {
       double s = 0.0;
       MCU(cudaMemcpyAsync(&s, net->loss_dev, sizeof(double), cudaMemcpyDeviceToHost, net->stream));
       MCU(cudaStreamSynchronize(net->stream));
-      last = s / ((double)B * kMlpOut);
+      last = s / ((double)B * net->n_out);
     }
   }
   MST(check_err(net));
@@ -759,13 +821,12 @@ int flsp_mlp_eval(flsp_mlp* net, double* loss) {
   double total = 0.0;
   for (int64_t p0 = 0; p0 < net->n_pairs; p0 += chunk) {
     const int64_t n = std::min<int64_t>(chunk, net->n_pairs - p0);
-    MST(mlp_pack_input(net, net->feat + p0 * kMlpIn, nullptr, n, nullptr));
+    MST(mlp_pack_input(net, net->feat + p0 * net->n_in, nullptr, n, nullptr));
     MST(mlp_forward_dev(net, n, false, nullptr));
     // loss only (the gradient buffers are scratch here)
     const int R = (int)round128(n);
     const int nblk = R / 256 + 1;
-    k_out_grad<<<nblk, 256, 0, net->stream>>>(net->y, 16, nullptr, net->targ + p0 * kMlpOut, nullptr, (int)n, R,
-                                              net->gout, net->loss_part, net->colsum);
+    out_grad_launch(net, nblk, nullptr, net->targ + p0 * net->n_out, nullptr, (int)n, R);
     MST(launch_status("k_out_grad"));
     k_sum_double<<<1, 1, 0, net->stream>>>(net->loss_part, nblk, net->loss_dev);
     double s = 0.0;
@@ -774,7 +835,7 @@ int flsp_mlp_eval(flsp_mlp* net, double* loss) {
     total += s;
   }
   MST(check_err(net));
-  *loss = total / ((double)net->n_pairs * kMlpOut);
+  *loss = total / ((double)net->n_pairs * net->n_out);
   return FLSP_OK;
 }
 
@@ -785,45 +846,51 @@ namespace flsp {
 
 #define DISPATCH_T(prec, F) ((prec) == FLSP_FP64 ? F(double) : F(float))
 
-int launch_patch_features(cudaStream_t s, int prec, const void* state, int nx, int ny, double h, const int* cells,
-                          int64_t n, const int* n_dev, float* feat) {
+int launch_patch_features(cudaStream_t s, int prec, int dim, const void* state, const int* n_cells, double h,
+                          const int* cells, int64_t n, const int* n_dev, float* feat) {
   if (n <= 0) return FLSP_OK;
-  const long long t = n * 9;
+  const long long t = n * (dim == 2 ? 9 : 27);
   const int blocks = (int)((t + 255) / 256);
-#define L_(T) (k_patch_features<T><<<blocks, 256, 0, s>>>((const T*)state, nx, ny, (float)(1.0 / h), (float)(64.0 * h), cells, n, n_dev, feat), 0)
+  const int nx = n_cells[0], ny = n_cells[1], nz = dim > 2 ? n_cells[2] : 1;
+  const float ih = (float)(1.0 / h), hf = (float)(64.0 * h);
+#define L_(T)                                                                                                   \
+  (dim == 2 ? (k_patch_features<2, T><<<blocks, 256, 0, s>>>((const T*)state, nx, ny, nz, ih, hf, cells, n, n_dev, \
+                                                             feat), 0)                                          \
+            : (k_patch_features<3, T><<<blocks, 256, 0, s>>>((const T*)state, nx, ny, nz, ih, hf, cells, n, n_dev, \
+                                                             feat), 0))
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_patch_features");
 }
 
-int launch_patch_targets(cudaStream_t s, int prec, const void* pre, const void* post, double h, const int* cells,
-                         int64_t n, float* targ) {
+int launch_patch_targets(cudaStream_t s, int prec, int nb, const void* pre, const void* post, double h,
+                         const int* cells, int64_t n, float* targ) {
   if (n <= 0) return FLSP_OK;
-  const int blocks = (int)((n * 9 + 255) / 256);
-#define L_(T) (k_patch_targets<T><<<blocks, 256, 0, s>>>((const T*)pre, (const T*)post, (float)(1.0 / h), cells, n, targ), 0)
+  const int blocks = (int)((n * nb + 255) / 256);
+#define L_(T) (k_patch_targets<T><<<blocks, 256, 0, s>>>((const T*)pre, (const T*)post, nb, (float)(1.0 / h), cells, n, targ), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_patch_targets");
 }
 
-int launch_apply_delta(cudaStream_t s, int prec, const void* pre, void* out, int64_t ndofs, double h, const int* cells,
-                       int64_t n, const int* n_dev, const float* y, int ldy) {
+int launch_apply_delta(cudaStream_t s, int prec, int nb, const void* pre, void* out, int64_t ndofs, double h,
+                       const int* cells, int64_t n, const int* n_dev, const float* y, int ldy) {
   const size_t es = prec == FLSP_FP64 ? 8 : 4;
   if (pre != out) MCU(cudaMemcpyAsync(out, pre, (size_t)ndofs * es, cudaMemcpyDeviceToDevice, s));
   if (n <= 0) return FLSP_OK;
-  const int blocks = (int)((n * 9 + 255) / 256);
-#define L_(T) (k_apply_delta<T><<<blocks, 256, 0, s>>>((T*)out, h, cells, n, n_dev, y, ldy), 0)
+  const int blocks = (int)((n * nb + 255) / 256);
+#define L_(T) (k_apply_delta<T><<<blocks, 256, 0, s>>>((T*)out, nb, h, cells, n, n_dev, y, ldy), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_apply_delta");
 }
 
-int launch_band_select(cudaStream_t s, int prec, const void* state, int64_t ncell, double thr, int* flags, int* work,
-                       int* cells, int* count_dev) {
+int launch_band_select(cudaStream_t s, int prec, int nb, const void* state, int64_t ncell, double thr, int* flags,
+                       int* work, int* cells, int* count_dev) {
   const int nblk = (int)((ncell + 255) / 256);
   int* bcount = work;
   int* boff = work + nblk;
-#define L_(T) (k_band_count<T><<<nblk, 256, 0, s>>>((const T*)state, ncell, 9, thr, flags, bcount), 0)
+#define L_(T) (k_band_count<T><<<nblk, 256, 0, s>>>((const T*)state, ncell, nb, thr, flags, bcount), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   MST(launch_status("k_band_count"));
@@ -833,23 +900,26 @@ int launch_band_select(cudaStream_t s, int prec, const void* state, int64_t ncel
   return launch_status("k_band_compact");
 }
 
-int launch_residual_flags(cudaStream_t s, int prec, const void* state, int nx, double h, const int* cells, int64_t n,
-                          const int* n_dev, double thr, int* flags, int* count_dev) {
-  (void)nx;
+int launch_residual_flags(cudaStream_t s, int prec, int dim, const void* state, double h, const int* cells,
+                          int64_t n, const int* n_dev, double thr, int* flags, int* count_dev) {
   MCU(cudaMemsetAsync(count_dev, 0, sizeof(int), s));
   if (n <= 0) return FLSP_OK;
   const int blocks = (int)((n + 127) / 128);
-#define L_(T) (k_residual<T><<<blocks, 128, 0, s>>>((const T*)state, 1.0 / h, cells, n, n_dev, thr, flags, count_dev), 0)
+#define L_(T)                                                                                                   \
+  (dim == 2 ? (k_residual<2, T><<<blocks, 128, 0, s>>>((const T*)state, 1.0 / h, cells, n, n_dev, thr, flags,     \
+                                                       count_dev), 0)                                          \
+            : (k_residual<3, T><<<blocks, 128, 0, s>>>((const T*)state, 1.0 / h, cells, n, n_dev, thr, flags,     \
+                                                       count_dev), 0))
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_residual");
 }
 
-int launch_merge_cells(cudaStream_t s, int prec, const void* src, void* out, const int* cells, const int* flags,
-                       int64_t n, const int* n_dev) {
+int launch_merge_cells(cudaStream_t s, int prec, int nb, const void* src, void* out, const int* cells,
+                       const int* flags, int64_t n, const int* n_dev) {
   if (n <= 0) return FLSP_OK;
-  const int blocks = (int)((n * 9 + 255) / 256);
-#define L_(T) (k_merge<T><<<blocks, 256, 0, s>>>((const T*)src, (T*)out, cells, flags, n, n_dev), 0)
+  const int blocks = (int)((n * nb + 255) / 256);
+#define L_(T) (k_merge<T><<<blocks, 256, 0, s>>>((const T*)src, (T*)out, nb, cells, flags, n, n_dev), 0)
   DISPATCH_T(prec, L_);
 #undef L_
   return launch_status("k_merge");

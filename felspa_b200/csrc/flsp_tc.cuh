@@ -108,7 +108,8 @@ enum TcEpilogue : int {
 
 struct TcGemmArgs {
   const __nv_bfloat16* A;     // packed M x K
-  const __nv_bfloat16* B;     // packed N x K
+  const __nv_bfloat16* B;     // packed N x K: rows b_row0 .. b_row0 + N - 1 of a packed b_rows x K
+  int b_rows, b_row0;         // matrix (b_rows = 0: B is exactly N x K); both multiples of 8
   int M, N, K;                // M % 128 == 0, N % 16 == 0 (<= 256), K % 64 == 0
   const float* bias;          // [N] (hidden / output)
   __nv_bfloat16* out_bf16;    // packed M x N_pack (hidden / back-act), N_pack = out_k
@@ -164,6 +165,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
     // producer: bulk copies of the A and B chunks of every K stage
     const char* ga = reinterpret_cast<const char*>(a.A);
     const char* gb = reinterpret_cast<const char*>(a.B);
+    const int rb = a.b_rows > 0 ? a.b_rows : N;
     for (int kc = 0; kc < nk && ok; ++kc) {
       const int s = kc % kTcStages;
       if (kc >= kTcStages) ok = mbar_wait(&empty[s], ((kc / kTcStages) - 1) & 1, 1 << 22);
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
       mbar_arrive_expect_tx(&full[s], stage_bytes);
       // A rows m0.. m0+127 of chunk kc, B rows 0..N-1 of chunk kc: contiguous
       bulk_g2s(sa, ga + ((long long)kc * (a.M / 8) + m0 / 8) * 1024, a_bytes, &full[s]);
-      bulk_g2s(sa + a_bytes, gb + (long long)kc * (N / 8) * 1024, b_bytes, &full[s]);
+      bulk_g2s(sa + a_bytes, gb + ((long long)kc * (rb / 8) + a.b_row0 / 8) * 1024, b_bytes, &full[s]);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer

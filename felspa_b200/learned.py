@@ -10,7 +10,9 @@ The network maps the 3 x 3 patch of a 2D degree-2 (Q basis) cell, 9
 Legendre coefficients per cell divided by the cell size h, plus 64 h, to
 the change of the centre cell's coefficients under the HJ sweep, divided
 by h: 82 -> 256 x 4 (GELU) -> 9, BF16 weights on the tensor cores, FP32
-accumulation, FP32 master weights and Adam.
+accumulation, FP32 master weights and Adam.  The 3D variant takes the
+3 x 3 x 3 patch of a 3D degree-2 cell (27 coefficients each) plus 64 h:
+730 -> 256 x 4 -> 27.
 """
 import ctypes as C
 
@@ -23,11 +25,19 @@ IN, HIDDEN, OUT = abi.MLP_IN, abi.MLP_HIDDEN, abi.MLP_OUT
 WIDTHS = (IN, HIDDEN, HIDDEN, HIDDEN, HIDDEN, OUT)
 
 
-def param_layout():
+def widths(dim=2):
+    """layer widths of the 2D or 3D patch network"""
+    if dim == 3:
+        return (abi.MLP3_IN, HIDDEN, HIDDEN, HIDDEN, HIDDEN, abi.MLP3_OUT)
+    return WIDTHS
+
+
+def param_layout(dim=2):
     """[(name, offset, shape)] of the flat parameter vector (W_l row-major [out][in])."""
     out, off = [], 0
+    W = widths(dim)
     for l in range(5):
-        ni, no = WIDTHS[l], WIDTHS[l + 1]
+        ni, no = W[l], W[l + 1]
         out.append((f"W{l + 1}", off, (no, ni)))
         off += ni * no
         out.append((f"b{l + 1}", off, (no,)))
@@ -35,9 +45,9 @@ def param_layout():
     return out
 
 
-def split_params(p):
+def split_params(p, dim=2):
     """W1, b1, ..., W5, b5 views of a flat parameter vector."""
-    return {name: p[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in param_layout()}
+    return {name: p[off:off + int(np.prod(shape))].reshape(shape) for name, off, shape in param_layout(dim)}
 
 
 def default_train_opts(**kw):
@@ -60,14 +70,18 @@ def default_learned_opts(**kw):
 
 
 class MLP:
-    def __init__(self, device=0, seed=0):
+    """dim = 2: the 3 x 3 patch network; dim = 3: the 3 x 3 x 3 patch network"""
+
+    def __init__(self, device=0, seed=0, dim=2):
         L = load()
         h = C.c_void_p()
-        check(L.flsp_mlp_create(int(device), C.c_uint64(seed), C.byref(h)))
+        patch = abi.PATCH_3D_Q2 if dim == 3 else abi.PATCH_2D_Q2
+        check(L.flsp_mlp_create_patch(patch, int(device), C.c_uint64(seed), C.byref(h)))
         self.h = h
-        n = C.c_int64(0)
-        check(L.flsp_mlp_n_params(C.byref(n)))
-        self.n_params = n.value
+        self.dim = dim
+        ni, no, n = C.c_int(0), C.c_int(0), C.c_int64(0)
+        check(L.flsp_mlp_info(h, C.byref(ni), C.byref(no), C.byref(n)))
+        self.n_in, self.n_out, self.n_params = ni.value, no.value, n.value
 
     def close(self):
         if getattr(self, "h", None):
@@ -90,15 +104,15 @@ class MLP:
         check(load().flsp_mlp_set_params(self.h, fp(p), p.size))
 
     def forward(self, x):
-        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, IN)
-        y = np.empty((x.shape[0], OUT), dtype=np.float32)
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.n_in)
+        y = np.empty((x.shape[0], self.n_out), dtype=np.float32)
         check(load().flsp_mlp_forward(self.h, fp(x), x.shape[0], fp(y)))
         return y
 
     def backward(self, x, dy):
         """gradient of sum(dy * net(x)) w.r.t. the parameters, summed over the batch"""
-        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, IN)
-        dy = np.ascontiguousarray(dy, dtype=np.float32).reshape(-1, OUT)
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.n_in)
+        dy = np.ascontiguousarray(dy, dtype=np.float32).reshape(-1, self.n_out)
         g = np.empty(self.n_params, dtype=np.float32)
         check(load().flsp_mlp_backward(self.h, fp(x), fp(dy), x.shape[0], fp(g)))
         return g
@@ -271,6 +285,106 @@ def learned_vs_plain(n=128, instances=24, train_steps=8000, seed=7):
     loss1 = net.eval()
     runs = [zalesak_run("none", n=n), zalesak_run("plain", n=n), zalesak_run("plain", n=n, use_graph=True),
             zalesak_run("learned", net, n=n), zalesak_run("learned", net, n=n, max_residual=1e9)]
+    net.close()
+    return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
+                         "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},
+            "runs": runs}
+
+
+# ----------------------------------------------------------------------
+# the 3D patch network (config 5's learned reinitialisation)
+# ----------------------------------------------------------------------
+def collect_training_pairs_3d(net, n=24, instances=8, periods=6, every=10, target=None, band_cells=6.0):
+    """3D pairs: spheres (random centres and radii, seeds 4000 + i) under
+    the deformation field and perturbed planes (seeds 100 + i) under the
+    plume rolls; before each collection the state is scaled by a random
+    factor in [0.5, 2] (the same interface, a level set that is not a
+    distance function), then the band patches are recorded and the sweep
+    `target` gives the targets."""
+    from . import fields as F
+    from .level_set import Mesh, Problem
+    target = target if target is not None else plain_reinit_opts(viscosity=0.0)
+    for i in range(instances):
+        r = np.random.default_rng(4000 + i)
+        pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+        if i % 2 == 0:
+            pb.set_velocity(F.deformation_3d())
+            c = r.uniform(0.35, 0.65, 3)
+            pb.project(F.sphere(tuple(float(v) for v in c), float(r.uniform(0.12, 0.25))))
+        else:
+            pb.set_velocity(F.plume_3d())
+            pb.project(F.perturbed_plane(seed=100 + i))
+        for _ in range(periods):
+            check(load().flsp_advance_steps(pb.h, int(every), 1e30))
+            pb.set_state(pb.get_state() * float(r.uniform(0.5, 2.0)))
+            net.collect(pb, band_cells, target)
+        pb.close()
+    return net.n_pairs
+
+
+def deformation_run_3d(method, net=None, n=48, every=10, T=3.0, plain=None, max_residual=0.05):
+    """The 3D deformation of the sphere r = 0.15 at (0.35, 0.35, 0.35) over
+    one period (T = 3: the flow reverses and the shape returns), degree-2 Q,
+    FP32, CFL 0.1, reinitialised every `every` steps by `method` ("none",
+    "plain" or "learned").  Wall-clock time of the whole run; L1 interface
+    error and volume change against the initial shape (FP64 reductions)."""
+    import time
+    from . import fields as F
+    from .level_set import Mesh, Problem
+    L = load()
+    plain = plain if plain is not None else plain_reinit_opts(viscosity=0.0)
+    pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+    pb.set_velocity(F.deformation_3d())
+    ic = F.sphere((0.35, 0.35, 0.35), 0.15)
+    pb.project(ic)
+    vol0 = pb.reduce(abi.RED_MASS_SHARP)
+    lo = default_learned_opts(max_residual=max_residual)
+    lo.fallback = abi.ReinitOpts.from_buffer_copy(plain)
+    lo.fallback.narrow_band = 1
+    lo.fallback.band_cells = lo.band_cells
+    nit = C.c_int(0)
+    steps = reinits = n_band = n_fb = 0
+    check(L.flsp_sync(pb.h))
+    t0 = time.perf_counter()
+    while pb.get_time() < T - 1e-12:
+        check(L.flsp_advance_steps(pb.h, int(every), float(T)))
+        steps += every
+        if method == "plain":
+            check(L.flsp_reinit(pb.h, C.byref(plain), C.byref(nit)))
+        elif method == "learned":
+            st = net.reinit(pb, lo)
+            n_band += st["n_band"]
+            n_fb += st["n_fallback"]
+        reinits += 1
+    check(L.flsp_sync(pb.h))
+    wall = time.perf_counter() - t0
+    out = {"method": method, "mesh": f"{n}^3", "steps": steps, "reinits": reinits, "wall_s": wall,
+           "dof_steps_per_s": pb.n_dofs * steps / wall,
+           "l1_interface_error": pb.reduce(abi.RED_L1_INTERFACE_IC, ic),
+           "volume_change": (pb.reduce(abi.RED_MASS_SHARP) - vol0) / vol0,
+           "grad_deviation": pb.reduce(abi.RED_GRAD_DEVIATION)}
+    if method == "learned":
+        out["fallback_fraction"] = n_fb / n_band if n_band else 0.0
+        out["max_residual"] = max_residual
+    pb.close()
+    return out
+
+
+def learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, seed=7):
+    """Train the 3D patch network on the plain sweep's pairs (on the GPU),
+    then run the sphere's deformation period with no reinit, the plain
+    sweep and the learned reinit with and without the residual fallback."""
+    import time
+    net = MLP(device=0, seed=seed, dim=3)
+    t0 = time.perf_counter()
+    n_pairs = collect_training_pairs_3d(net, n=train_n, instances=instances)
+    t1 = time.perf_counter()
+    loss0 = net.eval()
+    last = net.train(steps=train_steps, batch=8192, lr=1e-3, seed=1)
+    t2 = time.perf_counter()
+    loss1 = net.eval()
+    runs = [deformation_run_3d("none", n=n), deformation_run_3d("plain", n=n),
+            deformation_run_3d("learned", net, n=n), deformation_run_3d("learned", net, n=n, max_residual=1e9)]
     net.close()
     return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
                          "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},

@@ -54,6 +54,8 @@ PROTOTYPES = {
     "flsp_default_reinit_opts": (None, [C.POINTER(abi.ReinitOpts)]),
     "flsp_default_ls_opts": (None, [C.POINTER(abi.LSOpts)]),
     "flsp_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    "flsp_mlp_create_patch": (C.c_int, [C.c_int, C.c_int, C.c_uint64, C.POINTER(_vp)]),
+    "flsp_mlp_info": (C.c_int, [_vp, _ip, _ip, _i64p]),
     "flsp_mlp_destroy": (None, [_vp]),
     "flsp_mlp_n_params": (C.c_int, [_i64p]),
     "flsp_mlp_get_params": (C.c_int, [_vp, _fp, C.c_int64]),

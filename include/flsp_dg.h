@@ -326,6 +326,15 @@ int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis,
 #define FLSP_MLP_IN 82
 #define FLSP_MLP_HIDDEN 256
 #define FLSP_MLP_OUT 9
+/* The 3D variant (config 5's patch): 3 x 3 x 3 cells of a 3D degree-2 Q
+   state, 27 coefficients each, divided by h, plus 64 h (730 values, cells
+   z outer, y, x inner), to the change of the centre cell's 27
+   coefficients divided by h: 730 -> 256 x 4 -> 27, same layout rules. */
+#define FLSP_MLP3_IN 730
+#define FLSP_MLP3_OUT 27
+/* patch kinds of flsp_mlp_create_patch */
+#define FLSP_PATCH_2D_Q2 0
+#define FLSP_PATCH_3D_Q2 1
 
 typedef struct flsp_mlp flsp_mlp;
 
@@ -352,18 +361,22 @@ typedef struct flsp_learned_stats {
   int hj_ran;              /* the fallback sweep ran                      */
 } flsp_learned_stats;
 
-int flsp_mlp_create(int device, uint64_t seed, flsp_mlp** out);
+int flsp_mlp_create(int device, uint64_t seed, flsp_mlp** out);   /* 2D patch */
+int flsp_mlp_create_patch(int patch, int device, uint64_t seed, flsp_mlp** out);
 void flsp_mlp_destroy(flsp_mlp* net);
-int flsp_mlp_n_params(int64_t* n);
+int flsp_mlp_n_params(int64_t* n);   /* of the 2D network */
+/* input / output widths and parameter count of a network */
+int flsp_mlp_info(const flsp_mlp* net, int* n_in, int* n_out, int64_t* n_params);
 int flsp_mlp_get_params(flsp_mlp* net, float* params, int64_t n);
 int flsp_mlp_set_params(flsp_mlp* net, const float* params, int64_t n);
-/* y[batch][9] = net(x[batch][82]), host arrays */
+/* y[batch][n_out] = net(x[batch][n_in]), host arrays */
 int flsp_mlp_forward(flsp_mlp* net, const float* x, int64_t batch, float* y);
 /* gradient of sum_b dy[b] . y[b] w.r.t. every parameter (summed over the
    batch, parameter layout above), host arrays */
 int flsp_mlp_backward(flsp_mlp* net, const float* x, const float* dy, int64_t batch,
                       float* grad);
-/* training pairs from a handle (2D, degree 2, Q basis, square cells): the
+/* training pairs from a handle (degree 2, Q basis, square / cubic cells,
+   the network's dimension): the
    band cells' patches of the current state, then the handle is
    reinitialised with `target` and the centre cells' changes are the
    targets.  The handle is left reinitialised. */
