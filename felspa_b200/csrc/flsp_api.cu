@@ -264,7 +264,9 @@ int stage(flsp_handle* h, const void* in, const void* phin, void* out, int st, i
 }
 
 // one SSP-RK substep on the device clock (no host synchronisation)
-int enqueue_adv_step(flsp_handle* h) {
+// step_count: a step-count run (flsp_advance_steps, graph periods) rather
+// than a call for a time step (flsp_advance, the reference's advance_time)
+int enqueue_adv_step(flsp_handle* h, bool step_count = true) {
   AdvClockArgs ca;
   ca.cfl_max = h->cfl_max;
   ca.scale = adv_cfl_scaling(h->p);
@@ -272,6 +274,7 @@ int enqueue_adv_step(flsp_handle* h) {
   ca.ta = h->vel.ta;
   ca.tb = h->vel.tb;
   ca.rk = h->rk;
+  ca.step_count = step_count ? 1 : 0;
   ST(launch_adv_clock_begin(h->stream, h->clk, ca));
   const int x = h->cur, y = (h->cur + 1) % 3, z = (h->cur + 2) % 3;
   void* X = h->buf[x];
@@ -964,7 +967,7 @@ int flsp_advance(flsp_handle* h, double time_step, int single_cycle, double* adv
   double cum = 0.0;
   long long guard = 0;
   do {
-    ST(enqueue_adv_step(h));
+    ST(enqueue_adv_step(h, false));
     ST(sync_clock(h));
     cum = h->clk_host->scratch[1];
     if (!std::isfinite(h->clk_host->dt)) return fail(FLSP_ERR_NONFINITE, "non-finite time step");
@@ -1167,6 +1170,7 @@ int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch)
     ca.ta = h->vel.ta;
     ca.tb = h->vel.tb;
     ca.rk = h->rk;
+    ca.step_count = 1;
     ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
     ST(launch_adv_clock_begin(h->stream, h->clk, ca));
   } else {
@@ -1407,6 +1411,7 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
     q.ca.ta = h->vel.ta;
     q.ca.tb = h->vel.tb;
     q.ca.rk = h->rk;
+    q.ca.step_count = 1;
     q.adv_scale = adv_cfl_scaling(h->p);
     auto add = [&](const MeshArgs& m, std::vector<int2>& it) {
       const long long nt = nblocks(m);

@@ -14,13 +14,15 @@ __device__ __forceinline__ void adv_clock_begin_body(DevClock* c, const AdvClock
   const double ctn = time_factor(a.tkind, a.ta, a.tb, c->t);
   const double vd = fabs(ctn) * c->vd_static;
   c->vd_run = fmax(c->vd_run, vd);
-  const double suggest = a.cfl_max / (c->vd_run * a.scale);
+  double suggest = a.cfl_max / (c->vd_run * a.scale);
   const double remaining = c->scratch[0] - c->scratch[1];   // time_step - cumulative
-  double dt = fmin(suggest, remaining);
   // a velocity whose time factor vanishes (e.g. 1 - exp(-t) at t = 0) gives
-  // an infinite CFL substep; with a finite remaining time the reference rule
-  // takes the remaining time, but a step-count run has none: fall back to
-  // the estimate of the spatial field alone (|time factor| = 1)
+  // an infinite CFL substep.  A call for a time step (the reference rule)
+  // then takes the remaining time; a step-count run, whose horizon only
+  // caps the time, falls back to the estimate of the spatial field alone
+  // (|time factor| = 1)
+  if (a.step_count && !isfinite(suggest) && c->vd_static > 0.0) suggest = a.cfl_max / (c->vd_static * a.scale);
+  double dt = fmin(suggest, remaining);
   if (!isfinite(dt) && c->vd_static > 0.0) dt = a.cfl_max / (c->vd_static * a.scale);
   c->dt = dt;
   c->active = fabs(dt) <= kClockEps ? 0 : 1;   // TempoIntegrator skips zero steps

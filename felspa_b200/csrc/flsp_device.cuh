@@ -98,6 +98,7 @@ struct AdvClockArgs {
   int tkind;
   double ta, tb;
   int rk;
+  int step_count;   // 1: a step-count run (the horizon only caps the time)
 };
 
 // time factor kinds (flsp_time_kind)
