@@ -312,8 +312,11 @@ def collect_training_pairs_3d(net, n=24, instances=8, periods=6, every=10, targe
             c = r.uniform(0.35, 0.65, 3)
             pb.project(F.sphere(tuple(float(v) for v in c), float(r.uniform(0.12, 0.25))))
         else:
+            # the plume's time factor 1 - exp(-t) vanishes at t = 0; start
+            # where the rolls are established
             pb.set_velocity(F.plume_3d())
             pb.project(F.perturbed_plane(seed=100 + i))
+            pb.set_time(1.0)
         for _ in range(periods):
             check(load().flsp_advance_steps(pb.h, int(every), 1e30))
             pb.set_state(pb.get_state() * float(r.uniform(0.5, 2.0)))
