@@ -472,7 +472,7 @@ def learned_comparison_3d():
     return {
         "workload": "3D degree-2 Q sphere r 0.15 at (0.35,0.35,0.35), 48^3, deformation field over one period "
                     "(T = 3, the shape returns), CFL 0.1, FP32, reinit every 10 steps; plain = 5 fixed "
-                    "pseudo-steps (nu 0, CFL 0.1); learned = the 3x3x3-patch network (730 -> 256x4 -> 27) over "
+                    "pseudo-steps (LDG viscosity 1e-3, CFL 0.1: without it the repeated sweep diverges); learned = the 3x3x3-patch network (730 -> 256x4 -> 27) over "
                     "the 6-cell band, fallback to the narrow-band sweep where the cell residual exceeds 0.05; L1 "
                     "interface error and volume change vs the initial sphere; wall-clock DoF-steps/s",
         "training": {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r["training"].items()},

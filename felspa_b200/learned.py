@@ -303,7 +303,7 @@ def collect_training_pairs_3d(net, n=24, instances=8, periods=6, every=10, targe
     `target` gives the targets."""
     from . import fields as F
     from .level_set import Mesh, Problem
-    target = target if target is not None else plain_reinit_opts(viscosity=0.0)
+    target = target if target is not None else plain_reinit_opts()
     for i in range(instances):
         r = np.random.default_rng(4000 + i)
         pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
@@ -335,7 +335,7 @@ def deformation_run_3d(method, net=None, n=48, every=10, T=3.0, plain=None, max_
     from . import fields as F
     from .level_set import Mesh, Problem
     L = load()
-    plain = plain if plain is not None else plain_reinit_opts(viscosity=0.0)
+    plain = plain if plain is not None else plain_reinit_opts()
     pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
     pb.set_velocity(F.deformation_3d())
     ic = F.sphere((0.35, 0.35, 0.35), 0.15)
