@@ -432,7 +432,7 @@ def learned_comparison():
     degree-2 slotted-disk revolution; the network is trained here, on the
     GPU, on pairs produced by the plain sweep."""
     from felspa_b200.learned import learned_vs_plain
-    r = learned_vs_plain(n=256, instances=16, train_steps=12000)
+    r = learned_vs_plain(n=256, instances=24, train_steps=12000)
     runs = {}
     for x in r["runs"]:
         key = x["method"]
@@ -461,7 +461,7 @@ def learned_comparison_3d():
     """The 3D patch network (config 5's learned reinitialisation) against the
     plain HJ sweep on the 3D deformation of a sphere over one period."""
     from felspa_b200.learned import learned_vs_plain_3d
-    r = learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000)
+    r = learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, every=40)
     runs = {}
     for x in r["runs"]:
         key = x["method"]
@@ -471,7 +471,7 @@ def learned_comparison_3d():
                      if k not in ("method", "mesh")}
     return {
         "workload": "3D degree-2 Q sphere r 0.15 at (0.35,0.35,0.35), 48^3, deformation field over one period "
-                    "(T = 3, the shape returns), CFL 0.1, FP32, reinit every 10 steps; plain = 5 fixed "
+                    "(T = 3, the shape returns), CFL 0.1, FP32, reinit every 40 steps; plain = 5 fixed "
                     "pseudo-steps (LDG viscosity 1e-3, CFL 0.1: without it the repeated sweep diverges); learned = the 3x3x3-patch network (730 -> 256x4 -> 27) over "
                     "the 6-cell band, fallback to the narrow-band sweep where the cell residual exceeds 0.05; L1 "
                     "interface error and volume change vs the initial sphere; wall-clock DoF-steps/s",

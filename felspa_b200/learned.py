@@ -373,7 +373,7 @@ def deformation_run_3d(method, net=None, n=48, every=10, T=3.0, plain=None, max_
     return out
 
 
-def learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, seed=7):
+def learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, seed=7, every=40):
     """Train the 3D patch network on the plain sweep's pairs (on the GPU),
     then run the sphere's deformation period with no reinit, the plain
     sweep and the learned reinit with and without the residual fallback."""
@@ -386,8 +386,9 @@ def learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, seed=7)
     last = net.train(steps=train_steps, batch=8192, lr=1e-3, seed=1)
     t2 = time.perf_counter()
     loss1 = net.eval()
-    runs = [deformation_run_3d("none", n=n), deformation_run_3d("plain", n=n),
-            deformation_run_3d("learned", net, n=n), deformation_run_3d("learned", net, n=n, max_residual=1e9)]
+    runs = [deformation_run_3d("none", n=n, every=every), deformation_run_3d("plain", n=n, every=every),
+            deformation_run_3d("learned", net, n=n, every=every),
+            deformation_run_3d("learned", net, n=n, every=every, max_residual=1e9)]
     net.close()
     return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
                          "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},
