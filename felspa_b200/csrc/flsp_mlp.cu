@@ -304,11 +304,24 @@ __global__ void k_merge(const T* __restrict__ src, T* __restrict__ out, int nb, 
   out[c * nb + q] = src[c * nb + q];
 }
 
+// y[r][c] = sum_s part[s][r][c] (fixed order) for r < rows, c < cols
+__global__ void k_split_sum(const float* __restrict__ part, int splits, long long stride, int rows, int cols,
+                            int ldp, float* __restrict__ y, int ldy) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)rows * cols) return;
+  const int r = (int)(t / cols), c = (int)(t % cols);
+  float acc = 0.0f;
+  for (int s = 0; s < splits; ++s) acc += part[s * stride + (long long)r * ldp + c];
+  y[(long long)r * ldy + c] = acc;
+}
+
 // ------------------------------------------------------------------ GEMM launch
 template <int EPI>
-static int gemm(cudaStream_t st, const TcGemmArgs& a) {
+static int gemm(cudaStream_t st, const TcGemmArgs& a, int ksplit = 1) {
   if (a.M % kTcBM || a.N % 16 || a.N > 256 || a.N < 16 || a.K % kTcBK || a.K <= 0)
     return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: unsupported shape");
+  if (ksplit < 1 || ksplit > a.K / kTcBK || (ksplit > 1 && EPI != kEpiStoreF32))
+    return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: bad K split");
   const size_t smem = tc_gemm_smem(a.N);
   static bool attr_done[4][64] = {};
   int dev = 0;
@@ -318,7 +331,7 @@ static int gemm(cudaStream_t st, const TcGemmArgs& a) {
                              (int)tc_gemm_smem(256)));
     attr_done[EPI][dev] = true;
   }
-  tc_gemm_kernel<EPI><<<a.M / kTcBM, 128, smem, st>>>(a);
+  tc_gemm_kernel<EPI><<<dim3(a.M / kTcBM, ksplit), 128, smem, st>>>(a);
   return launch_status("tc_gemm_kernel");
 }
 
@@ -353,6 +366,7 @@ int mlp_ensure_cap(flsp_mlp* net, int64_t rows) {
   MCU(cudaMalloc(&net->tA, c * std::max(256, net->k_in) * 2));
   MCU(cudaMalloc(&net->tG, c * 256 * 2));
   MCU(cudaMalloc(&net->colsum, (c / 32 + 1) * 256 * 4));
+  if (!net->split) MCU(cudaMalloc(&net->split, (size_t)kMlpSplits * 256 * 256 * 4));
   MCU(cudaMalloc(&net->loss_part, (c / 256 + 1) * 8));
   net->cap = need;
   return FLSP_OK;
@@ -473,12 +487,28 @@ static int mlp_backward_dev(flsp_mlp* net, int64_t n) {
       a.M = grows;
       a.N = std::min(256, ain_k - c0);
       a.K = R;
-      a.y = net->g + L.w_off + c0;
-      a.ldy = L.n_in;
       a.n_valid = std::min(a.N, L.n_in - c0);
       a.m_valid = L.n_out;
       a.err = net->err;
-      if (a.n_valid > 0) MST(gemm<kEpiStoreF32>(st, a));
+      if (a.n_valid <= 0) continue;
+      // the batch is the GEMM's K: split it over up to kMlpSplits CTA rows
+      // (partial products, then a fixed-order sum) so that the few output
+      // tiles still fill the GPU
+      const int ks = std::max(1, std::min(kMlpSplits, (R / kTcBK) / 2));
+      if (ks == 1) {
+        a.y = net->g + L.w_off + c0;
+        a.ldy = L.n_in;
+        MST(gemm<kEpiStoreF32>(st, a));
+      } else {
+        a.y = net->split;
+        a.ldy = a.N;
+        a.split_stride = (long long)a.M * a.N;
+        MST(gemm<kEpiStoreF32>(st, a, ks));
+        const long long nt = (long long)a.m_valid * a.n_valid;
+        k_split_sum<<<(int)((nt + 255) / 256), 256, 0, st>>>(net->split, ks, a.split_stride, a.m_valid, a.n_valid,
+                                                           a.N, net->g + L.w_off + c0, L.n_in);
+        MST(launch_status("k_split_sum"));
+      }
     }
     if (l == 0) break;
     // G_{l-1} = (G W_l) * GELU'(z_{l-1}), with its column sums -> db_{l-1}
@@ -560,6 +590,7 @@ void flsp_mlp_destroy(flsp_mlp* net) {
   if (!net) return;
   cudaSetDevice(net->dev);
   if (net->stream) cudaStreamSynchronize(net->stream);
+  if (net->split) cudaFree(net->split);
   void* ps[] = {net->p, net->m, net->v, net->g, net->x, net->y, net->gout, net->gh[0], net->gh[1], net->tA,
                 net->tG, net->colsum, net->loss_part, net->loss_dev, net->err, net->feat, net->targ, net->idx};
   for (void* q : ps)

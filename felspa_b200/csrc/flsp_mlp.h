@@ -23,6 +23,7 @@
 namespace flsp {
 
 constexpr int kMlpLayers = 5;
+constexpr int kMlpSplits = 32;   // most K splits of a weight-gradient GEMM
 constexpr int kMlpIn = FLSP_MLP_IN, kMlpHidden = FLSP_MLP_HIDDEN, kMlpOut = FLSP_MLP_OUT;
 
 struct MlpLayer {
@@ -65,6 +66,7 @@ struct flsp_mlp {
   __nv_bfloat16* tA = nullptr;         // packed max(256, k_in) x cap (transposed activation / input)
   __nv_bfloat16* tG = nullptr;         // packed 256 x cap (transposed gradient; 128 rows for the output layer)
   float* colsum = nullptr;             // cap / 32 x 256 per-warp column sums
+  float* split = nullptr;              // kMlpSplits x 256 x 256 partial weight gradients
   double* loss_part = nullptr;         // per-block loss partials
   double* loss_dev = nullptr;
   int* err = nullptr;                  // device error word

@@ -121,6 +121,9 @@ struct TcGemmArgs {
   int ldy, n_valid, m_valid;
   int* err;                   // device error word
   const int* rows_dev;        // if set: only row tiles below this device-side count do work
+  long long split_stride;     // store epilogue with a K split (gridDim.y > 1): CTA row y of the
+                              // grid sums K chunks [y * nk / gridDim.y, (y + 1) * nk / gridDim.y)
+                              // and writes its partial product to y + blockIdx.y * split_stride
 };
 
 __device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -143,7 +146,10 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * kTcBM;
   if (a.rows_dev && m0 >= *a.rows_dev) return;   // uniform per CTA, before any barrier or TMEM
-  const int nk = a.K / kTcBK;
+  // this CTA's K chunks (all of them without a K split)
+  const int nk_all = a.K / kTcBK;
+  const int kb = (int)(((long long)blockIdx.y * nk_all) / gridDim.y);
+  const int nk = (int)(((long long)(blockIdx.y + 1) * nk_all) / gridDim.y) - kb;
   uint32_t ncols = 32;
   while ((int)ncols < N) ncols <<= 1;
 
@@ -173,8 +179,9 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
       unsigned char* sa = stages + (size_t)s * stage_bytes;
       mbar_arrive_expect_tx(&full[s], stage_bytes);
       // A rows m0.. m0+127 of chunk kc, B rows 0..N-1 of chunk kc: contiguous
-      bulk_g2s(sa, ga + ((long long)kc * (a.M / 8) + m0 / 8) * 1024, a_bytes, &full[s]);
-      bulk_g2s(sa + a_bytes, gb + ((long long)kc * (rb / 8) + a.b_row0 / 8) * 1024, b_bytes, &full[s]);
+      const long long kg = kb + kc;   // global K chunk
+      bulk_g2s(sa, ga + (kg * (a.M / 8) + m0 / 8) * 1024, a_bytes, &full[s]);
+      bulk_g2s(sa + a_bytes, gb + (kg * (rb / 8) + a.b_row0 / 8) * 1024, b_bytes, &full[s]);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer
@@ -252,9 +259,10 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const TcGemmArgs a) {
         }
       }
     } else {
+      float* y = a.y + (long long)blockIdx.y * a.split_stride;
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        if (c0 + i < a.n_valid && r < a.m_valid) a.y[(long long)r * a.ldy + c0 + i] = v[i];
+        if (c0 + i < a.n_valid && r < a.m_valid) y[(long long)r * a.ldy + c0 + i] = v[i];
     }
   }
   tc_fence_before();
