@@ -438,7 +438,9 @@ def learned_comparison():
         key = x["method"]
         if key == "plain" and x.get("graph_replay"):
             key = "plain_graph"
-        if key == "learned" and x.get("max_residual", 0) > 1e6:
+        elif key == "learned" and x.get("graph_replay"):
+            key = "learned_graph_no_fallback"
+        elif key == "learned" and x.get("max_residual", 0) > 1e6:
             key = "learned_no_fallback"
         runs[key] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in x.items()
                      if k not in ("method", "mesh", "graph_replay")}
@@ -454,6 +456,8 @@ def learned_comparison():
         "runs": runs,
         "learned_vs_best_plain_speed": runs["learned"]["dof_steps_per_s"] / best_plain,
         "learned_no_fallback_vs_best_plain_speed": runs["learned_no_fallback"]["dof_steps_per_s"] / best_plain,
+        "learned_graph_no_fallback_vs_best_plain_speed":
+            runs["learned_graph_no_fallback"]["dof_steps_per_s"] / best_plain,
     }
 
 

@@ -151,6 +151,7 @@ struct flsp_handle {
   void* lrn_save = nullptr;   // one state vector
   float* lrn_feat = nullptr;  // band patch features
   int64_t lrn_feat_cap = 0;
+  cudaEvent_t lrn_ev = nullptr;   // orders the network's stream with the handle's
   // compute-restricted narrow band of the reinitialisation
   int* nb_flags = nullptr;    // ncell band flags
   int* nb_lists = nullptr;    // 3 tile lists of ncell entries (HJ, LDG, WENO)
@@ -652,6 +653,7 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
     CU(cudaMalloc(&h->lrn_cells, (size_t)ncell * sizeof(int)));
     CU(cudaMalloc(&h->lrn_count, 2 * sizeof(int)));
     CU(cudaMallocHost(&h->lrn_count_host, 4 * sizeof(int)));
+    CU(cudaEventCreateWithFlags(&h->lrn_ev, cudaEventDisableTiming));
     CU(cudaMalloc(&h->lrn_save, (size_t)h->ndofs * h->tsize + kStatePad));
   }
   if (h->lrn_feat_cap < nfeat) {
@@ -661,6 +663,33 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
     h->lrn_feat_cap = nfeat;
   }
   return FLSP_OK;
+}
+
+// The network's part of a learned reinitialisation, enqueued on the
+// handle's stream without a host wait (graph-capturable once the buffers
+// exist): band cells of buf[pre], their patch features, the network (on its
+// own stream, ordered by an event both ways), and buf[out] = buf[pre] with
+// the band cells corrected.  Every launch is sized for all cells; the band's
+// size stays on the device.
+int enqueue_learned(flsp_handle* h, flsp_mlp* net, double band_cells, int pre, int out) {
+  const int64_t ncell = h->m.ncell;
+  const double hh = h->m.h[0];
+  const int* nband = h->lrn_count;
+  ST(launch_band_select(h->stream, h->prec, h->m.nb, h->buf[pre], ncell, band_cells * hh, h->lrn_flags,
+                        h->lrn_work, h->lrn_cells, h->lrn_count));
+  ST(launch_patch_features(h->stream, h->prec, h->dim, h->buf[pre], h->m.n, hh, h->lrn_cells, ncell, nband,
+                           h->lrn_feat));
+  CU(cudaEventRecord(h->lrn_ev, h->stream));
+  CU(cudaStreamWaitEvent(net->stream, h->lrn_ev, 0));
+  int st = mlp_pack_input(net, h->lrn_feat, nullptr, ncell, nband);
+  if (st == FLSP_OK) st = mlp_forward_dev(net, ncell, false, nband);
+  // join back even after a failed launch, so that a capture stays joined
+  const cudaError_t e1 = cudaEventRecord(h->lrn_ev, net->stream);
+  const cudaError_t e2 = cudaStreamWaitEvent(h->stream, h->lrn_ev, 0);
+  ST(st);
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(FLSP_ERR_CUDA, "learned reinit: stream join failed");
+  return launch_apply_delta(h->stream, h->prec, h->m.nb, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells,
+                            ncell, nband, net->y, net->y_ld);
 }
 
 // band cells of the current state: |mean phi| <= band_cells * h; returns the count
@@ -832,6 +861,7 @@ void flsp_destroy(flsp_handle* h) {
   for (void* q : lrn)
     if (q) cudaFree(q);
   if (h->lrn_count_host) cudaFreeHost(h->lrn_count_host);
+  if (h->lrn_ev) cudaEventDestroy(h->lrn_ev);
   if (h->clk) cudaFree(h->clk);
   if (h->clk_host) cudaFreeHost(h->clk_host);
   if (h->perm) cudaFree(h->perm);
@@ -1285,25 +1315,7 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   const int pre = h->cur;
   const int out = other(pre, -1);
   const int* nband = h->lrn_count;
-  ST(launch_band_select(h->stream, h->prec, h->m.nb, h->buf[pre], ncell, o->band_cells * hh, h->lrn_flags,
-                        h->lrn_work, h->lrn_cells, h->lrn_count));
-  ST(launch_patch_features(h->stream, h->prec, h->dim, h->buf[pre], h->m.n, hh, h->lrn_cells, ncell, nband,
-                           h->lrn_feat));
-  {
-    // the network runs on its own stream: order it after the features and back
-    cudaEvent_t ev;
-    CU(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    cudaEventRecord(ev, h->stream);
-    cudaStreamWaitEvent(net->stream, ev, 0);
-    int st = mlp_pack_input(net, h->lrn_feat, nullptr, ncell, nband);
-    if (st == FLSP_OK) st = mlp_forward_dev(net, ncell, false, nband);
-    cudaEventRecord(ev, net->stream);
-    cudaStreamWaitEvent(h->stream, ev, 0);
-    cudaEventDestroy(ev);
-    ST(st);
-  }
-  ST(launch_apply_delta(h->stream, h->prec, h->m.nb, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells, ncell,
-                        nband, net->y, net->y_ld));
+  ST(enqueue_learned(h, net, o->band_cells, pre, out));
   // band cells whose result is not distance-like enough take the HJ sweep
   ST(launch_residual_flags(h->stream, h->prec, h->dim, h->buf[out], hh, h->lrn_cells, ncell, nband,
                            o->max_residual, h->lrn_flags, h->lrn_count + 1));
@@ -1332,6 +1344,71 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   }
   h->n_since_reinit = 0;
   if (stats) *stats = stl;
+  return FLSP_OK;
+}
+
+int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o, int reinit_frequency,
+                              int n_steps) {
+  if (!h || !net || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  if (n_steps < 0 || reinit_frequency < 1) return fail(FLSP_ERR_BAD_ARG, "bad step counts");
+  if (!(o->band_cells > 0.0)) return fail(FLSP_ERR_BAD_ARG, "bad learned options");
+  CU(cudaSetDevice(h->dev));
+  ST(learned_check(h, net));
+  // buffers and attributes before any capture
+  ST(ensure_learned_buffers(h, h->m.ncell));
+  ST(mlp_ensure_cap(net, h->m.ncell));
+  ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
+  int done = 0;
+  while (done < n_steps) {
+    const int to_reinit = reinit_frequency - h->n_since_reinit;
+    if (to_reinit <= 0) { h->n_since_reinit = 0; continue; }
+    if (done + to_reinit <= n_steps) {
+      // a full period, replayed from its graph (key: buffer role, period,
+      // band width, the network and its buffers)
+      unsigned long long key = 0x6c6561726e656421ull;
+      auto mix = [&key](const void* p, size_t n) {
+        const unsigned char* b = (const unsigned char*)p;
+        for (size_t i = 0; i < n; ++i) { key ^= b[i]; key *= 1099511628211ull; }
+      };
+      mix(&h->cur, sizeof(h->cur));
+      mix(&to_reinit, sizeof(to_reinit));
+      mix(&o->band_cells, sizeof(o->band_cells));
+      mix(&net->uid, sizeof(net->uid));
+      mix(&net->cap, sizeof(net->cap));
+      auto it = h->graphs.find(key);
+      if (it == h->graphs.end()) {
+        const int cur0 = h->cur;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int st = FLSP_OK;
+        for (int s = 0; s < to_reinit && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
+        if (st == FLSP_OK) {
+          const int pre = h->cur, out = other(pre, -1);
+          st = enqueue_learned(h, net, o->band_cells, pre, out);
+          if (st == FLSP_OK) h->cur = out;
+        }
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+        if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); h->cur = cur0; return st; }
+        if (ce != cudaSuccess) { h->cur = cur0; return fail(FLSP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce)); }
+        GraphEntry ge;
+        ge.cur_after = h->cur;
+        h->cur = cur0;
+        CU(cudaGraphInstantiate(&ge.exec, g, 0));
+        cudaGraphDestroy(g);
+        it = h->graphs.emplace(key, ge).first;
+      }
+      CU(cudaGraphLaunch(it->second.exec, h->stream));
+      h->cur = it->second.cur_after;
+      done += to_reinit;
+      h->n_since_reinit = 0;
+    } else {
+      const int k = n_steps - done;
+      for (int s = 0; s < k; ++s) ST(enqueue_adv_step(h));
+      done += k;
+      h->n_since_reinit += k;
+    }
+  }
   return FLSP_OK;
 }
 

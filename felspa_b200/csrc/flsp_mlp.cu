@@ -316,13 +316,9 @@ __global__ void k_split_sum(const float* __restrict__ part, int splits, long lon
 }
 
 // ------------------------------------------------------------------ GEMM launch
+// the kernel's shared-memory attribute, once per epilogue and device
 template <int EPI>
-static int gemm(cudaStream_t st, const TcGemmArgs& a, int ksplit = 1) {
-  if (a.M % kTcBM || a.N % 16 || a.N > 256 || a.N < 16 || a.K % kTcBK || a.K <= 0)
-    return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: unsupported shape");
-  if (ksplit < 1 || ksplit > a.K / kTcBK || (ksplit > 1 && EPI != kEpiStoreF32))
-    return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: bad K split");
-  const size_t smem = tc_gemm_smem(a.N);
+static int gemm_attr() {
   static bool attr_done[4][64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -331,6 +327,17 @@ static int gemm(cudaStream_t st, const TcGemmArgs& a, int ksplit = 1) {
                              (int)tc_gemm_smem(256)));
     attr_done[EPI][dev] = true;
   }
+  return FLSP_OK;
+}
+
+template <int EPI>
+static int gemm(cudaStream_t st, const TcGemmArgs& a, int ksplit = 1) {
+  if (a.M % kTcBM || a.N % 16 || a.N > 256 || a.N < 16 || a.K % kTcBK || a.K <= 0)
+    return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: unsupported shape");
+  if (ksplit < 1 || ksplit > a.K / kTcBK || (ksplit > 1 && EPI != kEpiStoreF32))
+    return set_error(FLSP_ERR_BAD_ARG, "tensor-core GEMM: bad K split");
+  const size_t smem = tc_gemm_smem(a.N);
+  MST(gemm_attr<EPI>());
   tc_gemm_kernel<EPI><<<dim3(a.M / kTcBM, ksplit), 128, smem, st>>>(a);
   return launch_status("tc_gemm_kernel");
 }
@@ -345,6 +352,11 @@ static long long round128(long long n) { return ((n + 127) / 128) * 128; }
 
 // ------------------------------------------------------------------ host side
 int mlp_ensure_cap(flsp_mlp* net, int64_t rows) {
+  // kernel attributes here too: callers size the buffers before a capture
+  MST(gemm_attr<kEpiHidden>());
+  MST(gemm_attr<kEpiOutput>());
+  MST(gemm_attr<kEpiBackAct>());
+  MST(gemm_attr<kEpiStoreF32>());
   const int64_t need = round128(std::max<int64_t>(rows, 128));
   if (net->cap >= need) return FLSP_OK;
   auto fr = [](void* p) { if (p) cudaFree(p); };
@@ -634,6 +646,8 @@ int flsp_mlp_create_patch(int patch, int device, uint64_t seed, flsp_mlp** out) 
   MCU(cudaSetDevice(device));
   flsp_mlp* net = new flsp_mlp();
   net->dev = device;
+  static uint64_t next_uid = 1;   // graph keys of the learned periods tell networks apart by it
+  net->uid = next_uid++;
   net->patch = patch;
   net->n_in = patch == FLSP_PATCH_3D_Q2 ? FLSP_MLP3_IN : kMlpIn;
   net->n_out = patch == FLSP_PATCH_3D_Q2 ? FLSP_MLP3_OUT : kMlpOut;

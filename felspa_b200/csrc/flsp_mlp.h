@@ -36,6 +36,7 @@ struct MlpLayer {
 
 struct flsp_mlp {
   int dev = 0;
+  uint64_t uid = 0;                    // distinct per network created in this process
   int patch = FLSP_PATCH_2D_Q2;
   int n_in = flsp::kMlpIn, n_out = flsp::kMlpOut;   // network widths
   int k_in = 128;                      // GEMM K of the input (n_in rounded up to 64)

@@ -230,7 +230,14 @@ def zalesak_run(method, net=None, n=128, every=40, T=1.0, plain=None, max_residu
     steps = reinits = n_band = n_fb = 0
     check(L.flsp_sync(pb.h))
     t0 = time.perf_counter()
-    if method == "plain" and use_graph:
+    if method == "learned" and use_graph:
+        # learned periods replayed from captured CUDA graphs (the network's
+        # result everywhere in the band: no residual fallback)
+        nsteps = zalesak_run.steps_to_T.get((n, T))
+        check(L.flsp_ls_run_steps_learned(pb.h, net.h, C.byref(lo), int(every), int(nsteps)))
+        check(L.flsp_sync(pb.h))
+        steps, reinits = nsteps, nsteps // every
+    elif method == "plain" and use_graph:
         # fixed-count reinit replayed from captured CUDA graphs; the step
         # count is that of the host-driven run to T (CFL-limited, same for all)
         nsteps = zalesak_run.steps_to_T.get((n, T))
@@ -259,8 +266,8 @@ def zalesak_run(method, net=None, n=128, every=40, T=1.0, plain=None, max_residu
            "grad_deviation": pb.reduce(abi.RED_GRAD_DEVIATION)}
     if method == "learned":
         out["fallback_fraction"] = n_fb / n_band if n_band else 0.0
-        out["max_residual"] = max_residual
-    if method == "plain":
+        out["max_residual"] = None if use_graph else max_residual   # None: no residual test
+    if method in ("plain", "learned"):
         out["graph_replay"] = bool(use_graph)
     pb.close()
     return out
@@ -284,7 +291,8 @@ def learned_vs_plain(n=128, instances=24, train_steps=8000, seed=7):
     t2 = time.perf_counter()
     loss1 = net.eval()
     runs = [zalesak_run("none", n=n), zalesak_run("plain", n=n), zalesak_run("plain", n=n, use_graph=True),
-            zalesak_run("learned", net, n=n), zalesak_run("learned", net, n=n, max_residual=1e9)]
+            zalesak_run("learned", net, n=n), zalesak_run("learned", net, n=n, max_residual=1e9),
+            zalesak_run("learned", net, n=n, use_graph=True)]
     net.close()
     return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
                          "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},

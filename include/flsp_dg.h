@@ -392,6 +392,16 @@ int flsp_mlp_eval(flsp_mlp* net, double* loss);
 /* learned reinitialisation of the handle's state (replaces flsp_reinit) */
 int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o,
                         flsp_learned_stats* stats);
+/* n_steps advection substeps with a learned reinitialisation every
+   reinit_frequency steps, each period replayed from a captured CUDA graph
+   (like flsp_ls_run_steps).  No counterpart in the reference.  The
+   network's result is taken in every band cell: the residual test and the
+   HJ fallback of flsp_reinit_learned need a host decision and are not
+   part of these periods (o->max_residual and o->fallback are not used).
+   Enqueued; flsp_sync waits.  The first period of each buffer role sizes
+   the network's work buffers for every cell of the mesh.               */
+int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o,
+                              int reinit_frequency, int n_steps);
 void flsp_default_train_opts(flsp_train_opts* o);
 void flsp_default_learned_opts(flsp_learned_opts* o);
 

@@ -161,3 +161,25 @@ def test_learned_reinit_after_training():
     assert st["n_band"] > 0 and 0 <= st["n_fallback"] <= st["n_band"]
     pb.close()
     net.close()
+
+
+def test_learned_graph_periods_match_host_loop():
+    """learned periods replayed from CUDA graphs equal the host-driven loop
+    (advance, then the learned reinit with no fallback) bit for bit"""
+    import ctypes as C
+    from felspa_b200.lib import check, load
+    net = MLP(device=0, seed=9)
+    lo = default_learned_opts(max_residual=1e30)
+    a, b = make_problem(48, 11), make_problem(48, 11)
+    for _ in range(3):
+        advance(a, 8)
+        st = net.reinit(a, lo)
+        assert st["n_fallback"] == 0 and st["n_band"] > 0
+    check(load().flsp_ls_run_steps_learned(b.h, net.h, C.byref(lo), 8, 3 * 8))
+    check(load().flsp_sync(b.h))
+    assert a.get_time() == b.get_time()
+    sa, sb = a.get_state(), b.get_state()
+    assert np.all(np.isfinite(sb)) and np.array_equal(sa, sb)
+    a.close()
+    b.close()
+    net.close()
