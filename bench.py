@@ -432,7 +432,7 @@ def learned_comparison():
     degree-2 slotted-disk revolution; the network is trained here, on the
     GPU, on pairs produced by the plain sweep."""
     from felspa_b200.learned import learned_vs_plain
-    r = learned_vs_plain(n=256, instances=24, train_steps=12000)
+    r = learned_vs_plain(n=256, instances=32, train_steps=12000)
     runs = {}
     for x in r["runs"]:
         key = x["method"]
