@@ -156,3 +156,16 @@ def test_group_entry_points_without_gpu(flsp):
     assert L.flsp_group_run_periods(None, C.byref(ctl), 1) == abi.FLSP_ERR_BAD_ARG
     assert L.flsp_group_sync(None) == abi.FLSP_ERR_BAD_ARG
     L.flsp_group_destroy(None)
+
+
+def test_patch_network_entry_points_without_gpu(flsp):
+    """the 3D patch network and the graph-replayed learned periods reject
+    bad arguments and report a missing device"""
+    L = flsp.load()
+    h = C.c_void_p()
+    assert L.flsp_mlp_create_patch(7, 0, 1, C.byref(h)) in (abi.FLSP_ERR_BAD_ARG, abi.FLSP_ERR_NO_DEVICE)
+    assert L.flsp_mlp_create_patch(abi.PATCH_3D_Q2, 0, 1, C.byref(h)) == abi.FLSP_ERR_NO_DEVICE
+    assert L.flsp_mlp_info(None, None, None, None) == abi.FLSP_ERR_BAD_ARG
+    lo = abi.LearnedOpts()
+    L.flsp_default_learned_opts(C.byref(lo))
+    assert L.flsp_ls_run_steps_learned(None, None, C.byref(lo), 10, 10) == abi.FLSP_ERR_BAD_ARG
