@@ -379,6 +379,18 @@ def run_ours(args):
                     "5-pseudo-step plain reinit) of all 9 problems replayed from ONE CUDA graph (one branch per "
                     "problem); compared with the same periods replayed problem by problem",
             **config5_group(periods=4)}
+        if not args.no_learned:
+            # config 5's learned reinit every 5 steps, through the 3D patch network
+            from felspa_b200.learned import MLP, collect_training_pairs_3d
+            net3 = MLP(device=0, seed=7, dim=3)
+            collect_training_pairs_3d(net3, n=24, instances=8)
+            net3.train(steps=3000, batch=8192, lr=1e-3, seed=1)
+            line["variants"]["config5_group_learned"] = {
+                "what": "the config-5 group with the learned reinit every 5 steps (the 3x3x3-patch network, "
+                        "trained here on 24^3 sphere / plume pairs; no fallback), all 9 problems in one graph per "
+                        "period",
+                **config5_group(periods=4, net=net3)}
+            net3.close()
     if world == 1 and not args.no_batched:
         from felspa_b200.batch import config3_benchmark
         r = config3_benchmark()

@@ -1879,20 +1879,21 @@ void flsp_group_destroy(flsp_group* g) {
   delete g;
 }
 
-int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) {
-  if (!g || !o || n_periods < 0) return fail(FLSP_ERR_BAD_ARG, "bad argument");
-  if (o->reinit_frequency < 1 || !o->execute_reinit || o->reinit.mode != FLSP_REINIT_FIXED)
-    return fail(FLSP_ERR_BAD_ARG, "group periods need a fixed-count reinit (FLSP_REINIT_FIXED)");
-  const flsp_reinit_opts ro = o->reinit;
+}  // extern "C"
+
+namespace {
+
+// what a group period runs: the fixed-count plain reinit (ro) or the
+// learned reinit without fallback (net, lo)
+struct GroupMode {
+  int freq = 0;
+  const flsp_reinit_opts* ro = nullptr;
+  flsp_mlp* net = nullptr;
+  const flsp_learned_opts* lo = nullptr;
+};
+
+int group_run(flsp_group* g, const GroupMode& gm, int n_periods) {
   const int n = (int)g->h.size();
-  CU(cudaSetDevice(g->dev));
-  for (flsp_handle* h : g->h) {
-    if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
-    if (h->n_since_reinit != 0) return fail(FLSP_ERR_BAD_ARG, "a group member is inside a reinit period");
-    ST(validate_reinit(h, &ro));
-    if (ro.viscosity > 0.0) ST(ensure_ldg_buffers(h));
-    if (ro.narrow_band) ST(ensure_band_buffers(h));
-  }
   // the group's stream waits for every member's earlier work
   for (int i = 0; i < n; ++i) {
     CU(cudaEventRecord(g->join[i], g->h[i]->stream));
@@ -1905,8 +1906,13 @@ int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) 
       for (size_t i = 0; i < nb; ++i) { key ^= b[i]; key *= 1099511628211ull; }
     };
     for (flsp_handle* h : g->h) mix(&h->cur, sizeof(h->cur));
-    mix(&o->reinit_frequency, sizeof(o->reinit_frequency));
-    mix(&ro, sizeof(ro));
+    mix(&gm.freq, sizeof(gm.freq));
+    if (gm.ro) mix(gm.ro, sizeof(*gm.ro));
+    if (gm.net) {
+      mix(&gm.net->uid, sizeof(gm.net->uid));
+      mix(&gm.net->cap, sizeof(gm.net->cap));
+      mix(&gm.lo->band_cells, sizeof(gm.lo->band_cells));
+    }
     auto gi = g->graphs.find(key);
     if (gi == g->graphs.end()) {
       std::vector<int> cur0(n);
@@ -1919,7 +1925,20 @@ int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) 
         flsp_handle* h = g->h[i];
         ce = cudaStreamWaitEvent(h->stream, g->fork, 0);   // the member's stream joins the capture
         if (ce == cudaSuccess) st = launch_adv_clock_horizon(h->stream, h->clk, INFINITY);
-        if (ce == cudaSuccess && st == FLSP_OK) st = enqueue_period(h, &ro, o->reinit_frequency);
+        if (ce == cudaSuccess && st == FLSP_OK) {
+          if (gm.net) {
+            // the members' network passes share the network's buffers: they
+            // follow one another on its stream (member order)
+            for (int s = 0; s < gm.freq && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
+            if (st == FLSP_OK) {
+              const int pre = h->cur, out = other(pre, -1);
+              st = enqueue_learned(h, gm.net, gm.lo->band_cells, pre, out);
+              if (st == FLSP_OK) h->cur = out;
+            }
+          } else {
+            st = enqueue_period(h, gm.ro, gm.freq);
+          }
+        }
         if (ce == cudaSuccess) ce = cudaEventRecord(g->join[i], h->stream);
         if (ce == cudaSuccess) ce = cudaStreamWaitEvent(g->stream, g->join[i], 0);
       }
@@ -1948,6 +1967,50 @@ int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) 
   CU(cudaEventRecord(g->fork, g->stream));
   for (flsp_handle* h : g->h) CU(cudaStreamWaitEvent(h->stream, g->fork, 0));
   return FLSP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods) {
+  if (!g || !o || n_periods < 0) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  if (o->reinit_frequency < 1 || !o->execute_reinit || o->reinit.mode != FLSP_REINIT_FIXED)
+    return fail(FLSP_ERR_BAD_ARG, "group periods need a fixed-count reinit (FLSP_REINIT_FIXED)");
+  const flsp_reinit_opts ro = o->reinit;
+  CU(cudaSetDevice(g->dev));
+  for (flsp_handle* h : g->h) {
+    if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+    if (h->n_since_reinit != 0) return fail(FLSP_ERR_BAD_ARG, "a group member is inside a reinit period");
+    ST(validate_reinit(h, &ro));
+    if (ro.viscosity > 0.0) ST(ensure_ldg_buffers(h));
+    if (ro.narrow_band) ST(ensure_band_buffers(h));
+  }
+  GroupMode gm;
+  gm.freq = o->reinit_frequency;
+  gm.ro = &ro;
+  return group_run(g, gm, n_periods);
+}
+
+int flsp_group_run_periods_learned(flsp_group* g, flsp_mlp* net, const flsp_learned_opts* o, int reinit_frequency,
+                                   int n_periods) {
+  if (!g || !net || !o || n_periods < 0 || reinit_frequency < 1) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  if (!(o->band_cells > 0.0)) return fail(FLSP_ERR_BAD_ARG, "bad learned options");
+  CU(cudaSetDevice(g->dev));
+  int64_t max_cells = 0;
+  for (flsp_handle* h : g->h) {
+    if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+    if (h->n_since_reinit != 0) return fail(FLSP_ERR_BAD_ARG, "a group member is inside a reinit period");
+    ST(learned_check(h, net));
+    ST(ensure_learned_buffers(h, h->m.ncell));
+    max_cells = std::max<int64_t>(max_cells, h->m.ncell);
+  }
+  ST(mlp_ensure_cap(net, max_cells));
+  GroupMode gm;
+  gm.freq = reinit_frequency;
+  gm.net = net;
+  gm.lo = o;
+  return group_run(g, gm, n_periods);
 }
 
 int flsp_group_sync(flsp_group* g) {

@@ -82,6 +82,7 @@ PROTOTYPES = {
     "flsp_group_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
     "flsp_group_destroy": (None, [_vp]),
     "flsp_group_run_periods": (C.c_int, [_vp, C.POINTER(abi.LSOpts), C.c_int]),
+    "flsp_group_run_periods_learned": (C.c_int, [_vp, _vp, C.POINTER(abi.LearnedOpts), C.c_int, C.c_int]),
     "flsp_group_sync": (C.c_int, [_vp]),
     "flsp_group_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
 }

@@ -457,6 +457,12 @@ typedef struct flsp_group flsp_group;
 int flsp_group_create(flsp_handle* const* handles, int n, flsp_group** out);
 void flsp_group_destroy(flsp_group* g);
 int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods);
+/* the same with the learned reinitialisation (no fallback, as in
+   flsp_ls_run_steps_learned): every member advances reinit_frequency
+   substeps and takes the network's result in its band; the members'
+   network passes follow one another on the network's stream             */
+int flsp_group_run_periods_learned(flsp_group* g, flsp_mlp* net, const flsp_learned_opts* o,
+                                   int reinit_frequency, int n_periods);
 int flsp_group_sync(flsp_group* g);
 int flsp_group_stream(const flsp_group* g, void** stream);
 

@@ -75,3 +75,36 @@ def test_group_orders_member_work():
     g.close()
     for pb in pbs:
         pb.close()
+
+
+def test_group_learned_periods_match_each_problem_alone():
+    """learned periods of a group (the members' network passes one after
+    another on the network's stream) equal each member's own graph-replayed
+    learned periods"""
+    from felspa_b200.learned import MLP, default_learned_opts
+    net = MLP(device=0, seed=4, dim=3)
+    lo = default_learned_opts()
+
+    def members():
+        out = []
+        for n, seed in ((12, 5), (10, 6)):
+            pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+            pb.set_velocity(F.deformation_3d())
+            pb.project(F.sphere((0.4, 0.5, 0.5), 0.2))
+            out.append(pb)
+        return out
+
+    grouped, alone = members(), members()
+    g = Group(grouped)
+    g.run_periods_learned(net, lo, 4, 3)
+    for pb in alone:
+        check(load().flsp_ls_run_steps_learned(pb.h, net.h, C.byref(lo), 4, 12))
+        pb.sync()
+    for a, b in zip(grouped, alone):
+        sa, sb = a.get_state(), b.get_state()
+        assert np.all(np.isfinite(sa))
+        assert np.array_equal(sa, sb)
+    g.close()
+    for pb in grouped + alone:
+        pb.close()
+    net.close()
