@@ -367,33 +367,33 @@ def run_ours(args):
                 **variant_rate(abi.FP32, local, N_CELLS, F.deformation_3d(), F.sphere((0.35, 0.35, 0.35), 0.15), 10,
                                narrow_band=1)},
             "large_128cubed": {
-                "what": "config-5 scale: 128^3 Q2 FP32 (56.6 M DoFs), plume rolls u = curl(0, psi, 0), "
+                "what": "large 3D run: 128^3 Q2 FP32 (56.6 M DoFs), plume rolls u = curl(0, psi, 0), "
                         "psi = 0.5 sin(pi x) sin(pi y) sin(pi z)(1 - exp(-t)), perturbed plane z = 0.5 + 0.02 sum of "
                         "16 cosine modes; plain full-sweep reinit",
                 **variant_rate(abi.FP32, local, 128, F.plume_3d(), F.perturbed_plane(seed=5), 4)},
         }
-        from felspa_b200.batch import config5_group
-        line["variants"]["config5_group"] = {
-            "what": "config-5 structure: the 128^3 Q2 FP32 plume problem and 8 side 64^3 problems (perturbed "
+        from felspa_b200.batch import plume_group
+        line["variants"]["plume_group"] = {
+            "what": "a large 3D run with side problems: the 128^3 Q2 FP32 plume problem and 8 side 64^3 problems (perturbed "
                     "planes, seeds 5..13) advanced together, each reinit period (5 SSP-RK3 substeps + a fixed "
                     "5-pseudo-step plain reinit) of all 9 problems replayed from ONE CUDA graph (one branch per "
                     "problem); compared with the same periods replayed problem by problem",
-            **config5_group(periods=4)}
+            **plume_group(periods=4)}
         if not args.no_learned:
-            # config 5's learned reinit every 5 steps, through the 3D patch network
+            # the same group with the learned reinit every 5 steps (the 3D patch network)
             from felspa_b200.learned import MLP, collect_training_pairs_3d
             net3 = MLP(device=0, seed=7, dim=3)
             collect_training_pairs_3d(net3, n=24, instances=8)
             net3.train(steps=3000, batch=8192, lr=1e-3, seed=1)
-            line["variants"]["config5_group_learned"] = {
-                "what": "the config-5 group with the learned reinit every 5 steps (the 3x3x3-patch network, "
+            line["variants"]["plume_group_learned"] = {
+                "what": "the plume group with the learned reinit every 5 steps (the 3x3x3-patch network, "
                         "trained here on 24^3 sphere / plume pairs; no fallback), all 9 problems in one graph per "
                         "period",
-                **config5_group(periods=4, net=net3)}
+                **plume_group(periods=4, net=net3)}
             net3.close()
     if world == 1 and not args.no_batched:
-        from felspa_b200.batch import config3_benchmark
-        r = config3_benchmark()
+        from felspa_b200.batch import uneven_batch_benchmark
+        r = uneven_batch_benchmark()
         line["batched"] = {
             "workload": "256 independent 2D Q problems, meshes log-uniform 32^2..256^2, degree U{1,2,3}, union of 1-4 "
                         "circles, 8-mode Fourier stream-function velocity (seeds default_rng(1000+i)), 500 SSP-RK3 "
@@ -474,7 +474,7 @@ def learned_comparison():
 
 
 def learned_comparison_3d():
-    """The 3D patch network (config 5's learned reinitialisation) against the
+    """The 3D patch network (learned reinitialisation of large 3D runs) against the
     plain HJ sweep on the 3D deformation of a sphere over one period."""
     from felspa_b200.learned import learned_vs_plain_3d
     r = learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, every=40)

@@ -73,7 +73,7 @@ class Batch:
         return s.value
 
 
-def config3_instances(n_problems=256, seed_base=1000, n_min=32, n_max=256):
+def uneven_batch_instances(n_problems=256, seed_base=1000, n_min=32, n_max=256):
     """The batched configuration: problem i draws from default_rng(seed_base + i)
     a mesh size N = round(32 * 8^U) (log-uniform 32..256), a degree in {1,2,3};
     its IC is a union of 1-4 circles (centres U[0.2,0.8]^2, radii U[0.05,0.2])
@@ -98,7 +98,7 @@ def make_batch(instances, precision=abi.FP32, cfl_max=0.1):
     return b
 
 
-def config3_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, compare_problems=32, compare_steps=50):
+def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, compare_problems=32, compare_steps=50):
     """Batched configuration: DoF-steps/s of the whole batch (device time of
     `steps` steps with a reinit every `reinit_every`, CUDA events on the batch
     stream) and the autotuner's report; on a subset, for comparison, the same
@@ -109,7 +109,7 @@ def config3_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, co
     from .lib import check, load
     ctl = abi.default_ls_opts(reinit_frequency=reinit_every,
                               reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=n_pseudo))
-    inst = config3_instances(n_problems)
+    inst = uneven_batch_instances(n_problems)
     b = make_batch(inst, precision=abi.FP32)
     t0 = time.perf_counter()
     tune = b.autotune()
@@ -210,7 +210,7 @@ class Group:
         return s.value
 
 
-def config5_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_pseudo=5, degree=2, net=None):
+def plume_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_pseudo=5, degree=2, net=None):
     """The large 3D configuration's structure: a main n_main^3 Q2 FP32 problem
     and n_sides n_side^3 side problems (plume rolls u = curl(0, psi, 0),
     perturbed-plane ICs with seeds 5, 6, ...), one graph per reinit period

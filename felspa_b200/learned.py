@@ -300,7 +300,7 @@ def learned_vs_plain(n=128, instances=24, train_steps=8000, seed=7):
 
 
 # ----------------------------------------------------------------------
-# the 3D patch network (config 5's learned reinitialisation)
+# the 3D patch network (learned reinitialisation of large 3D runs)
 # ----------------------------------------------------------------------
 def collect_training_pairs_3d(net, n=24, instances=8, periods=6, every=10, target=None, band_cells=6.0):
     """3D pairs: spheres (random centres and radii, seeds 4000 + i) under

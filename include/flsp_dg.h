@@ -326,7 +326,7 @@ int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis,
 #define FLSP_MLP_IN 82
 #define FLSP_MLP_HIDDEN 256
 #define FLSP_MLP_OUT 9
-/* The 3D variant (config 5's patch): 3 x 3 x 3 cells of a 3D degree-2 Q
+/* The 3D variant: 3 x 3 x 3 cells of a 3D degree-2 Q
    state, 27 coefficients each, divided by h, plus 64 h (730 values, cells
    z outer, y, x inner), to the change of the centre cell's 27
    coefficients divided by h: 730 -> 256 x 4 -> 27, same layout rules. */

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from felspa_b200 import abi
-from felspa_b200.batch import config3_instances, make_batch
+from felspa_b200.batch import uneven_batch_instances, make_batch
 from felspa_b200.level_set import Mesh, Problem
 
 pytestmark = pytest.mark.gpu
@@ -25,7 +25,7 @@ def control(limiter=-1):
 
 @pytest.mark.parametrize("limiter", [-1, 0])
 def test_batch_matches_single_problems(limiter):
-    inst = config3_instances(6, n_min=16, n_max=40)
+    inst = uneven_batch_instances(6, n_min=16, n_max=40)
     b = make_batch(inst, precision=abi.FP64)
     tune = b.autotune()
     b.run_steps(25, control(limiter))
@@ -50,7 +50,7 @@ def test_batch_matches_single_problems(limiter):
 
 
 def test_batch_fp32_close_to_fp64():
-    inst = config3_instances(5, n_min=16, n_max=48)
+    inst = uneven_batch_instances(5, n_min=16, n_max=48)
     outs = []
     for prec in (abi.FP32, abi.FP64):
         b = make_batch(inst, precision=prec)
