@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libflsp_dg.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-UNITS = ["flsp_api.cu", "flsp_k_adv.cu", "flsp_k_sep2.cu", "flsp_k_sep3.cu", "flsp_k_hj.cu", "flsp_k_misc.cu", "flsp_mlp.cu", "flsp_k_batch.cu"]
+UNITS = ["flsp_api.cu", "flsp_k_adv.cu", "flsp_k_sep2.cu", "flsp_k_sep3.cu", "flsp_k_hj.cu", "flsp_k_misc.cu", "flsp_mlp.cu", "flsp_k_batch.cu", "flsp_io.cu"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
          "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 

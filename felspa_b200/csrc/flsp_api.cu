@@ -158,6 +158,8 @@ struct flsp_handle {
   int* nb_counts = nullptr;   // their device counts
   bool nb_use[3] = {false, false, false};   // lists in force for the launches
   std::map<unsigned long long, GraphEntry> graphs;
+  // exported files (PVDCollector: time and VTU name of every export)
+  std::vector<std::pair<double, std::string>> pvd;
 
   Ctx ctx() const {
     Ctx c;
@@ -922,6 +924,63 @@ int flsp_get_state(flsp_handle* h, double* coeffs, int64_t n) {
   CU(cudaMemcpyAsync(coeffs, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
   return FLSP_OK;
+}
+
+int flsp_eval_patches(flsp_handle* h, int n_sub, double* values, int64_t n) {
+  if (!h || !values) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n_sub < 1 || n_sub > 16) return fail(FLSP_ERR_BAD_ARG, "n_sub must be in 1..16");
+  const long long ns1 = n_sub + 1, npt = h->dim == 3 ? ns1 * ns1 * ns1 : ns1 * ns1;
+  if (n != h->m.ncell * npt) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
+  CU(cudaSetDevice(h->dev));
+  // the FP64 staging buffer (2 dim n_dofs doubles) holds the corner values
+  // of every degree; finer patches may need a buffer of their own
+  const bool own = n > (long long)h->ndofs * 2 * h->dim;
+  double* dev = h->stage64;
+  if (own) CU(cudaMalloc(&dev, sizeof(double) * (size_t)n));
+  int st = launch_eval_patches(h->ctx(), h->buf[h->cur], h->perm, n_sub, dev);
+  if (st == FLSP_OK) {
+    cudaError_t e = cudaMemcpyAsync(values, dev, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) st = fail(FLSP_ERR_CUDA, std::string("eval_patches copy: ") + cudaGetErrorString(e));
+  }
+  if (own) cudaFree(dev);
+  return st;
+}
+
+int flsp_export_solutions(flsp_handle* h, const char* path, const char* label) {
+  if (!h || !path || !label || !label[0]) return fail(FLSP_ERR_BAD_ARG, "null or empty argument");
+  CU(cudaSetDevice(h->dev));
+  double t = 0.0;
+  ST(flsp_get_time(h, &t));
+  if (!(t >= 0.0)) return fail(FLSP_ERR_BAD_ARG, "negative time (PVDCollector::append_record)");
+  char num[32];
+  std::snprintf(num, sizeof(num), "%09zu", h->pvd.size() + 1);
+  const std::string master = std::string(label) + "_" + num + ".vtu";
+  std::vector<double> values((size_t)h->m.ncell << h->dim);
+  ST(flsp_eval_patches(h, 1, values.data(), (int64_t)values.size()));
+  flsp_mesh_desc md;
+  std::memset(&md, 0, sizeof(md));
+  md.dim = h->dim;
+  for (int e = 0; e < 3; ++e) {
+    md.n[e] = e < h->dim ? h->m.n[e] : 1;
+    md.lo[e] = e < h->dim ? h->m.lo[e] : 0.0;
+    md.hi[e] = e < h->dim ? h->m.lo[e] + h->m.n[e] * h->m.h[e] : 1.0;
+  }
+  std::vector<int64_t> order;
+  if (h->perm) {
+    order.resize((size_t)h->m.ncell);
+    CU(cudaMemcpy(order.data(), h->perm, sizeof(int64_t) * order.size(), cudaMemcpyDeviceToHost));
+    md.host_cell_order = order.data();
+  }
+  ST(write_vtu_file(&md, 1, values.data(), label, (std::string(path) + master).c_str()));
+  h->pvd.emplace_back(t, master);
+  std::vector<double> times;
+  std::vector<const char*> files;
+  for (const auto& r : h->pvd) {
+    times.push_back(r.first);
+    files.push_back(r.second.c_str());
+  }
+  return write_pvd_file((std::string(path) + label + ".pvd").c_str(), (int)h->pvd.size(), times.data(), files.data());
 }
 
 int flsp_set_time(flsp_handle* h, double t) {

@@ -182,4 +182,11 @@ int launch_hj_clock_begin(cudaStream_t s, DevClock* clk, double cfl_max, int p, 
                           double min_diam, double adv_scale);
 int launch_hj_clock_end(cudaStream_t s, DevClock* clk);
 
+// ---------------- output (flsp_io.cu) ----------------
+// out[k * (n_sub+1)^dim + j] = the state of host cell k at its patch vertex j
+int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int n_sub, double* out);
+int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
+                   const char* filename);
+int write_pvd_file(const char* filename, int n, const double* times, const char* const* files);
+
 }  // namespace flsp

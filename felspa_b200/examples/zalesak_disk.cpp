@@ -7,7 +7,11 @@
 // (-2.499999, 15)-(2.499999, 40), reinit every 40 substeps with CFL 0.3,
 // 628 calls of advance_time(1.0, false) for one revolution.
 //
-//   zalesak_disk [n_outer_steps=628] [viscosity=0]
+//   zalesak_disk [n_outer_steps=628] [viscosity=0] [export_prefix]
+//
+// With an export prefix the solution is written as VTU files (plus a PVD
+// collection) before the loop, after the first and after the last outer
+// step, as the reference test does.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +37,7 @@ static std::vector<int64_t> dealii_order(int nsub, int nref) {
 int main(int argc, char** argv) {
   const int n_outer = argc > 1 ? std::atoi(argv[1]) : 628;
   const double viscosity = argc > 2 ? std::atof(argv[2]) : 0.0;
+  const char* export_prefix = argc > 3 ? argv[3] : nullptr;
   try {
     flsp::Mesh mesh;
     mesh.dim = 2;
@@ -50,7 +55,11 @@ int main(int argc, char** argv) {
     const std::vector<double> initial = ls.get_solution_vector();
     const double mass0 = ls.integrate_mass();
 
-    for (int i = 0; i < n_outer; ++i) ls.advance_time(1.0, false);
+    if (export_prefix) ls.export_solutions(export_prefix);
+    for (int i = 0; i < n_outer; ++i) {
+      ls.advance_time(1.0, false);
+      if (export_prefix && (i == 0 || i == n_outer - 1)) ls.export_solutions(export_prefix);
+    }
 
     std::printf("time %.6f dofs %lld\n", ls.get_time(), (long long)ls.n_dofs());
     std::printf("mean |coeff - initial| %.6e\n", ls.compute_error(initial));

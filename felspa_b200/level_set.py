@@ -193,6 +193,35 @@ class Problem:
         check(load().flsp_reduce(self.h, which, icd, C.byref(out)))
         return out.value
 
+    def eval_patches(self, n_sub=1):
+        """values at the (n_sub+1)^dim equispaced vertices of every cell
+        (DataOut::build_patches(n_sub)); shape (n_cells, (n_sub+1)^dim),
+        cells in host order, vertices x fastest"""
+        npt = (n_sub + 1) ** self.mesh.dim
+        out = np.empty(self.mesh.n_cells * npt)
+        check(load().flsp_eval_patches(self.h, int(n_sub), dp(out), out.size))
+        return out.reshape(self.mesh.n_cells, npt)
+
+    def export_solutions(self, path, label):
+        """<path><label>_<count>.vtu plus <path><label>.pvd (pde_base.cc:93-115)"""
+        check(load().flsp_export_solutions(self.h, str(path).encode(), str(label).encode()))
+
+
+def write_vtu(mesh, values, label, filename, n_sub=1):
+    """host-side VTU writer (no GPU): `values` as Problem.eval_patches returns them"""
+    md = mesh.desc()
+    v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+    if v.size != mesh.n_cells * (n_sub + 1) ** mesh.dim:
+        raise ValueError("values must hold (n_sub+1)^dim values per cell")
+    check(load().flsp_write_vtu(C.byref(md), int(n_sub), dp(v), str(label).encode(), str(filename).encode()))
+
+
+def write_pvd(filename, records):
+    """host-side PVD writer (no GPU): records = [(time, vtu file name), ...]"""
+    times = np.ascontiguousarray([float(t) for t, _ in records], dtype=np.float64)
+    names = (C.c_char_p * max(len(records), 1))(*[str(f).encode() for _, f in records])
+    check(load().flsp_write_pvd(str(filename).encode(), len(records), dp(times), names))
+
 
 def reduce_noalloc(mesh, fe_degree, basis, precision, state_ptr, which, result_ptr, ref_ptr=None,
                    ic=None, stream=None):
@@ -213,6 +242,8 @@ def reduce_noalloc(mesh, fe_degree, basis, precision, state_ptr, which, result_p
 # ----------------------------------------------------------------------
 class AdvectSimulator:
     """dg::AdvectSimulator: DG advection with CFL-limited SSP-RK substeps."""
+
+    label = "Advect"   # default label string (include/felspa/pde/advection.h:132)
 
     def __init__(self, mesh, fe_degree, basis=abi.BASIS_Q, precision=abi.FP64, rk_order=3,
                  cfl_max=0.9, device=0, problem=None):
@@ -249,6 +280,12 @@ class AdvectSimulator:
 
     def get_solution_vector(self):
         return self.problem.get_state()
+
+    def export_solutions(self, path, label=None):
+        """SimulatorBase::export_solutions(path): the solution's cell-corner
+        values as <path><label>_<9-digit count>.vtu, and <path><label>.pvd
+        listing every export of this simulator with its time."""
+        self.problem.export_solutions(path, label or self.label)
 
     def get_time(self):
         return self.problem.get_time()
@@ -291,6 +328,8 @@ class ReinitSimulatorLDG:
 
 class LevelSetSurface(AdvectSimulator):
     """ls::LevelSetSurface<AdvectSimulator, ReinitSimulatorLDG>."""
+
+    label = "LevelSet"   # default label string (include/felspa/level_set/level_set.h:201)
 
     def __init__(self, mesh, fe_degree, basis=abi.BASIS_Q, precision=abi.FP64, rk_order=3,
                  cfl_max=0.9, device=0, control=None):

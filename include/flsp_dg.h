@@ -284,6 +284,32 @@ int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch)
 int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic,
                 double* out);
 
+/* output --------------------------------------------------------------- */
+/* Values of the state at the (n_sub+1)^dim equispaced vertices of every
+   cell: the patch deal.II's DataOut::build_patches(n_sub) builds, which
+   LevelSetSurface::export_solution uses with n_sub = 1
+   (include/felspa/level_set/src/level_set.implement.h:313-342).
+   n = n_cells (n_sub+1)^dim values, cells in host order, vertices x
+   fastest; evaluated on the device in FP64 from the state (FP64 or FP32).
+   1 <= n_sub <= 16.                                                     */
+int flsp_eval_patches(flsp_handle* h, int n_sub, double* values, int64_t n);
+/* SimulatorBase::export_solutions(path) (src/pde/pde_base.cc:93-115):
+   writes <path><label>_<9-digit export count>.vtu (ASCII VTK unstructured
+   grid, one patch of corner values per cell, point data named `label`)
+   and records (time, file name); <path><label>.pvd is rewritten with every
+   record so far on each call (the reference's PVDCollector,
+   src/base/io.cc:142-166, writes it once, at destruction).  `path` is a
+   prefix (a directory ends with '/').                                  */
+int flsp_export_solutions(flsp_handle* h, const char* path, const char* label);
+/* The host-side writers behind flsp_export_solutions; they need no GPU.
+   flsp_write_vtu: `values` as flsp_eval_patches returns them for `mesh`
+   (its host_cell_order gives the cell of each patch).  flsp_write_pvd:
+   n records (time, VTU file name), deal.II's write_pvd_record layout.  */
+int flsp_write_vtu(const flsp_mesh_desc* mesh, int n_sub, const double* values,
+                   const char* label, const char* filename);
+int flsp_write_pvd(const char* filename, int n, const double* times,
+                   const char* const* files);
+
 /* Allocation-free reduction.  No counterpart in the reference: FELSPA
    computes these diagnostics on the host.  Same arithmetic as flsp_reduce,
    but for callers that cannot allocate device memory: host codes that own

@@ -76,8 +76,8 @@ class Problem {
 class AdvectSimulator {
  public:
   AdvectSimulator(const Mesh& mesh, unsigned int fe_degree, int basis = FLSP_BASIS_P,
-                  int precision = FLSP_FP64)
-      : problem_(mesh, make_opts(fe_degree, basis, precision)) {}
+                  int precision = FLSP_FP64, const std::string& label = "Advect")
+      : problem_(mesh, make_opts(fe_degree, basis, precision)), label_(label) {}
   virtual ~AdvectSimulator() = default;
 
   // AdvectSimulator::initialize(ScalarFunction, ptr_velocity_field)
@@ -122,6 +122,13 @@ class AdvectSimulator {
     for (size_t i = 0; i < s.size(); ++i) acc += std::abs(s[i] - reference[i]);
     return acc / (double)s.size();
   }
+  // SimulatorBase::export_solutions(path) (pde_base.cc:93-115): the
+  // solution's cell-corner values as <path><label>_<9-digit count>.vtu and
+  // <path><label>.pvd listing every export with its time
+  void export_solutions(const std::string& path) const {
+    check(flsp_export_solutions(h(), path.c_str(), label_.c_str()), "flsp_export_solutions");
+  }
+  const std::string& get_label_string() const { return label_; }
   int64_t n_dofs() const { return problem_.n_dofs(); }
   flsp_handle* h() const { return problem_.handle(); }
 
@@ -135,6 +142,7 @@ class AdvectSimulator {
     return o;
   }
   Problem problem_;
+  std::string label_;
 };
 
 class ReinitSimulatorLDG {
@@ -156,8 +164,8 @@ class ReinitSimulatorLDG {
 class LevelSetSurface : public AdvectSimulator {
  public:
   LevelSetSurface(const Mesh& mesh, unsigned int fe_degree, int basis = FLSP_BASIS_P,
-                  int precision = FLSP_FP64)
-      : AdvectSimulator(mesh, fe_degree, basis, precision), reinit_(h()) {
+                  int precision = FLSP_FP64, const std::string& label = "LevelSet")
+      : AdvectSimulator(mesh, fe_degree, basis, precision, label), reinit_(h()) {
     flsp_default_ls_opts(&control_);
   }
   flsp_ls_opts& control() { return control_; }
