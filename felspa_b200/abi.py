@@ -31,6 +31,7 @@ F_ONE, F_LIN, F_SIN, F_COS, F_SINSQ, F_SINPI, F_COSPI, F_SINPISQ = range(8)
 T_ONE, T_COS, T_COSPI, T_ONE_MINUS_EXP = range(4)
 IC_SPHERE, IC_RECT, IC_HEIGHT, IC_UNION, IC_DIFF, IC_INTERSECT = range(6)
 REINIT_BAND, REINIT_GLOBAL, REINIT_FIXED = range(3)
+CURV_REFERENCE, CURV_NEIGHBOUR = range(2)
 (RED_MASS, RED_MASS_ERROR, RED_L1_INTERFACE, RED_MEAN_ABS_DIFF, RED_GRAD_DEVIATION,
  RED_MAX_ABS, RED_L2_ERROR_IC, RED_L1_INTERFACE_IC, RED_MASS_SHARP) = range(9)
 NOALLOC_MAX_CELLS = 65536 * 128   # flsp_reduce_noalloc scratch limit (cells)

@@ -93,6 +93,7 @@ int upload_tables(int dev) {
   ST(upload_tables_sep2());
   ST(upload_tables_sep3());
   ST(upload_tables_batch());
+  ST(upload_tables_io());
   if (dev >= 0 && dev < 64) g_tables_ready[dev] = true;
   return FLSP_OK;
 }
@@ -945,6 +946,19 @@ int flsp_eval_patches(flsp_handle* h, int n_sub, double* values, int64_t n) {
   }
   if (own) cudaFree(dev);
   return st;
+}
+
+int flsp_curvature(flsp_handle* h, int mode, double* kappa, int64_t n) {
+  if (!h || !kappa) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (mode != FLSP_CURV_REFERENCE && mode != FLSP_CURV_NEIGHBOUR) return fail(FLSP_ERR_BAD_ARG, "bad curvature mode");
+  if (n != h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
+  CU(cudaSetDevice(h->dev));
+  // FP64 staging (2 dim n_dofs doubles): the result, then the inverse permutation
+  int64_t* pos = reinterpret_cast<int64_t*>(h->stage64 + h->ndofs);
+  ST(launch_curvature(h->ctx(), h->buf[h->cur], h->perm, pos, mode, h->stage64));
+  CU(cudaMemcpyAsync(kappa, h->stage64, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return FLSP_OK;
 }
 
 int flsp_export_solutions(flsp_handle* h, const char* path, const char* label) {

@@ -18,8 +18,15 @@
 #include <vector>
 
 #include "flsp_launch.h"
+#include "flsp_tables.h"
 
 namespace flsp {
+
+int upload_tables_io() {
+  cudaError_t e = upload_tables_here();
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("tables: ") + cudaGetErrorString(e));
+  return FLSP_OK;
+}
 
 // values of the orthonormal Legendre polynomials L_0..L_{n1-1} on [0,1]
 // at s: L_a(s) = sqrt(2a+1) P_a(2s-1), P by Bonnet's recurrence
@@ -77,6 +84,220 @@ int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int 
   else
     eval_patch_kernel<float><<<grid, 256, 0, c.stream>>>(c.m, c.dim, c.p + 1, n_sub, (const float*)phi, perm, out);
   return launch_status("eval_patch_kernel");
+}
+
+// ---------------------------------------------------------------------
+// Curvature estimate, LevelSetSurface::CurvatureEstimator::estimate
+// (include/felspa/level_set/src/level_set.implement.h:600-812): the weak
+// divergence of n = grad phi / |grad phi| on QGauss(p+1) cell and face
+// rules, the mass solve (|K| I), then |coefficient|.  One thread per cell,
+// FP64 arithmetic from the FP64 or FP32 state:
+//   cell:     R_i -= sum_q grad psi_i . n JxW                     (:747-763)
+//   boundary: R_i += n . normal psi_i JxW                          (:796-811)
+//   interior face, per component d (:766-792):
+//     s = (n_in[d] - n_ex[d]) / (phi_in - phi_ex),
+//     F[d] = s > 0 ? (normal[d] > 0 ? n_in[d] : n_ex[d])
+//          : s < 0 ? (normal[d] > 0 ? n_ex[d] : n_in[d]) : 0 (also for NaN);
+//     only F along the face normal survives F . normal (the tangential
+//     entries are finite or zero).
+// mode FLSP_CURV_REFERENCE: the face belongs to the cell with the lower
+// CellId (its position in the host order, :717) and both of its terms go
+// to that cell's DoFs, psi^in F.normal - psi^ex F.normal with psi^ex the
+// same-index basis function of the neighbour at the shared points: the
+// reference binds its exterior copy to the cell (copy_ex.reinit(cell),
+// :731), so the neighbour receives nothing from that face.
+// mode FLSP_CURV_NEIGHBOUR: every cell adds psi_i F.normal_own over each of
+// its interior faces (F is the same from either side), the exterior term
+// of a standard DG flux.
+// ---------------------------------------------------------------------
+__global__ void inv_perm_kernel(const int64_t* __restrict__ perm, long long n, int64_t* __restrict__ pos) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    pos[perm[k]] = k;
+}
+
+// value and gradient (physical) of a Q-layout cell polynomial from the
+// per-axis factors Lx[e][a] (values) and Dx[e][a] (reference derivatives)
+template <int DIM, int N1>
+__device__ __forceinline__ void eval_point(const double* cq, const double (&Lx)[3][kMaxN1],
+                                           const double (&Dx)[3][kMaxN1], const double* ih, double* val,
+                                           double* g) {
+  constexpr int NZ = DIM > 2 ? N1 : 1;
+  double v = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
+#pragma unroll
+  for (int a2 = 0; a2 < NZ; ++a2)
+#pragma unroll
+    for (int a1 = 0; a1 < N1; ++a1)
+#pragma unroll
+      for (int a0 = 0; a0 < N1; ++a0) {
+        const double c = cq[a0 + N1 * (a1 + N1 * a2)];
+        const double z = DIM > 2 ? Lx[2][a2] : 1.0, dz = DIM > 2 ? Dx[2][a2] : 0.0;
+        v += c * Lx[0][a0] * Lx[1][a1] * z;
+        g0 += c * Dx[0][a0] * Lx[1][a1] * z;
+        g1 += c * Lx[0][a0] * Dx[1][a1] * z;
+        g2 += c * Lx[0][a0] * Lx[1][a1] * dz;
+      }
+  *val = v;
+  g[0] = g0 * ih[0];
+  g[1] = g1 * ih[1];
+  g[2] = DIM > 2 ? g2 * ih[2] : 0.0;
+}
+
+template <int DIM, int P, typename T>
+__global__ void __launch_bounds__(128) curvature_kernel(const MeshArgs m, const T* __restrict__ phi,
+                                                        const int64_t* __restrict__ pos, int mode,
+                                                        double* __restrict__ out) {
+  constexpr int N1 = P + 1, NM = DIM > 2 ? N1 * N1 * N1 : N1 * N1, NZ = DIM > 2 ? N1 : 1;
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= m.ncell) return;
+  const Tab1D<double>& tb = tab<double>(P);
+  const int I[3] = {(int)(c % m.n[0]), (int)((c / m.n[0]) % m.n[1]), DIM > 2 ? (int)(c / ((long long)m.n[0] * m.n[1])) : 0};
+  const double ih[3] = {1.0 / m.h[0], 1.0 / m.h[1], DIM > 2 ? 1.0 / m.h[2] : 1.0};
+  const double vol = m.vol;
+  auto load = [&](long long cell, double* cq) {
+#pragma unroll
+    for (int q = 0; q < NM; ++q) {
+      const int gi = m.q2g[q];
+      cq[q] = gi >= 0 ? (double)phi[cell * m.nb + gi] : 0.0;
+    }
+  };
+  double cq[NM], R[NM];
+  load(c, cq);
+#pragma unroll
+  for (int q = 0; q < NM; ++q) R[q] = 0.0;
+  double Lx[3][kMaxN1], Dx[3][kMaxN1];
+
+  // ---- cell term
+  for (int q2 = 0; q2 < NZ; ++q2)
+    for (int q1 = 0; q1 < N1; ++q1)
+      for (int q0 = 0; q0 < N1; ++q0) {
+        const int qq[3] = {q0, q1, q2};
+#pragma unroll
+        for (int e = 0; e < DIM; ++e)
+#pragma unroll
+          for (int a = 0; a < N1; ++a) {
+            Lx[e][a] = tb.Ll[a][qq[e]];
+            Dx[e][a] = tb.Dl[a][qq[e]];
+          }
+        double val, g[3];
+        eval_point<DIM, N1>(cq, Lx, Dx, ih, &val, g);
+        const double nrm = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+        const double n0 = g[0] / nrm, n1 = g[1] / nrm, n2 = g[2] / nrm;
+        const double jxw = tb.wl[q0] * tb.wl[q1] * (DIM > 2 ? tb.wl[q2] : 1.0) * vol;
+#pragma unroll
+        for (int a2 = 0; a2 < NZ; ++a2)
+#pragma unroll
+          for (int a1 = 0; a1 < N1; ++a1)
+#pragma unroll
+            for (int a0 = 0; a0 < N1; ++a0) {
+              const double z = DIM > 2 ? Lx[2][a2] : 1.0;
+              double dot = (Dx[0][a0] * Lx[1][a1] * z * ih[0]) * n0 + (Lx[0][a0] * Dx[1][a1] * z * ih[1]) * n1;
+              if (DIM > 2) dot += (Lx[0][a0] * Lx[1][a1] * Dx[2][a2] * ih[2]) * n2;
+              R[a0 + N1 * (a1 + N1 * a2)] -= dot * jxw;
+            }
+      }
+
+  // ---- faces
+  for (int f = 0; f < 2 * DIM; ++f) {
+    const int E = f / 2, side = f % 2;
+    const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+    int J[3] = {I[0], I[1], I[2]};
+    J[E] += side ? 1 : -1;
+    const bool boundary = J[E] < 0 || J[E] >= m.n[E];
+    const long long nbc = boundary ? -1 : J[0] + (long long)m.n[0] * (J[1] + (long long)m.n[1] * J[2]);
+    if (!boundary && mode == FLSP_CURV_REFERENCE) {
+      const long long pc = pos ? pos[c] : c, pn = pos ? pos[nbc] : nbc;
+      if (pc > pn) continue;   // the neighbour owns this face
+    }
+    const double sgn = side ? 1.0 : -1.0;
+    const double area = vol * (E == 0 ? ih[0] : (E == 1 ? ih[1] : ih[2]));
+    double cn[NM];
+    if (!boundary) load(nbc, cn);
+    for (int qb = 0; qb < (DIM > 2 ? N1 : 1); ++qb)
+      for (int qa = 0; qa < N1; ++qa) {
+        const double jxw = tb.wl[qa] * (DIM > 2 ? tb.wl[qb] : 1.0) * area;
+#pragma unroll
+        for (int a = 0; a < N1; ++a) {
+          Lx[t0][a] = tb.Ll[a][qa];
+          Dx[t0][a] = tb.Dl[a][qa];
+          if (DIM > 2) {
+            Lx[t1][a] = tb.Ll[a][qb];
+            Dx[t1][a] = tb.Dl[a][qb];
+          }
+          Lx[E][a] = side ? tb.L1[a] : tb.L0[a];
+          Dx[E][a] = side ? tb.D1[a] : tb.D0[a];
+        }
+        double pin, gin[3];
+        eval_point<DIM, N1>(cq, Lx, Dx, ih, &pin, gin);
+        const double nin = sqrt(gin[0] * gin[0] + gin[1] * gin[1] + gin[2] * gin[2]);
+        double fn;
+        if (boundary) {
+          fn = gin[E] / nin * sgn;
+        } else {
+          // the neighbour's trace: its own face on the other side
+#pragma unroll
+          for (int a = 0; a < N1; ++a) {
+            Lx[E][a] = side ? tb.L0[a] : tb.L1[a];
+            Dx[E][a] = side ? tb.D0[a] : tb.D1[a];
+          }
+          double pex, gex[3];
+          eval_point<DIM, N1>(cn, Lx, Dx, ih, &pex, gex);
+          const double nex = sqrt(gex[0] * gex[0] + gex[1] * gex[1] + gex[2] * gex[2]);
+          const double ui = gin[E] / nin, ue = gex[E] / nex;
+          const double sh = (ui - ue) / (pin - pex);
+          double F = 0.0;
+          if (sh > 0.0) F = sgn > 0 ? ui : ue;
+          else if (sh < 0.0) F = sgn > 0 ? ue : ui;
+          fn = F * sgn;
+          // restore the own side's normal factors for the test functions
+#pragma unroll
+          for (int a = 0; a < N1; ++a) Lx[E][a] = side ? tb.L1[a] : tb.L0[a];
+        }
+        const double ref_ex = (!boundary && mode == FLSP_CURV_REFERENCE) ? 1.0 : 0.0;
+#pragma unroll
+        for (int a2 = 0; a2 < NZ; ++a2)
+#pragma unroll
+          for (int a1 = 0; a1 < N1; ++a1)
+#pragma unroll
+            for (int a0 = 0; a0 < N1; ++a0) {
+              const int aa[3] = {a0, a1, a2};
+              double tang = 1.0;
+#pragma unroll
+              for (int e = 0; e < DIM; ++e)
+                if (e != E) tang *= Lx[e][aa[e]];
+              const double lin = side ? tb.L1[aa[E]] : tb.L0[aa[E]];
+              const double lex = side ? tb.L0[aa[E]] : tb.L1[aa[E]];
+              double r = R[a0 + N1 * (a1 + N1 * a2)];
+              r += (lin * tang) * fn * jxw;
+              if (ref_ex != 0.0) r -= (lex * tang) * fn * jxw;
+              R[a0 + N1 * (a1 + N1 * a2)] = r;
+            }
+      }
+  }
+  const long long dst = (pos ? pos[c] : c) * m.nb;
+#pragma unroll
+  for (int q = 0; q < NM; ++q) {
+    const int gi = m.q2g[q];
+    if (gi >= 0) out[dst + gi] = fabs(R[q] / vol);
+  }
+}
+
+int launch_curvature(const Ctx& c, const void* phi, const int64_t* perm, int64_t* pos_scratch, int mode,
+                     double* out) {
+  const int64_t* pos = nullptr;
+  if (perm) {
+    const int grid = (int)std::min<long long>((c.m.ncell + 255) / 256, 148LL * 16);
+    inv_perm_kernel<<<grid, 256, 0, c.stream>>>(perm, c.m.ncell, pos_scratch);
+    int st = launch_status("inv_perm_kernel");
+    if (st) return st;
+    pos = pos_scratch;
+  }
+  const int blocks = (int)((c.m.ncell + 127) / 128);
+  return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
+    constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
+    using T = decltype(tz);
+    curvature_kernel<DIM, P, T><<<blocks, 128, 0, c.stream>>>(c.m, reinterpret_cast<const T*>(phi), pos, mode, out);
+    return launch_status("curvature_kernel");
+  });
 }
 
 namespace {

@@ -188,5 +188,10 @@ int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int 
 int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
                    const char* filename);
 int write_pvd_file(const char* filename, int n, const double* times, const char* const* files);
+int upload_tables_io();
+// curvature estimate of the state into out (host DoF order, FP64);
+// pos_scratch: n_cells int64 for the inverse permutation (used when perm)
+int launch_curvature(const Ctx& c, const void* phi, const int64_t* perm, int64_t* pos_scratch, int mode,
+                     double* out);
 
 }  // namespace flsp

@@ -193,6 +193,12 @@ class Problem:
         check(load().flsp_reduce(self.h, which, icd, C.byref(out)))
         return out.value
 
+    def curvature(self, mode=abi.CURV_REFERENCE):
+        """curvature coefficients of the state (host DoF order, FP64)"""
+        out = np.empty(self.n_dofs)
+        check(load().flsp_curvature(self.h, int(mode), dp(out), out.size))
+        return out
+
     def eval_patches(self, n_sub=1):
         """values at the (n_sub+1)^dim equispaced vertices of every cell
         (DataOut::build_patches(n_sub)); shape (n_cells, (n_sub+1)^dim),
@@ -362,6 +368,14 @@ class LevelSetSurface(AdvectSimulator):
             self.problem.sync()
 
     # diagnostics (FP64 device reductions)
+    def estimate_curvature(self, mode=abi.CURV_REFERENCE):
+        """CurvatureEstimator::estimate (level_set.implement.h:600-620):
+        |M^-1 RHS| of the weak divergence of grad phi / |grad phi|, per
+        coefficient.  CURV_REFERENCE keeps the reference's face loop, whose
+        exterior face term lands in the face owner's DoFs; CURV_NEIGHBOUR
+        gives it to the neighbour (cell means approach the mean curvature)."""
+        return self.problem.curvature(mode)
+
     def integrate_mass(self):
         return self.problem.reduce(abi.RED_MASS)
 

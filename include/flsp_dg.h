@@ -34,6 +34,11 @@
  *                                  (level_set.implement.h:215-295), AdvectSimulator::
  *                                  compute_error (advection.cc:452-484),
  *                                  ReinitSimulatorLDG::gradient_deviation (reinit.cc:491-526)
+ *   flsp_curvature                 LevelSetSurface::CurvatureEstimator::estimate
+ *                                  (level_set.implement.h:600-812)
+ *   flsp_eval_patches /            SimulatorBase::export_solutions (src/pde/pde_base.cc:93-115),
+ *   flsp_export_solutions          LevelSetSurface::export_solution (level_set.implement.h:313-342),
+ *                                  PVDCollector (src/base/io.cc:110-166)
  */
 #ifndef FLSP_DG_H
 #define FLSP_DG_H
@@ -283,6 +288,26 @@ int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch)
 /* reductions ---------------------------------------------------------- */
 int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic,
                 double* out);
+
+/* curvature ------------------------------------------------------------ */
+/* LevelSetSurface::CurvatureEstimator::estimate
+   (include/felspa/level_set/src/level_set.implement.h:600-812): the weak
+   divergence of grad phi / |grad phi| of the current state with QGauss(p+1)
+   cell and face rules and the upwind-by-"shock speed" face flux, divided by
+   |K| (the mass solve), then the absolute value of every coefficient.
+   FLSP_CURV_REFERENCE reproduces the reference, whose face loop binds the
+   exterior face term to the face's owner (the cell with the lower CellId,
+   i.e. the earlier one in the host cell order; level_set.implement.h:731):
+   both face terms go to the owner and the neighbour gets none, so the
+   cell-mean coefficient vanishes away from the boundary.
+   FLSP_CURV_NEIGHBOUR gives the exterior term to the neighbour (a standard
+   DG divergence; its cell means approach the mean curvature, e.g. 1/r for
+   a circle in 2D).  kappa: n_dofs values, host DoF order, FP64.          */
+enum flsp_curvature_mode {
+  FLSP_CURV_REFERENCE = 0,
+  FLSP_CURV_NEIGHBOUR = 1
+};
+int flsp_curvature(flsp_handle* h, int mode, double* kappa, int64_t n);
 
 /* output --------------------------------------------------------------- */
 /* Values of the state at the (n_sub+1)^dim equispaced vertices of every

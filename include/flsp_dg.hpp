@@ -193,6 +193,13 @@ class LevelSetSurface : public AdvectSimulator {
     check(flsp_reduce(h(), FLSP_RED_MASS_ERROR, &analytical, &out), "flsp_reduce");
     return out;
   }
+  // CurvatureEstimator::estimate (level_set.implement.h:600-620);
+  // FLSP_CURV_NEIGHBOUR gives the exterior face term to the neighbour
+  std::vector<double> estimate_curvature(int mode = FLSP_CURV_REFERENCE) const {
+    std::vector<double> out((size_t)n_dofs());
+    check(flsp_curvature(h(), mode, out.data(), (int64_t)out.size()), "flsp_curvature");
+    return out;
+  }
   double integrate_mass() const {
     double out = 0.0;
     check(flsp_reduce(h(), FLSP_RED_MASS, nullptr, &out), "flsp_reduce");

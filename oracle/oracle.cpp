@@ -104,6 +104,7 @@ struct orc_problem {
   // shape tables: val[i*np+q], grad[(i*np+q)*3+d] (reference derivatives)
   std::vector<double> vc, gc, vl, gl;
   std::vector<double> vfc[6], vfl[6];
+  std::vector<double> gfl[6];         // reference gradients at the QGauss(p+1) face points
   std::vector<double> vvert, gvert;  // at the 2^dim vertices (QTrapezoid order)
   int nvert;
 
@@ -450,7 +451,7 @@ int orc_create(const flsp_mesh_desc* mesh, int degree, int basis,
     pr->fc[f] = make_face_quad(pr->dim, p + 2, f);
     pr->fl[f] = make_face_quad(pr->dim, p + 1, f);
     table(pr, pr->fc[f].xi, pr->vfc[f], nullptr);
-    table(pr, pr->fl[f].xi, pr->vfl[f], nullptr);
+    table(pr, pr->fl[f].xi, pr->vfl[f], &pr->gfl[f]);
   }
   std::vector<std::array<double, 3>> verts;
   pr->nvert = 1 << pr->dim;
@@ -1308,6 +1309,111 @@ int orc_mlp_backward(int n_layers, const int* widths, const double* const* W,
       }
       g = gi;
     }
+  }
+  return FLSP_OK;
+}
+
+// LevelSetSurface::CurvatureEstimator::estimate
+// (include/felspa/level_set/src/level_set.implement.h:600-620): RHS by
+// local_assembly (:667-742) with QGauss(p+1) cell and face rules, the
+// advection system's mass solve (|K| I for the orthonormal basis), then the
+// absolute value of every coefficient.  Per cell:
+//   cell_assembly (:747-763): R_i -= sum_q grad psi_i . grad phi / |grad phi| JxW;
+//   boundary_assembly (:796-811): R_i += (grad phi / |grad phi|) . n psi_i JxW;
+//   face_assembly (:766-792) on interior faces, computed by the cell with the
+//   lower CellId (:717; `order` gives that order: order[k] = lattice index of
+//   the k-th cell, NULL = lexicographic), per component d:
+//     s = (n_in[d] - n_ex[d]) / (phi_in - phi_ex)     (n = grad phi / |grad phi|)
+//     F[d] = s > 0 ? (normal[d] > 0 ? n_in[d] : n_ex[d])
+//          : s < 0 ? (normal[d] > 0 ? n_ex[d] : n_in[d]) : 0    (NaN -> 0)
+//   and R_in,i += psi_i^in F.n JxW, R_ex,i -= psi_i^ex F.n JxW, where the
+//   exterior copy is bound to the owning cell (copy_ex.reinit(cell), :731),
+//   so both terms land in the owner's DoFs (psi^ex: the neighbour's basis
+//   function of the same index at the shared points) and the neighbour
+//   receives nothing from that face.
+// to_neighbour != 0: the exterior term goes to the neighbour's DoFs instead
+// (each cell adds psi_i F.n_own JxW on every interior face; F is the same
+// from either side), i.e. the weak divergence of grad phi / |grad phi|.
+int orc_curvature(orc_problem* pr, const double* phi, const int64_t* order, int to_neighbour,
+                  double* kappa) {
+  const int nb = pr->nb, dim = pr->dim, np = pr->ql.np;
+  std::vector<long> pos(pr->ncell);
+  for (long k = 0; k < pr->ncell; ++k) {
+    const long c = order ? (long)order[k] : k;
+    if (c < 0 || c >= pr->ncell) return FLSP_ERR_BAD_ARG;
+    pos[c] = k;
+  }
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < pr->ncell; ++c) {
+    const double* pc = phi + c * nb;
+    double R[128] = {0};
+    // cell term
+    for (int q = 0; q < np; ++q) {
+      double g[3] = {0, 0, 0};
+      for (int j = 0; j < nb; ++j)
+        for (int d = 0; d < dim; ++d) g[d] += pc[j] * (pr->gl[((size_t)j * np + q) * 3 + d] / pr->h[d]);
+      double nrm = 0.0;
+      for (int d = 0; d < dim; ++d) nrm += g[d] * g[d];
+      nrm = std::sqrt(nrm);
+      const double jxw = pr->ql.w[q] * pr->vol;
+      for (int i = 0; i < nb; ++i) {
+        double dot = 0.0;
+        for (int d = 0; d < dim; ++d) dot += (pr->gl[((size_t)i * np + q) * 3 + d] / pr->h[d]) * (g[d] / nrm);
+        R[i] -= dot * jxw;
+      }
+    }
+    // faces
+    for (int f = 0; f < 2 * dim; ++f) {
+      const int ax = f / 2, s = f % 2;
+      const long nbc = pr->neighbor(c, f);
+      if (nbc >= 0 && !to_neighbour && pos[c] > pos[nbc]) continue;   // the neighbour owns this face
+      const FaceQuad& fq = pr->fl[f];
+      const int nf = fq.np;
+      const double area = pr->vol / pr->h[ax];
+      double normal[3] = {0, 0, 0};
+      normal[ax] = s ? 1.0 : -1.0;
+      auto trace = [&](const double* pcc, int ff, int q, double* val, double* g) {
+        *val = 0.0;
+        g[0] = g[1] = g[2] = 0.0;
+        for (int j = 0; j < nb; ++j) {
+          *val += pcc[j] * pr->vfl[ff][(size_t)j * nf + q];
+          for (int d = 0; d < dim; ++d) g[d] += pcc[j] * (pr->gfl[ff][((size_t)j * nf + q) * 3 + d] / pr->h[d]);
+        }
+      };
+      for (int q = 0; q < nf; ++q) {
+        const double jxw = fq.w[q] * area;
+        double pin, gin[3];
+        trace(pc, f, q, &pin, gin);
+        double nin = 0.0;
+        for (int d = 0; d < dim; ++d) nin += gin[d] * gin[d];
+        nin = std::sqrt(nin);
+        if (nbc < 0) {
+          double fn = 0.0;
+          for (int d = 0; d < dim; ++d) fn += gin[d] / nin * normal[d];
+          for (int i = 0; i < nb; ++i) R[i] += fn * pr->vfl[f][(size_t)i * nf + q] * jxw;
+          continue;
+        }
+        double pex, gex[3];
+        trace(phi + nbc * nb, f ^ 1, q, &pex, gex);
+        double nex = 0.0;
+        for (int d = 0; d < dim; ++d) nex += gex[d] * gex[d];
+        nex = std::sqrt(nex);
+        double F[3] = {0, 0, 0};
+        for (int d = 0; d < dim; ++d) {
+          const double sh = (gin[d] / nin - gex[d] / nex) / (pin - pex);
+          if (sh > 0.0) F[d] = normal[d] > 0 ? gin[d] / nin : gex[d] / nex;
+          else if (sh < 0.0) F[d] = normal[d] > 0 ? gex[d] / nex : gin[d] / nin;
+          else F[d] = 0.0;
+        }
+        double fn = 0.0;
+        for (int d = 0; d < dim; ++d) fn += F[d] * normal[d];
+        for (int i = 0; i < nb; ++i) {
+          R[i] += pr->vfl[f][(size_t)i * nf + q] * fn * jxw;
+          if (!to_neighbour) R[i] -= pr->vfl[f ^ 1][(size_t)i * nf + q] * fn * jxw;
+        }
+      }
+    }
+    for (int i = 0; i < nb; ++i) kappa[c * nb + i] = std::fabs(R[i] / pr->vol);
   }
   return FLSP_OK;
 }

@@ -81,6 +81,12 @@ double orc_hj_cfl(orc_problem* pr, const double* phi_grad_src,
 int orc_reinit(orc_problem* pr, double* phi, const flsp_reinit_opts* o,
                int* n_iter);
 int orc_weno(orc_problem* pr, double* phi, int* n_troubled);
+/* curvature estimate (level_set.implement.h:600-812), lexicographic cells;
+   order: the CellId order of the cells (NULL = lexicographic);
+   to_neighbour: exterior face terms to the neighbour (0: to the owner, as
+   the reference)                                                         */
+int orc_curvature(orc_problem* pr, const double* phi, const int64_t* order, int to_neighbour,
+                  double* kappa);
 int orc_minmod_flags(orc_problem* pr, const double* phi, int* flags);
 
 /* level-set driver */

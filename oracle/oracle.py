@@ -61,6 +61,7 @@ def lib():
         L.orc_reinit.argtypes = [C.c_void_p, _dp, C.POINTER(abi.ReinitOpts), _ip]
         L.orc_weno.argtypes = [C.c_void_p, _dp, _ip]
         L.orc_minmod_flags.argtypes = [C.c_void_p, _dp, _ip]
+        L.orc_curvature.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_int, _dp]
         L.orc_ls_advance.argtypes = [C.c_void_p, _dp, C.POINTER(Clock), C.c_int, C.c_double,
                                      C.POINTER(abi.LSOpts), C.c_double, C.c_int, _dp]
         L.orc_reduce.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(abi.ICDesc), _dp]
@@ -201,6 +202,18 @@ class Problem:
         f = np.zeros(self.n_dofs // self.nb, dtype=np.int32)
         _check(lib().orc_minmod_flags(self.h, _p(phi), f.ctypes.data_as(_ip)), "minmod")
         return f
+
+    def curvature(self, phi, order=None, to_neighbour=False):
+        """CurvatureEstimator::estimate on lexicographic cells; `order` =
+        the cells' CellId order (host_cell_order), None = lexicographic;
+        to_neighbour: exterior face terms to the neighbour (False: to the
+        face's owner, as the reference)"""
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.zeros(self.n_dofs)
+        o = np.ascontiguousarray(order, dtype=np.int64) if order is not None else None
+        _check(lib().orc_curvature(self.h, _p(phi), o.ctypes.data_as(C.c_void_p) if o is not None else None,
+                                   1 if to_neighbour else 0, _p(out)), "curvature")
+        return out
 
     def ls_advance(self, phi, time_step, opts=None, single_step=False, rk_order=3, cfl_max=0.9):
         o = opts if opts is not None else abi.default_ls_opts()
