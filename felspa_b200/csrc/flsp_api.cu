@@ -1312,6 +1312,55 @@ int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch)
   return FLSP_OK;
 }
 
+int flsp_autotune(flsp_handle* h, int reps, int* tile, int* cand_tiles, double* cand_ms, int* n_cand) {
+  if (!h || reps < 1) return fail(FLSP_ERR_BAD_ARG, "bad argument");
+  if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
+  CU(cudaSetDevice(h->dev));
+  // the timing runs advance the device clock's substep state: keep a copy
+  ST(sync_clock(h));
+  const DevClock saved_clk = *h->clk_host;
+  const int saved[3] = {h->adv_tile[0], h->adv_tile[1], h->adv_tile[2]};
+  int cand[FLSP_MAX_TILE_CANDIDATES][3], nc = 0, best = -1;
+  double best_ms = INFINITY;
+  const Ctx c = h->ctx();
+  ST(adv_tile_candidates(c, h->veldev(), cand, &nc));
+  int st = FLSP_OK;
+  for (int i = 0; i < nc && st == FLSP_OK; ++i) {
+    if (cand_tiles)
+      for (int d = 0; d < 3; ++d) cand_tiles[3 * i + d] = cand[i][d];
+    if (cand_ms) cand_ms[i] = NAN;
+    if (adv_prepare(c, h->veldev(), cand[i]) != FLSP_OK) continue;   // does not fit this GPU
+    for (int d = 0; d < 3; ++d) h->adv_tile[d] = cand[i][d];
+    double ms = 0.0;
+    st = flsp_time_kernel(h, 0, reps, &ms);
+    if (cand_ms && st == FLSP_OK) cand_ms[i] = ms;
+    if (st == FLSP_OK && ms < best_ms) {
+      best_ms = ms;
+      best = i;
+    }
+  }
+  const int* pick = (st == FLSP_OK && best >= 0) ? cand[best] : saved;
+  for (int d = 0; d < 3; ++d) h->adv_tile[d] = pick[d];
+  const int st2 = adv_prepare(c, h->veldev(), h->adv_tile);
+  clear_graphs(h);
+  *h->clk_host = saved_clk;
+  CU(cudaMemcpyAsync(h->clk, h->clk_host, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  if (st) return st;
+  if (best < 0) return fail(FLSP_ERR_UNSUPPORTED, "no stage tile fits");
+  if (st2) return st2;
+  if (tile)
+    for (int d = 0; d < 3; ++d) tile[d] = h->adv_tile[d];
+  if (n_cand) *n_cand = nc;
+  return FLSP_OK;
+}
+
+int flsp_stage_tile(const flsp_handle* h, int* tile) {
+  if (!h || !tile) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  for (int d = 0; d < 3; ++d) tile[d] = h->adv_tile[d];
+  return FLSP_OK;
+}
+
 int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic, double* out) {
   if (!h || !out) return fail(FLSP_ERR_BAD_ARG, "null argument");
   CU(cudaSetDevice(h->dev));

@@ -55,6 +55,17 @@ int adv_default_tile(const Ctx& c, const VelDev& v, int* tile) {
   });
 }
 
+int adv_tile_candidates(const Ctx& c, const VelDev& v, int (*out)[3], int* n) {
+  static const int c2[][3] = {{32, 8, 1}, {16, 16, 1}, {16, 8, 1}, {8, 8, 1}};
+  static const int c3s[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}};
+  static const int c3q[][3] = {{8, 8, 4}, {8, 4, 4}, {4, 4, 4}, {4, 4, 2}};
+  const int(*cand)[3] = c.dim == 2 ? c2 : (use_sep_kernel(v) ? c3s : c3q);
+  *n = c.dim == 2 ? 4 : (use_sep_kernel(v) ? 3 : 4);
+  for (int i = 0; i < *n; ++i)
+    for (int d = 0; d < 3; ++d) out[i][d] = cand[i][d];
+  return FLSP_OK;
+}
+
 int adv_prepare(const Ctx& c, const VelDev& v, const int* tile) {
   if (use_sep_kernel(v)) return sep_unit(1, c, &v, tile, nullptr);
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {

@@ -142,6 +142,8 @@ int sep3_call(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* 
 // tile: cells per CTA (nullptr = default); smem attribute is set on first use
 int adv_default_tile(const Ctx& c, const VelDev& v, int* tile);
 int adv_prepare(const Ctx& c, const VelDev& v, const int* tile);
+// the tile shapes the stage kernel for this velocity is built with (at most 8)
+int adv_tile_candidates(const Ctx& c, const VelDev& v, int (*out)[3], int* n);
 int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* phin, void* out,
                      const DevClock* clk, int stage, int combine, double ct_explicit,
                      const int* tile);

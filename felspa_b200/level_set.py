@@ -193,6 +193,21 @@ class Problem:
         check(load().flsp_reduce(self.h, which, icd, C.byref(out)))
         return out.value
 
+    def autotune(self, reps=10):
+        """time every stage-kernel tile on this problem and keep the
+        fastest; returns (tile, {tile: ms per stage launch})"""
+        t = (C.c_int * 3)()
+        ct = (C.c_int * (3 * 8))()
+        cm = (C.c_double * 8)()
+        n = C.c_int(0)
+        check(load().flsp_autotune(self.h, int(reps), t, ct, cm, C.byref(n)))
+        return tuple(t), {tuple(ct[3 * i:3 * i + 3]): cm[i] for i in range(n.value)}
+
+    def stage_tile(self):
+        t = (C.c_int * 3)()
+        check(load().flsp_stage_tile(self.h, t))
+        return tuple(t)
+
     def curvature(self, mode=abi.CURV_REFERENCE):
         """curvature coefficients of the state (host DoF order, FP64)"""
         out = np.empty(self.n_dofs)

@@ -48,6 +48,8 @@ PROTOTYPES = {
     "flsp_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "flsp_time_kernel": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "flsp_reduce": (C.c_int, [_vp, C.c_int, C.POINTER(abi.ICDesc), _dp]),
+    "flsp_autotune": (C.c_int, [_vp, C.c_int, _ip, _ip, _dp, _ip]),
+    "flsp_stage_tile": (C.c_int, [_vp, _ip]),
     "flsp_curvature": (C.c_int, [_vp, C.c_int, _dp, C.c_int64]),
     "flsp_eval_patches": (C.c_int, [_vp, C.c_int, _dp, C.c_int64]),
     "flsp_export_solutions": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),

@@ -285,6 +285,21 @@ int flsp_stream(const flsp_handle* h, void** stream);
    per repetition), 1 = reinit pseudo-step kernel.                      */
 int flsp_time_kernel(flsp_handle* h, int which, int reps, double* ms_per_launch);
 
+/* Tile autotuner of the advection stage kernel (no counterpart in the
+   reference, whose assembly has no tiles): times every CTA tile shape the
+   stage kernel is built with on this problem (flsp_time_kernel, `reps`
+   RK3 steps each; the state and the device clock are kept) and keeps the
+   fastest; `tile` (3 ints, or NULL) receives it.  Optional reports:
+   cand_tiles (3 x FLSP_MAX_TILE_CANDIDATES ints) the shapes tried,
+   cand_ms (FLSP_MAX_TILE_CANDIDATES) their ms per stage launch (NaN where a
+   shape does not fit), n_cand their count.  Captured graphs are dropped.
+   flsp_stage_tile reports the tile in force (set at flsp_set_velocity to
+   the first shape with two CTAs per SM).                                */
+#define FLSP_MAX_TILE_CANDIDATES 8
+int flsp_autotune(flsp_handle* h, int reps, int* tile, int* cand_tiles, double* cand_ms,
+                  int* n_cand);
+int flsp_stage_tile(const flsp_handle* h, int* tile);
+
 /* reductions ---------------------------------------------------------- */
 int flsp_reduce(flsp_handle* h, int which, const flsp_ic_desc* ic,
                 double* out);

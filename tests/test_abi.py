@@ -108,6 +108,14 @@ def test_bad_arguments_rejected(flsp):
     o.degree = 3
     assert L.flsp_create(C.byref(m), C.byref(o), C.byref(h)) == abi.FLSP_ERR_UNSUPPORTED
     assert L.flsp_create(None, C.byref(o), C.byref(h)) == abi.FLSP_ERR_BAD_ARG
+    # handle-level entry points refuse a missing handle before touching a device
+    d = C.c_double(0.0)
+    t = (C.c_int * 3)()
+    assert L.flsp_autotune(None, 3, t, None, None, None) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_stage_tile(None, t) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_curvature(None, abi.CURV_REFERENCE, C.byref(d), 1) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_eval_patches(None, 1, C.byref(d), 1) == abi.FLSP_ERR_BAD_ARG
+    assert L.flsp_export_solutions(None, b"./", b"LevelSet") == abi.FLSP_ERR_BAD_ARG
 
 
 def test_product_does_not_reference_oracle():
