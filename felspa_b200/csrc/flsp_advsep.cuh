@@ -22,7 +22,8 @@
 // 16-byte phase from HBM so that 27-value cells need no splitting) and its
 // operator rows arrive by TMA bulk copies on one mbarrier; the RK
 // combination is fused into a coalesced store that prefetches phi^n into
-// registers.  Tile shapes are compile-time.
+// registers (float4 rows where FP32 alignment allows).  Tile shapes are
+// compile-time.
 //
 // The per-axis operators are tabulated once per velocity on the host in
 // FP64 (optab, one row per component d, axis e and cell index i:
@@ -516,7 +517,60 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
   constexpr int RPW = (NROW + NW - 1) / NW, KPR = (ROWE + 31) / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nx = min(TX, m.n[0] - ox);
-  if constexpr (!PB) {
+  // FP32 rows of whole tiles start on 16-byte boundaries in HBM, in the box
+  // copy (same 16-byte phase) and in the R buffer when TX * NM and the row
+  // pitch n[0] * NM are multiples of 4: float4 loads and stores
+  constexpr bool VEC = !PB && sizeof(T) == 4 && (TX * NM) % 4 == 0;
+  const bool vec_ok = VEC && nx == TX && ((long long)m.n[0] * NM) % 4 == 0 &&
+                      ((reinterpret_cast<uintptr_t>(a.out) | reinterpret_cast<uintptr_t>(a.phi_n)) & 15) == 0;
+  if (VEC && vec_ok) {
+    constexpr int RV = TX * NM / 4, KV = (RV + 31) / 32;   // float4 per row, per lane
+    constexpr int CV = RPW > 1 ? 2 : 1;                     // rows with loads in flight together
+#pragma unroll
+    for (int j0 = 0; j0 < RPW; j0 += CV) {
+      float4 pn[CV][KV];
+#pragma unroll
+      for (int jj = 0; jj < CV; ++jj) {
+        const int r = warp + NW * (j0 + jj);
+        const int ly = r % TY, lz = r / TY;
+        const bool rok = j0 + jj < RPW && r < NROW && oy + ly < m.n[1] && (DIM < 3 || oz + lz < m.n[2]);
+        const long long gbase =
+            ((long long)m.n[0] * ((oy + ly) + (long long)m.n[1] * (DIM > 2 ? oz + lz : 0)) + ox) * NM;
+        const float4* src = reinterpret_cast<const float4*>(a.phi_n + (rok ? gbase : 0));
+#pragma unroll
+        for (int k = 0; k < KV; ++k) {
+          const int e = lane + 32 * k;
+          pn[jj][k] = (need_n && active && rok && e < RV) ? __ldg(src + e) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int jj = 0; jj < CV; ++jj) {
+        const int r = warp + NW * (j0 + jj);
+        const int ly = r % TY, lz = r / TY;
+        if (!(j0 + jj < RPW && r < NROW && oy + ly < m.n[1] && (DIM < 3 || oz + lz < m.n[2]))) continue;
+        const long long gbase =
+            ((long long)m.n[0] * ((oy + ly) + (long long)m.n[1] * (DIM > 2 ? oz + lz : 0)) + ox) * NM;
+        const float4* cs = reinterpret_cast<const float4*>(cellp(0, ly, lz));
+        const float4* rs = reinterpret_cast<const float4*>(rbuf + (size_t)TX * r * NM);
+        float4* dst = reinterpret_cast<float4*>(a.out + gbase);
+#pragma unroll
+        for (int k = 0; k < KV; ++k) {
+          const int e = lane + 32 * k;
+          if (e >= RV) continue;
+          const float4 cv = cs[e];
+          float4 o = cv;
+          if (active) {
+            const float4 rv = rs[e], nv = pn[jj][k];
+            o.x = combine_value<float>(a.combine, cv.x, nv.x, rv.x, (float)dt);
+            o.y = combine_value<float>(a.combine, cv.y, nv.y, rv.y, (float)dt);
+            o.z = combine_value<float>(a.combine, cv.z, nv.z, rv.z, (float)dt);
+            o.w = combine_value<float>(a.combine, cv.w, nv.w, rv.w, (float)dt);
+          }
+          dst[e] = o;
+        }
+      }
+    }
+  } else if constexpr (!PB) {
     // rows in chunks of CH, a chunk's phi^n loads all in flight together
     constexpr int CH = RPW * KPR > 16 ? (RPW > 2 ? 2 : RPW) : RPW;
 #pragma unroll
