@@ -161,6 +161,10 @@ struct flsp_handle {
   std::map<unsigned long long, GraphEntry> graphs;
   // exported files (PVDCollector: time and VTU name of every export)
   std::vector<std::pair<double, std::string>> pvd;
+  // last curvature estimate (host DoF order, FP64) and the time it belongs to
+  double* curv = nullptr;
+  bool has_curv = false;
+  double curv_time = 0.0;
 
   Ctx ctx() const {
     Ctx c;
@@ -868,6 +872,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->clk) cudaFree(h->clk);
   if (h->clk_host) cudaFreeHost(h->clk_host);
   if (h->perm) cudaFree(h->perm);
+  if (h->curv) cudaFree(h->curv);
   if (h->stage64) cudaFree(h->stage64);
   if (h->partial) cudaFree(h->partial);
   if (h->red_out) cudaFree(h->red_out);
@@ -953,11 +958,18 @@ int flsp_curvature(flsp_handle* h, int mode, double* kappa, int64_t n) {
   if (mode != FLSP_CURV_REFERENCE && mode != FLSP_CURV_NEIGHBOUR) return fail(FLSP_ERR_BAD_ARG, "bad curvature mode");
   if (n != h->ndofs) return fail(FLSP_ERR_BAD_ARG, "size mismatch");
   CU(cudaSetDevice(h->dev));
-  // FP64 staging (2 dim n_dofs doubles): the result, then the inverse permutation
+  double t = 0.0;
+  ST(flsp_get_time(h, &t));
+  // kept on the device for the exports (CurvatureEstimator's vector)
+  if (!h->curv) CU(cudaMalloc(&h->curv, sizeof(double) * (size_t)h->ndofs));
+  h->has_curv = false;
+  // FP64 staging (2 dim n_dofs doubles) holds the inverse permutation
   int64_t* pos = reinterpret_cast<int64_t*>(h->stage64 + h->ndofs);
-  ST(launch_curvature(h->ctx(), h->buf[h->cur], h->perm, pos, mode, h->stage64));
-  CU(cudaMemcpyAsync(kappa, h->stage64, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  ST(launch_curvature(h->ctx(), h->buf[h->cur], h->perm, pos, mode, h->curv));
+  CU(cudaMemcpyAsync(kappa, h->curv, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
+  h->has_curv = true;
+  h->curv_time = t;
   return FLSP_OK;
 }
 
@@ -986,7 +998,24 @@ int flsp_export_solutions(flsp_handle* h, const char* path, const char* label) {
     CU(cudaMemcpy(order.data(), h->perm, sizeof(int64_t) * order.size(), cudaMemcpyDeviceToHost));
     md.host_cell_order = order.data();
   }
-  ST(write_vtu_file(&md, 1, values.data(), label, (std::string(path) + master).c_str()));
+  // the curvature goes along when it belongs to the current time
+  // (level_set.implement.h:325-330; TimedPhysicsObject::is_synced_with,
+  // numerics::is_nearly_equal with tolerance 1e-12)
+  std::vector<double> kvals;
+  const double tc = h->curv_time;
+  const bool synced = (t < 1.0 && tc < 1.0) ? std::fabs(t - tc) < 1e-12
+                                            : std::fabs(t - tc) < 1e-12 * std::max(std::fabs(t), std::fabs(tc));
+  if (h->has_curv && synced) {
+    kvals.resize(values.size());
+    Ctx c64 = h->ctx();
+    c64.prec = FLSP_FP64;   // the curvature vector is FP64, already in host cell order
+    ST(launch_eval_patches(c64, h->curv, nullptr, 1, h->stage64));
+    CU(cudaMemcpyAsync(kvals.data(), h->stage64, sizeof(double) * kvals.size(), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+  }
+  const std::string klabel = std::string(label) + "Curvature";
+  ST(write_vtu_file(&md, 1, values.data(), label, (std::string(path) + master).c_str(),
+                    kvals.empty() ? nullptr : kvals.data(), klabel.c_str()));
   h->pvd.emplace_back(t, master);
   std::vector<double> times;
   std::vector<const char*> files;

@@ -307,7 +307,7 @@ bool write_all(FILE* f, const std::string& s) { return std::fwrite(s.data(), 1, 
 }  // namespace
 
 int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
-                   const char* filename) {
+                   const char* filename, const double* values2, const char* label2) {
   if (!mesh || !values || !label || !filename || !label[0] || !filename[0])
     return set_error(FLSP_ERR_BAD_ARG, "null or empty argument");
   const int dim = mesh->dim;
@@ -403,7 +403,17 @@ int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, 
     s += buf;
     flush(false);
   }
-  s += "</DataArray>\n</PointData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n";
+  s += "</DataArray>\n";
+  if (values2 && label2 && label2[0]) {
+    s += std::string("<DataArray type=\"Float64\" Name=\"") + label2 + "\" format=\"ascii\">\n";
+    for (long long i = 0; i < n_points; ++i) {
+      std::snprintf(buf, sizeof(buf), "%.17g\n", values2[i]);
+      s += buf;
+      flush(false);
+    }
+    s += "</DataArray>\n";
+  }
+  s += "</PointData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n";
   flush(true);
   ok = (std::fclose(f) == 0) && ok;
   if (!ok) return set_error(FLSP_ERR_BAD_ARG, std::string("write failed: ") + filename);
@@ -438,7 +448,7 @@ int write_pvd_file(const char* filename, int n, const double* times, const char*
 
 extern "C" int flsp_write_vtu(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
                               const char* filename) {
-  return flsp::write_vtu_file(mesh, n_sub, values, label, filename);
+  return flsp::write_vtu_file(mesh, n_sub, values, label, filename, nullptr, nullptr);
 }
 
 extern "C" int flsp_write_pvd(const char* filename, int n, const double* times, const char* const* files) {

@@ -187,8 +187,9 @@ int launch_hj_clock_end(cudaStream_t s, DevClock* clk);
 // ---------------- output (flsp_io.cu) ----------------
 // out[k * (n_sub+1)^dim + j] = the state of host cell k at its patch vertex j
 int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int n_sub, double* out);
+// values2 / label2 (or NULL): a second point-data array
 int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
-                   const char* filename);
+                   const char* filename, const double* values2, const char* label2);
 int write_pvd_file(const char* filename, int n, const double* times, const char* const* files);
 int upload_tables_io();
 // curvature estimate of the state into out (host DoF order, FP64);

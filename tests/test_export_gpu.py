@@ -108,3 +108,27 @@ def test_cpp_driver_exports(flsp, tmp_path):
     assert [x.get("file") for x in ds] == names
     t = [float(x.get("timestep")) for x in ds]
     assert t[0] == 0.0 and 0.0 < t[1] < t[2]
+
+
+def test_export_writes_synced_curvature(flsp, oracle, tmp_path):
+    """as LevelSetSurface::export_solution (level_set.implement.h:325-330):
+    the curvature estimate goes into the VTU as <label>Curvature while its
+    time equals the solution's, and is left out once the solution moves on"""
+    n = (16, 16)
+    ls = LevelSetSurface(Mesh(2, n), 2, basis=abi.BASIS_Q, precision=abi.FP64, cfl_max=0.1)
+    ls.initialize(F.sphere((0.5, 0.5), 0.3), F.ccw_rotation())
+    kappa = ls.estimate_curvature(abi.CURV_NEIGHBOUR)
+    prefix = str(tmp_path) + "/"
+    ls.export_solutions(prefix)
+    root = ET.parse(str(tmp_path / "LevelSet_000000001.vtu")).getroot()
+    arrays = root.findall("UnstructuredGrid/Piece/PointData/DataArray")
+    assert [a.get("Name") for a in arrays] == ["LevelSet", "LevelSetCurvature"]
+    got = np.array(arrays[1].text.split(), dtype=np.float64)
+    orc = oracle.Problem(2, n, 2, abi.BASIS_Q)
+    want = oracle_patches(orc, kappa, 2, 1).ravel()
+    assert rel(got, want) <= TOL
+    ls.advance_time(0.01)
+    ls.export_solutions(prefix)
+    root = ET.parse(str(tmp_path / "LevelSet_000000002.vtu")).getroot()
+    assert [a.get("Name") for a in root.findall("UnstructuredGrid/Piece/PointData/DataArray")] == ["LevelSet"]
+    ls.problem.close()
