@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
                       ((reinterpret_cast<uintptr_t>(a.out) | reinterpret_cast<uintptr_t>(a.phi_n)) & 15) == 0;
   if (VEC && vec_ok) {
     constexpr int RV = TX * NM / 4, KV = (RV + 31) / 32;   // float4 per row, per lane
-    constexpr int CV = RPW > 1 ? 2 : 1;                     // rows with loads in flight together
+    constexpr int CV = RPW;                                 // rows with loads in flight together
 #pragma unroll
     for (int j0 = 0; j0 < RPW; j0 += CV) {
       float4 pn[CV][KV];
