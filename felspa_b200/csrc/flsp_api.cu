@@ -1584,8 +1584,11 @@ struct flsp_batch {
   int2* items_hj = nullptr;
   int2* items_weno = nullptr;
   int n_adv = 0, n_hj = 0, n_weno = 0;
-  size_t smem_adv = 0, smem_hj = 0, smem_weno = 0;
-  int grid_adv = 1, grid_hj = 1, grid_weno = 1;
+  // per kernel kind (adv, hj, weno) and degree 1..3: the items' range in the
+  // kind's list (sorted by degree), shared memory, persistent grid
+  int deg_off[3][4] = {}, deg_cnt[3][4] = {};
+  size_t deg_smem[3][4] = {};
+  int deg_grid[3][4] = {};
   bool built = false;
   std::map<unsigned long long, GraphEntry> graphs;
 };
@@ -1611,7 +1614,7 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
   const int n = (int)b->h.size();
   std::vector<BatchProb> pr((size_t)n);
   std::vector<int2> ia, ih, iw;
-  size_t sa = 0, sh = 0, sw = 0;
+  size_t sa[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0}, sw[4] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i) {
     flsp_handle* h = b->h[i];
     BatchProb& q = pr[(size_t)i];
@@ -1648,13 +1651,14 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
     add(q.m_adv, ia);
     add(q.m_hj, ih);
     add(q.m_weno, iw);
+    if (h->p < 1 || h->p > 3) return fail(FLSP_ERR_UNSUPPORTED, "batched problems: degree 1..3");
     size_t x = 0;
     ST(batch_smem(kBatchKindAdv, h->p, b->prec, adv_tile, v.n_terms, &x));
-    sa = std::max(sa, x);
+    sa[h->p] = std::max(sa[h->p], x);
     ST(batch_smem(kBatchKindHJ, h->p, b->prec, hj_tile, 0, &x));
-    sh = std::max(sh, x);
+    sh[h->p] = std::max(sh[h->p], x);
     ST(batch_smem(kBatchKindWeno, h->p, b->prec, kWenoTile, 0, &x));
-    sw = std::max(sw, x);
+    sw[h->p] = std::max(sw[h->p], x);
   }
   // most expensive items first (higher degree, more velocity terms): blocks
   // take items round-robin, so the long ones spread over the whole grid and
@@ -1680,12 +1684,24 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
   b->n_adv = (int)ia.size();
   b->n_hj = (int)ih.size();
   b->n_weno = (int)iw.size();
-  b->smem_adv = sa;
-  b->smem_hj = sh;
-  b->smem_weno = sw;
-  ST(batch_prepare(kBatchKindAdv, b->prec, sa, adv_tile[0] * adv_tile[1], b->n_adv, &b->grid_adv));
-  ST(batch_prepare(kBatchKindHJ, b->prec, sh, hj_tile[0] * hj_tile[1], b->n_hj, &b->grid_hj));
-  ST(batch_prepare(kBatchKindWeno, b->prec, sw, kWenoTile[0] * kWenoTile[1], b->n_weno, &b->grid_weno));
+  // the lists are sorted by degree (descending): one range, one launch per degree
+  const std::vector<int2>* lists[3] = {&ia, &ih, &iw};
+  const size_t* smems[3] = {sa, sh, sw};
+  const int threads[3] = {adv_tile[0] * adv_tile[1], hj_tile[0] * hj_tile[1], kWenoTile[0] * kWenoTile[1]};
+  for (int k = 0; k < 3; ++k) {
+    for (int p = 0; p < 4; ++p) b->deg_off[k][p] = b->deg_cnt[k][p] = b->deg_grid[k][p] = 0;
+    const std::vector<int2>& it = *lists[k];
+    for (size_t j = 0; j < it.size(); ++j) {
+      const int p = pr[(size_t)it[j].x].p;
+      if (b->deg_cnt[k][p] == 0) b->deg_off[k][p] = (int)j;
+      ++b->deg_cnt[k][p];
+    }
+    for (int p = 1; p <= 3; ++p) {
+      b->deg_smem[k][p] = smems[k][p];
+      if (b->deg_cnt[k][p] > 0)
+        ST(batch_prepare(k, b->prec, p, smems[k][p], threads[k], b->deg_cnt[k][p], &b->deg_grid[k][p]));
+    }
+  }
   for (int d = 0; d < 3; ++d) {
     b->adv_tile[d] = adv_tile[d];
     b->hj_tile[d] = hj_tile[d];
@@ -1705,14 +1721,39 @@ int batch_sync_problems(flsp_batch* b) {
   return FLSP_OK;
 }
 
+// the stage / reinit step / limiter of every problem: one launch per degree
+int batch_adv_all(flsp_batch* b, int thr, int in, int pn, int out, int stage, int combine) {
+  for (int p = 3; p >= 1; --p)
+    if (b->deg_cnt[kBatchKindAdv][p] > 0)
+      ST(launch_batch_adv(b->stream, b->prec, p, b->probs, b->items_adv + b->deg_off[kBatchKindAdv][p],
+                          b->deg_cnt[kBatchKindAdv][p], b->deg_grid[kBatchKindAdv][p], thr,
+                          b->deg_smem[kBatchKindAdv][p], in, pn, out, stage, combine));
+  return FLSP_OK;
+}
+
+int batch_hj_all(flsp_batch* b, int thr, int src, int phi0, int dst, int mode, int rk) {
+  for (int p = 3; p >= 1; --p)
+    if (b->deg_cnt[kBatchKindHJ][p] > 0)
+      ST(launch_batch_hj(b->stream, b->prec, p, b->probs, b->items_hj + b->deg_off[kBatchKindHJ][p],
+                         b->deg_cnt[kBatchKindHJ][p], b->deg_grid[kBatchKindHJ][p], thr,
+                         b->deg_smem[kBatchKindHJ][p], src, phi0, dst, mode, rk));
+  return FLSP_OK;
+}
+
+int batch_weno_all(flsp_batch* b, int in, int out) {
+  for (int p = 3; p >= 1; --p)
+    if (b->deg_cnt[kBatchKindWeno][p] > 0)
+      ST(launch_batch_weno(b->stream, b->prec, p, b->probs, b->items_weno + b->deg_off[kBatchKindWeno][p],
+                           b->deg_cnt[kBatchKindWeno][p], b->deg_grid[kBatchKindWeno][p],
+                           kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out));
+  return FLSP_OK;
+}
+
 int batch_enqueue_step(flsp_batch* b) {
   ST(launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvBegin, 0.0));
   const int x = b->cur, y = (x + 1) % 3, z = (x + 2) % 3;
   const int thr = b->adv_tile[0] * b->adv_tile[1];
-  auto st = [&](int in, int pn, int out, int k, int comb) {
-    return launch_batch_adv(b->stream, b->prec, b->probs, b->items_adv, b->n_adv, b->grid_adv, thr, b->smem_adv, in,
-                            pn, out, k, comb);
-  };
+  auto st = [&](int in, int pn, int out, int k, int comb) { return batch_adv_all(b, thr, in, pn, out, k, comb); };
   if (b->rk == 1) {
     ST(st(x, x, y, 0, kRK1));
     b->cur = y;
@@ -1734,19 +1775,16 @@ int batch_enqueue_reinit(flsp_batch* b, const flsp_reinit_opts* o, bool limiter)
   const int phi0 = b->cur;
   const int thr = b->hj_tile[0] * b->hj_tile[1];
   ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjReset, 0.0));
-  ST(launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, thr, b->smem_hj, phi0, phi0, -1,
-                     kHJCflOnly, o->rk_order));
+  ST(batch_hj_all(b, thr, phi0, phi0, -1, kHJCflOnly, o->rk_order));
   for (int k = 0; k < o->n_pseudo_steps; ++k) {
     ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjBegin, o->cfl_max));
     const int src = b->cur;
     const int dst = (src == phi0) ? (phi0 + 1) % 3 : other(src, phi0);
-    ST(launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, thr, b->smem_hj, src, phi0,
-                       dst, kHJStep, o->rk_order));
+    ST(batch_hj_all(b, thr, src, phi0, dst, kHJStep, o->rk_order));
     int res = dst;
     if (limiter) {
       const int lim = other(dst, phi0);
-      ST(launch_batch_weno(b->stream, b->prec, b->probs, b->items_weno, b->n_weno, b->grid_weno,
-                           kWenoTile[0] * kWenoTile[1], b->smem_weno, dst, lim));
+      ST(batch_weno_all(b, dst, lim));
       res = lim;
     }
     b->cur = res;
@@ -1850,8 +1888,7 @@ int flsp_batch_autotune(flsp_batch* b, flsp_batch_tuning* out) {
     const int x = b->cur, y = (x + 1) % 3;
     double ms = 0.0;
     ST(time_it([&]() {
-      return launch_batch_adv(b->stream, b->prec, b->probs, b->items_adv, b->n_adv, b->grid_adv, ca[c][0] * ca[c][1],
-                              b->smem_adv, x, x, y, 0, kRK3a);
+      return batch_adv_all(b, ca[c][0] * ca[c][1], x, x, y, 0, kRK3a);
     }, &ms));
     t.adv_cand[c][0] = ca[c][0];
     t.adv_cand[c][1] = ca[c][1];
@@ -1868,8 +1905,7 @@ int flsp_batch_autotune(flsp_batch* b, flsp_batch_tuning* out) {
     const int x = b->cur;
     double ms = 0.0;
     ST(time_it([&]() {
-      return launch_batch_hj(b->stream, b->prec, b->probs, b->items_hj, b->n_hj, b->grid_hj, ch[c][0] * ch[c][1],
-                             b->smem_hj, x, x, -1, kHJCflOnly, 1);
+      return batch_hj_all(b, ch[c][0] * ch[c][1], x, x, -1, kHJCflOnly, 1);
     }, &ms));
     t.hj_cand[c][0] = ch[c][0];
     t.hj_cand[c][1] = ch[c][1];

@@ -1,13 +1,16 @@
 // flsp_k_batch.cu — batched problems: many independent 2D level-set
 // problems (their own meshes, degrees 1..3, velocities and clocks) advance
 // in ONE persistent launch per RK stage (and one per reinit pseudo-step and
-// limiter pass).  A block walks a list of work items (problem, tile) and
-// runs the same per-tile bodies as the single-problem kernels
-// (adv_stage_tile, hjq_tile, weno_tile), switching on the item's degree.
-// The tile shapes are launch parameters picked by the batch autotuner.
+// limiter pass) per degree.  A block walks a list of work items (problem,
+// tile) of one degree and runs the same per-tile bodies as the
+// single-problem kernels (adv_stage_tile, hjq_tile, weno_tile); each degree
+// has its own instantiation, so its registers, shared memory and occupancy
+// are its own, not those of the most demanding degree in the batch.  The
+// tile shapes are launch parameters picked by the batch autotuner.
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "flsp_advect.cuh"
 #include "flsp_clock.cuh"
@@ -49,36 +52,27 @@ __device__ __forceinline__ void make_adv_args(const BatchProb& pr, int ix, int i
   a.dt_explicit = 0.0;
 }
 
-template <typename T>
+template <typename T, int P>
 __global__ void __launch_bounds__(256, 2)
     batch_adv_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int ix,
                      int in_n, int iout, int stage, int combine) {
   // the item's arguments are assembled once per block in shared memory
   // (every thread reads them, like a plain launch's kernel parameters)
   __shared__ AdvArgs<T> a;
-  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
-    if (threadIdx.x == 0) {
-      make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
-      pdeg = probs[w.x].p;
-    }
+    if (threadIdx.x == 0) make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
     __syncthreads();
-    switch (pdeg) {
-      case 1: adv_stage_tile<2, 1, T>(a, w.y); break;
-      case 2: adv_stage_tile<2, 2, T>(a, w.y); break;
-      default: adv_stage_tile<2, 3, T>(a, w.y); break;
-    }
+    adv_stage_tile<2, P, T>(a, w.y);
     __syncthreads();   // shared memory is reused by the next item
   }
 }
 
-template <typename T>
+template <typename T, int P>
 __global__ void __launch_bounds__(128)
     batch_hj_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int isrc,
                     int iphi0, int idst, int mode, int rk) {
   __shared__ HJArgs<T> a;
-  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
     if (threadIdx.x == 0) {
@@ -93,24 +87,18 @@ __global__ void __launch_bounds__(128)
       a.dt_explicit = 0.0;
       a.block = pr.m_hj.ncell * pr.m_hj.nb;
       a.rdiff = nullptr;
-      pdeg = pr.p;
     }
     __syncthreads();
-    switch (pdeg) {
-      case 1: hjq_tile<2, 1, T>(a, w.y); break;
-      case 2: hjq_tile<2, 2, T>(a, w.y); break;
-      default: hjq_tile<2, 3, T>(a, w.y); break;
-    }
+    hjq_tile<2, P, T>(a, w.y);
     __syncthreads();
   }
 }
 
-template <typename T>
+template <typename T, int P>
 __global__ void __launch_bounds__(256)
     batch_weno_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int iin,
                       int iout) {
   __shared__ WenoArgs<T> a;
-  __shared__ int pdeg;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
     if (threadIdx.x == 0) {
@@ -119,14 +107,9 @@ __global__ void __launch_bounds__(256)
       a.in = reinterpret_cast<const T*>(pr.buf[iin]);
       a.out = reinterpret_cast<T*>(pr.buf[iout]);
       a.count = nullptr;
-      pdeg = pr.p;
     }
     __syncthreads();
-    switch (pdeg) {
-      case 1: weno_tile<1, T>(a, w.y); break;
-      case 2: weno_tile<2, T>(a, w.y); break;
-      default: weno_tile<3, T>(a, w.y); break;
-    }
+    weno_tile<P, T>(a, w.y);
     __syncthreads();
   }
 }
@@ -189,56 +172,79 @@ int launch_batch_clock(cudaStream_t s, const BatchProb* probs, int n, int what, 
   return launch_status("batch_clock_kernel");
 }
 
-template <typename T>
+// f(integral_constant<int, p>) for the degree p in 1..3
+template <typename F>
+int with_degree(int p, F&& f) {
+  switch (p) {
+    case 1: return f(std::integral_constant<int, 1>());
+    case 2: return f(std::integral_constant<int, 2>());
+    case 3: return f(std::integral_constant<int, 3>());
+  }
+  return set_error(FLSP_ERR_UNSUPPORTED, "batched problems: degree 1..3");
+}
+
+template <typename T, int P>
 static int batch_attr(int kind, size_t smem) {
   cudaError_t e = cudaSuccess;
   const int s = (int)smem;
-  if (kind == kBatchKindAdv) e = cudaFuncSetAttribute(batch_adv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  else if (kind == kBatchKindHJ) e = cudaFuncSetAttribute(batch_hj_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
-  else e = cudaFuncSetAttribute(batch_weno_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  if (kind == kBatchKindAdv) e = cudaFuncSetAttribute(batch_adv_kernel<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  else if (kind == kBatchKindHJ) e = cudaFuncSetAttribute(batch_hj_kernel<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+  else e = cudaFuncSetAttribute(batch_weno_kernel<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
   if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("batch attr: ") + cudaGetErrorString(e));
   return FLSP_OK;
 }
 
-int batch_prepare(int kind, int prec, size_t smem, int threads, int n_items, int* grid) {
+int batch_prepare(int kind, int prec, int p, size_t smem, int threads, int n_items, int* grid) {
   if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "batch tile too large for shared memory");
-  int st = prec == FLSP_FP64 ? batch_attr<double>(kind, smem) : batch_attr<float>(kind, smem);
-  if (st) return st;
-  auto g = [&](auto tz) -> int {
-    using T = decltype(tz);
-    if (kind == kBatchKindAdv) return persistent_grid(batch_adv_kernel<T>, threads, smem, n_items);
-    if (kind == kBatchKindHJ) return persistent_grid(batch_hj_kernel<T>, threads, smem, n_items);
-    return persistent_grid(batch_weno_kernel<T>, threads, smem, n_items);
-  };
-  *grid = prec == FLSP_FP64 ? g((double)0) : g((float)0);
-  return FLSP_OK;
+  return with_degree(p, [&](auto PC) -> int {
+    constexpr int P = decltype(PC)::value;
+    int st = prec == FLSP_FP64 ? batch_attr<double, P>(kind, smem) : batch_attr<float, P>(kind, smem);
+    if (st) return st;
+    auto g = [&](auto tz) -> int {
+      using T = decltype(tz);
+      if (kind == kBatchKindAdv) return persistent_grid(batch_adv_kernel<T, P>, threads, smem, n_items);
+      if (kind == kBatchKindHJ) return persistent_grid(batch_hj_kernel<T, P>, threads, smem, n_items);
+      return persistent_grid(batch_weno_kernel<T, P>, threads, smem, n_items);
+    };
+    *grid = prec == FLSP_FP64 ? g((double)0) : g((float)0);
+    return FLSP_OK;
+  });
 }
 
-int launch_batch_adv(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                     int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine) {
-  if (prec == FLSP_FP64)
-    batch_adv_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
-  else
-    batch_adv_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
-  return launch_status("batch_adv_kernel");
+int launch_batch_adv(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                     int grid, int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine) {
+  return with_degree(p, [&](auto PC) -> int {
+    constexpr int P = decltype(PC)::value;
+    if (prec == FLSP_FP64)
+      batch_adv_kernel<double, P><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
+    else
+      batch_adv_kernel<float, P><<<grid, threads, smem, s>>>(probs, items, n_items, ix, in_n, iout, stage, combine);
+    return launch_status("batch_adv_kernel");
+  });
 }
 
-int launch_batch_hj(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                    int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk) {
-  if (prec == FLSP_FP64)
-    batch_hj_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
-  else
-    batch_hj_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
-  return launch_status("batch_hj_kernel");
+int launch_batch_hj(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                    int grid, int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk) {
+  return with_degree(p, [&](auto PC) -> int {
+    constexpr int P = decltype(PC)::value;
+    if (prec == FLSP_FP64)
+      batch_hj_kernel<double, P><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
+    else
+      batch_hj_kernel<float, P><<<grid, threads, smem, s>>>(probs, items, n_items, isrc, iphi0, idst, mode, rk);
+    return launch_status("batch_hj_kernel");
+  });
 }
 
-int launch_batch_weno(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                      int threads, size_t smem, int iin, int iout) {
-  if (prec == FLSP_FP64)
-    batch_weno_kernel<double><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
-  else
-    batch_weno_kernel<float><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
-  return launch_status("batch_weno_kernel");
+int launch_batch_weno(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                      int grid, int threads, size_t smem, int iin, int iout) {
+  return with_degree(p, [&](auto PC) -> int {
+    constexpr int P = decltype(PC)::value;
+    if (prec == FLSP_FP64)
+      batch_weno_kernel<double, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
+    else
+      batch_weno_kernel<float, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
+    return launch_status("batch_weno_kernel");
+  });
 }
 
 }  // namespace flsp

@@ -60,15 +60,16 @@ enum BatchClockOp : int {
 int upload_tables_batch();
 // shared memory one problem needs for a tile of the given kind
 int batch_smem(int kind, int p, int prec, const int* tile, int n_terms, size_t* bytes);
-// kernel attributes for `smem` and the persistent grid for n_items
-int batch_prepare(int kind, int prec, size_t smem, int threads, int n_items, int* grid);
+// kernel attributes of the degree-p kernel for `smem` and its persistent
+// grid for n_items (every item of a launch has degree p)
+int batch_prepare(int kind, int prec, int p, size_t smem, int threads, int n_items, int* grid);
 int launch_batch_clock(cudaStream_t s, const BatchProb* probs, int n, int what, double cfl_max);
-int launch_batch_adv(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                     int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine);
-int launch_batch_hj(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                    int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk);
-int launch_batch_weno(cudaStream_t s, int prec, const BatchProb* probs, const int2* items, int n_items, int grid,
-                      int threads, size_t smem, int iin, int iout);
+int launch_batch_adv(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                     int grid, int threads, size_t smem, int ix, int in_n, int iout, int stage, int combine);
+int launch_batch_hj(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                    int grid, int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk);
+int launch_batch_weno(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
+                      int grid, int threads, size_t smem, int iin, int iout);
 
 // restrict a launch's MeshArgs to the narrow-band tile list of `kind`
 inline void apply_band(const Ctx& c, int kind, MeshArgs& m) {
