@@ -32,6 +32,9 @@ def cases():
                              F.sphere((0.35, 0.35, 0.35), 0.15), "rhs"),
         "sphere_p2_3d_grad": (3, (6, 5, 4), 2, abi.BASIS_P, F.deformation_3d(),
                               F.sphere((0.45, 0.5, 0.55), 0.3), "grad"),
+        "circles_q2_curvature": (2, (16, 16), 2, abi.BASIS_Q, F.ccw_rotation(),
+                                 F.sphere((0.4731, 0.5193), 0.25) + F.sphere((0.6817, 0.3109), 0.17),
+                                 "curvature"),
     }
 
 
@@ -56,15 +59,20 @@ def compute(name, spec):
     elif what == "grad":
         gl, gr = pr.hj_gradients(phi0)
         out["result"] = np.concatenate([gl.ravel(), gr.ravel()])
+    elif what == "curvature":
+        out["result"] = pr.curvature(phi0)
+        out["result_neighbour"] = pr.curvature(phi0, to_neighbour=True)
     return out
 
 
-def main():
+def main(names=None):
     for name, spec in cases().items():
+        if names and name not in names:
+            continue
         out = compute(name, spec)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(name, {k: v.shape for k, v in out.items()})
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -300,7 +300,7 @@ def test_reinit_viscosity(oracle, flsp, dim, p, basis, mode):
 
 
 @pytest.mark.parametrize("name", ["zalesak_p1_rhs", "zalesak_q2_rk3", "circles_q2_reinit", "sphere_q2_3d_rhs",
-                                  "sphere_p2_3d_grad"])
+                                  "sphere_p2_3d_grad", "circles_q2_curvature"])
 def test_golden_fixtures(flsp, name):
     """the library against the committed oracle fixtures (tests/golden/)"""
     import importlib.util
@@ -324,6 +324,9 @@ def test_golden_fixtures(flsp, name):
         ReinitSimulatorLDG(sim.problem).run_iteration(abi.default_reinit_opts(mode=abi.REINIT_FIXED,
                                                                               n_pseudo_steps=3))
         got = sim.get_solution_vector()
+    elif what == "curvature":
+        got = sim.problem.curvature(abi.CURV_REFERENCE)
+        assert rel(sim.problem.curvature(abi.CURV_NEIGHBOUR), ref["result_neighbour"]) <= 1e-11
     else:
         gl, gr = ReinitSimulatorLDG(sim.problem).local_left_right_gradients()
         got = np.concatenate([gl.ravel(), gr.ravel()])

@@ -245,7 +245,7 @@ def test_mlp_gradient_fd(oracle):
 
 
 @pytest.mark.parametrize("name", ["zalesak_p1_rhs", "zalesak_q2_rk3", "circles_q2_reinit", "sphere_q2_3d_rhs",
-                                  "sphere_p2_3d_grad"])
+                                  "sphere_p2_3d_grad", "circles_q2_curvature"])
 def test_golden(oracle, name):
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
