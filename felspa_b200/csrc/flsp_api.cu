@@ -975,6 +975,10 @@ int flsp_curvature(flsp_handle* h, int mode, double* kappa, int64_t n) {
 
 int flsp_export_solutions(flsp_handle* h, const char* path, const char* label) {
   if (!h || !path || !label || !label[0]) return fail(FLSP_ERR_BAD_ARG, "null or empty argument");
+  for (const char* c = label; *c; ++c)
+    if (!((*c >= 'a' && *c <= 'z') || (*c >= 'A' && *c <= 'Z') || (*c >= '0' && *c <= '9') || *c == '_' ||
+          *c == '-' || *c == '.'))
+      return fail(FLSP_ERR_BAD_ARG, "labels may hold letters, digits, '_', '-' and '.' only");
   CU(cudaSetDevice(h->dev));
   double t = 0.0;
   ST(flsp_get_time(h, &t));

@@ -302,6 +302,18 @@ int launch_curvature(const Ctx& c, const void* phi, const int64_t* perm, int64_t
 
 namespace {
 
+// labels become XML attribute values and parts of file names: letters,
+// digits, '_', '-' and '.' only
+bool plain_label(const char* s) {
+  if (!s || !s[0]) return false;
+  for (const char* c = s; *c; ++c) {
+    const bool ok = (*c >= 'a' && *c <= 'z') || (*c >= 'A' && *c <= 'Z') || (*c >= '0' && *c <= '9') || *c == '_' ||
+                    *c == '-' || *c == '.';
+    if (!ok) return false;
+  }
+  return true;
+}
+
 bool write_all(FILE* f, const std::string& s) { return std::fwrite(s.data(), 1, s.size(), f) == s.size(); }
 
 }  // namespace
@@ -310,6 +322,8 @@ int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, 
                    const char* filename, const double* values2, const char* label2) {
   if (!mesh || !values || !label || !filename || !label[0] || !filename[0])
     return set_error(FLSP_ERR_BAD_ARG, "null or empty argument");
+  if (!plain_label(label) || (values2 && !plain_label(label2)))
+    return set_error(FLSP_ERR_BAD_ARG, "labels may hold letters, digits, '_', '-' and '.' only");
   const int dim = mesh->dim;
   if (dim != 2 && dim != 3) return set_error(FLSP_ERR_BAD_ARG, "dim must be 2 or 3");
   if (n_sub < 1 || n_sub > 16) return set_error(FLSP_ERR_BAD_ARG, "n_sub must be in 1..16");
@@ -431,9 +445,9 @@ int write_pvd_file(const char* filename, int n, const double* times, const char*
       "  <Collection>\n";
   char buf[64];
   for (int i = 0; i < n; ++i) {
-    if (!files[i]) {
+    if (!files[i] || !plain_label(files[i])) {
       std::fclose(f);
-      return set_error(FLSP_ERR_BAD_ARG, "null file name");
+      return set_error(FLSP_ERR_BAD_ARG, "PVD records: file names of letters, digits, '_', '-' and '.' only");
     }
     std::snprintf(buf, sizeof(buf), "%.17g", times[i]);
     s += std::string("    <DataSet timestep=\"") + buf + "\" group=\"\" part=\"0\" file=\"" + files[i] + "\"/>\n";

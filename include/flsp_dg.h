@@ -339,7 +339,8 @@ int flsp_eval_patches(flsp_handle* h, int n_sub, double* values, int64_t n);
    and records (time, file name); <path><label>.pvd is rewritten with every
    record so far on each call (the reference's PVDCollector,
    src/base/io.cc:142-166, writes it once, at destruction).  `path` is a
-   prefix (a directory ends with '/').  As the reference, the last
+   prefix (a directory ends with '/'); `label` holds letters, digits, '_',
+   '-' and '.' only (it names files and XML attributes).  As the reference, the last
    flsp_curvature result is written too, as `<label>Curvature`, when its
    time equals the state's (within 1e-12, numerics::is_nearly_equal).   */
 int flsp_export_solutions(flsp_handle* h, const char* path, const char* label);

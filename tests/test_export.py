@@ -142,3 +142,8 @@ def test_writers_reject_bad_arguments(flsp, tmp_path):
         write_vtu(mesh, np.zeros(16), "phi", str(tmp_path / "missing_dir" / "a.vtu"))
     with pytest.raises(FlspError):
         write_pvd(str(tmp_path / "missing_dir" / "a.pvd"), [])
+    # labels and record names become XML attributes and file names
+    with pytest.raises(FlspError):
+        write_vtu(mesh, np.zeros(16), 'phi" evil="1', str(tmp_path / "b.vtu"))
+    with pytest.raises(FlspError):
+        write_pvd(str(tmp_path / "b.pvd"), [(0.0, "a<b.vtu")])
