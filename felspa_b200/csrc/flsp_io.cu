@@ -437,6 +437,11 @@ int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, 
 int write_pvd_file(const char* filename, int n, const double* times, const char* const* files) {
   if (!filename || !filename[0] || n < 0 || (n > 0 && (!times || !files)))
     return set_error(FLSP_ERR_BAD_ARG, "null or empty argument");
+  // every record is checked before the file is opened, so a rejected call
+  // leaves an existing collection as it was
+  for (int i = 0; i < n; ++i)
+    if (!files[i] || !plain_label(files[i]))
+      return set_error(FLSP_ERR_BAD_ARG, "PVD records: file names of letters, digits, '_', '-' and '.' only");
   FILE* f = std::fopen(filename, "wb");
   if (!f) return set_error(FLSP_ERR_BAD_ARG, std::string("cannot open ") + filename);
   std::string s =
@@ -445,10 +450,6 @@ int write_pvd_file(const char* filename, int n, const double* times, const char*
       "  <Collection>\n";
   char buf[64];
   for (int i = 0; i < n; ++i) {
-    if (!files[i] || !plain_label(files[i])) {
-      std::fclose(f);
-      return set_error(FLSP_ERR_BAD_ARG, "PVD records: file names of letters, digits, '_', '-' and '.' only");
-    }
     std::snprintf(buf, sizeof(buf), "%.17g", times[i]);
     s += std::string("    <DataSet timestep=\"") + buf + "\" group=\"\" part=\"0\" file=\"" + files[i] + "\"/>\n";
   }

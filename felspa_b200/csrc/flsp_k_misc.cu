@@ -1,8 +1,11 @@
 // flsp_k_misc.cu — limiter, projection, reductions, clocks, DoF order
 // (instantiations + launchers).
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "flsp_launch.h"
@@ -185,12 +188,52 @@ constexpr long long kNoAllocDoubles = 2LL * kNoAllocBlocks + 2;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];   // ~1 MiB
 static __device__ __align__(256) flsp_ic_desc g_noalloc_ic;
 
+// Set-up state per device ordinal, valid for the CUDA context it was made
+// in: after cudaDeviceReset the next call on that device runs in a new
+// primary context (new module, zeroed constant tables, possibly another
+// symbol address), so the context's unique id is part of the key.
 struct NoAllocDevice {
-  bool ready = false;
+  unsigned long long ctx_id = 0;   // 0: not set up
   double* scratch = nullptr;
   flsp_ic_desc* ic = nullptr;
 };
 NoAllocDevice g_noalloc_dev[64];
+std::mutex g_noalloc_mu[64];
+
+// unique id of the calling thread's current CUDA context (driver entry
+// points fetched through the runtime, so the library does not link libcuda)
+int current_context_id(int dev, unsigned long long* id) {
+  typedef CUresult (*GetCurrent)(CUcontext*);
+  typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_current = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      get_id = nullptr;
+  });
+  if (!get_current || !get_id) return flsp::set_error(FLSP_ERR_CUDA, "driver entry points cuCtxGetCurrent/cuCtxGetId");
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return flsp::set_error(FLSP_ERR_CUDA, "cuCtxGetCurrent failed");
+  if (!ctx) {   // no context yet on this thread: make the device's primary context current
+    cudaError_t e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return flsp::set_error(FLSP_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return flsp::set_error(FLSP_ERR_CUDA, "no current CUDA context");
+  }
+  if (get_id(ctx, id) != CUDA_SUCCESS) return flsp::set_error(FLSP_ERR_CUDA, "cuCtxGetId failed");
+  return FLSP_OK;
+}
+
+// the IC description travels as a kernel parameter (copied at launch, so
+// the caller's host struct is not read after the call returns)
+__global__ void noalloc_set_ic(const flsp_ic_desc ic, flsp_ic_desc* dst) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = ic;
+}
 
 __global__ void noalloc_finalize(const double* sums, int which, long long ndofs, double* result) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -220,7 +263,8 @@ extern "C" int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int b
   const bool need_ref = which == FLSP_RED_L1_INTERFACE || which == FLSP_RED_MEAN_ABS_DIFF;
   if (need_ic && !ic) return set_error(FLSP_ERR_BAD_ARG, "this reduction needs an IC");
   if (need_ref && !ref_state) return set_error(FLSP_ERR_BAD_ARG, "this reduction needs ref_state");
-  if (ic && (ic->n_nodes < 1 || ic->n_nodes > FLSP_MAX_IC_NODES || ic->root < 0 || ic->root >= ic->n_nodes))
+  if (ic && (ic->n_nodes < 1 || ic->n_nodes > FLSP_MAX_IC_NODES || ic->root < 0 || ic->root >= ic->n_nodes ||
+             ic->n_waves < 0 || ic->n_waves > FLSP_MAX_IC_WAVES))
     return set_error(FLSP_ERR_BAD_ARG, "bad IC description");
   long long ncell = 1;
   for (int d = 0; d < mesh->dim; ++d) {
@@ -235,15 +279,29 @@ extern "C" int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int b
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_error(FLSP_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) return set_error(FLSP_ERR_BAD_ARG, "device ordinal out of range");
-  NoAllocDevice& nd = g_noalloc_dev[dev];
-  if (!nd.ready) {   // once per device, with that device current
-    int st = upload_tables_misc();
+  unsigned long long ctx_id = 0;
+  {
+    const int st = current_context_id(dev, &ctx_id);
     if (st) return st;
-    e = cudaGetSymbolAddress((void**)&nd.scratch, g_noalloc_scratch);
-    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    e = cudaGetSymbolAddress((void**)&nd.ic, g_noalloc_ic);
-    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    nd.ready = true;
+  }
+  double* scratch = nullptr;
+  flsp_ic_desc* ic_dev = nullptr;
+  {
+    // once per device and context, with that device current
+    std::lock_guard<std::mutex> lock(g_noalloc_mu[dev]);
+    NoAllocDevice& nd = g_noalloc_dev[dev];
+    if (nd.ctx_id != ctx_id) {
+      nd.ctx_id = 0;
+      int st = upload_tables_misc();
+      if (st) return st;
+      e = cudaGetSymbolAddress((void**)&nd.scratch, g_noalloc_scratch);
+      if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      e = cudaGetSymbolAddress((void**)&nd.ic, g_noalloc_ic);
+      if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      nd.ctx_id = ctx_id;
+    }
+    scratch = nd.scratch;
+    ic_dev = nd.ic;
   }
 
   Ctx c;
@@ -279,13 +337,14 @@ extern "C" int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int b
       }
   m.nb = nb;
 
-  if (ic) {
-    e = cudaMemcpyAsync(nd.ic, ic, sizeof(flsp_ic_desc), cudaMemcpyHostToDevice, c.stream);
-    if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("IC copy: ") + cudaGetErrorString(e));
+  if (need_ic) {
+    noalloc_set_ic<<<1, 1, 0, c.stream>>>(*ic, ic_dev);
+    const int st = launch_status("noalloc_set_ic");
+    if (st) return st;
   }
-  double* partial = nd.scratch;
-  double* sums = nd.scratch + 2LL * kNoAllocBlocks;
-  int st = launch_reduce(c, which, state, need_ref ? ref_state : nullptr, need_ic ? nd.ic : nullptr, partial, sums);
+  double* partial = scratch;
+  double* sums = scratch + 2LL * kNoAllocBlocks;
+  int st = launch_reduce(c, which, state, need_ref ? ref_state : nullptr, need_ic ? ic_dev : nullptr, partial, sums);
   if (st) return st;
   noalloc_finalize<<<1, 1, 0, c.stream>>>(sums, which, ncell * nb, result);
   return launch_status("noalloc_finalize");

@@ -243,6 +243,9 @@ int flsp_set_state(flsp_handle* h, const double* coeffs, int64_t n);
 int flsp_get_state(flsp_handle* h, double* coeffs, int64_t n);
 int flsp_set_time(flsp_handle* h, double t);
 int flsp_get_time(const flsp_handle* h, double* t);
+/* advection substeps executed since create (the reference keeps no such
+   counter; its drivers count their advance_time calls)                 */
+int flsp_get_step_count(const flsp_handle* h, int64_t* n_substeps);
 /* save the current state as the comparison snapshot of the reductions */
 int flsp_snapshot(flsp_handle* h);
 
@@ -361,16 +364,18 @@ int flsp_write_pvd(const char* filename, int n, const double* times,
    state is the caller's device array (lexicographic cells, deal.II DoF
    order inside a cell, double for FLSP_FP64 / float for FLSP_FP32),
    `ref_state` the caller's device array for the snapshot reductions (or
-   NULL), `ic` a host IC description (or NULL), and the scalar result is
-   written to the caller's device double `result`.  Work is enqueued on
-   `stream` (a cudaStream_t, NULL = default stream) and not waited for.
-   Scratch space is a file-scope device array of 1 MiB (partial sums of at
-   most FLSP_NOALLOC_MAX_CELLS cells); larger meshes are rejected with
-   FLSP_ERR_BAD_ARG.  The first call on a device uploads the basis tables
-   and looks up the array's device address (synchronous); make that first
-   call before any stream capture.  All calls on a device share the array
-   and it keeps the last call's contents: calls that overlap on the GPU
-   race.                                                                 */
+   NULL), `ic` a host IC description (or NULL; it is passed to the device
+   as a kernel argument, so the caller may free it when the call
+   returns), and the scalar result is written to the caller's device
+   double `result`.  Work is enqueued on `stream` (a cudaStream_t, NULL =
+   default stream) and not waited for.  Scratch space is a file-scope
+   device array of 1 MiB (partial sums of at most FLSP_NOALLOC_MAX_CELLS
+   cells); larger meshes are rejected with FLSP_ERR_BAD_ARG.  The first
+   call on a device (and the first call after cudaDeviceReset, which gives
+   the device a new context) uploads the basis tables and looks up the
+   array's device address (synchronous); make that first call before any
+   stream capture.  All calls on a device share the array and it keeps
+   the last call's contents: calls that overlap on the GPU race.          */
 #define FLSP_NOALLOC_MAX_CELLS (65536LL * 128LL)
 int flsp_reduce_noalloc(const flsp_mesh_desc* mesh, int degree, int basis,
                         int precision, const void* state,

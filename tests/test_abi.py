@@ -177,3 +177,38 @@ def test_patch_network_entry_points_without_gpu(flsp):
     lo = abi.LearnedOpts()
     L.flsp_default_learned_opts(C.byref(lo))
     assert L.flsp_ls_run_steps_learned(None, None, C.byref(lo), 10, 10) == abi.FLSP_ERR_BAD_ARG
+
+
+def test_noalloc_argument_checks_without_gpu(flsp):
+    """flsp_reduce_noalloc checks its arguments before any device call:
+    a reduction that needs an IC or a comparison state without one, a bad
+    reduction kind, a bad IC description (the pointers are never
+    dereferenced on the host, so stand-in addresses suffice here)."""
+    from felspa_b200 import fields as F
+    from felspa_b200.level_set import Mesh, reduce_noalloc
+    mesh = Mesh(2, (16, 16))
+    fake = 0x100000   # stand-in device address
+    for which in (abi.RED_MASS_ERROR, abi.RED_L2_ERROR_IC, abi.RED_L1_INTERFACE_IC):
+        with pytest.raises(flsp.FlspError, match="needs an IC"):
+            reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, which, fake)
+    for which in (abi.RED_L1_INTERFACE, abi.RED_MEAN_ABS_DIFF):
+        with pytest.raises(flsp.FlspError, match="needs ref_state"):
+            reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, which, fake)
+    for which in (-1, abi.RED_MASS_SHARP + 1):
+        with pytest.raises(flsp.FlspError, match="bad reduction kind"):
+            reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, which, fake)
+
+    class BadIC:
+        def __init__(self, **kw):
+            self.d = F.zalesak_disk().desc()
+            for k, v in kw.items():
+                setattr(self.d, k, v)
+
+        def desc(self):
+            return self.d
+
+    for kw in ({"n_nodes": 0}, {"root": 7}, {"n_waves": -1}, {"n_waves": 33}):
+        with pytest.raises(flsp.FlspError, match="bad IC"):
+            reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, abi.RED_MASS_ERROR, fake, ic=BadIC(**kw))
+    with pytest.raises(flsp.FlspError, match="null argument"):
+        reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, 0, abi.RED_MASS, fake)

@@ -147,3 +147,14 @@ def test_writers_reject_bad_arguments(flsp, tmp_path):
         write_vtu(mesh, np.zeros(16), 'phi" evil="1', str(tmp_path / "b.vtu"))
     with pytest.raises(FlspError):
         write_pvd(str(tmp_path / "b.pvd"), [(0.0, "a<b.vtu")])
+
+
+def test_rejected_pvd_leaves_existing_collection(flsp, tmp_path):
+    """a call with a bad record name fails before the file is opened: the
+    collection written earlier stays as it was"""
+    f = tmp_path / "LevelSet.pvd"
+    write_pvd(str(f), [(0.0, "LevelSet_000000000.vtu"), (0.5, "LevelSet_000000001.vtu")])
+    before = f.read_bytes()
+    with pytest.raises(FlspError):
+        write_pvd(str(f), [(0.0, "LevelSet_000000000.vtu"), (1.0, "../x.vtu")])
+    assert f.read_bytes() == before
