@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP64 run of the same periods (accuracy of the FP32 mode)")
+    ap.add_argument("--no-oracle-checks", action="store_true",
+                    help="skip the FP64/FP32 GPU runs against the oracle (64^3 first period, Zalesak revolutions)")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the narrow-band and 128^3 variants of the 3D workload")
     ap.add_argument("--no-batched", action="store_true",
@@ -137,31 +139,48 @@ class ClockSampler:
 # ----------------------------------------------------------------------
 # CPU side: the oracle (CPU FP64 restatement of the reference path)
 # ----------------------------------------------------------------------
-def cpu_rate(n_slab_z=16, repeats=1):
-    """DoF-steps/s of the CPU FP64 restatement on a bounded sample: a
-    64 x 64 x n_slab_z slab of the same 64^3 mesh (same cell size), one
-    SSP-RK3 step and one reinit pseudo-step, amortised to the workload's
-    10 steps + 5 pseudo-steps per period."""
-    from oracle import oracle as O
-    from felspa_b200 import abi, fields as F
-    h = 1.0 / N_CELLS
-    pr = O.Problem(3, (N_CELLS, N_CELLS, n_slab_z), DEGREE, abi.BASIS_Q,
-                   lo=(0.0, 0.0, 0.3), hi=(1.0, 1.0, 0.3 + n_slab_z * h))
-    pr.set_velocity(F.deformation_3d())
-    phi = pr.project(F.sphere((0.35, 0.35, 0.35), 0.15))
-    t_step, t_pseudo = [], []
-    ro = abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=1)
-    for _ in range(repeats):
+def workload_config():
+    """the workload, identical on both arms' lines"""
+    return {"workload": WORKLOAD, "mesh": "64^3", "degree": DEGREE, "basis": "Q", "n_dofs": 7077888,
+            "velocity": "3D deformation, T=3", "ic": "sphere r=0.15 at (0.35,0.35,0.35)", "rk": "SSP-RK3",
+            "cfl": CFL, "reinit_every": REINIT_EVERY, "pseudo_steps": N_PSEUDO,
+            "step": "one reinit period: 10 SSP-RK3 substeps + a 5-pseudo-step reinit",
+            "l2": "GPU: flushed between steps (256 MiB write); CPU: every state vector (57 MB) exceeds its caches"}
+
+
+class CpuSample:
+    """The CPU FP64 restatement on the full 64^3 mesh of the workload.  A
+    bench step times one SSP-RK3 substep and one 5-pseudo-step reinit (the
+    whole reinitialisation of a period: set-up, CFL pass, 5 pseudo-steps);
+    the period's rate amortises them as the GPU does, 10 substeps per
+    reinit: rate = n_dofs * 10 / (10 t_substep + t_reinit)."""
+
+    def __init__(self):
+        from oracle import oracle as O
+        from felspa_b200 import abi, fields as F
+        self.abi = abi
+        self.pr = O.Problem(3, (N_CELLS,) * 3, DEGREE, abi.BASIS_Q)
+        self.pr.set_velocity(F.deformation_3d())
+        self.phi = self.pr.project(F.sphere((0.35, 0.35, 0.35), 0.15))
+        self.ro = abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=N_PSEUDO)
+        self.n_dofs = self.pr.n_dofs
+
+    def step(self):
         t0 = time.perf_counter()
-        pr.advance(phi, 1.0, single_cycle=True, cfl_max=CFL)
+        self.pr.advance(self.phi, 1e30, single_cycle=True, cfl_max=CFL)
         t1 = time.perf_counter()
-        pr.reinit(phi, ro)
+        st, _ = self.pr.reinit(self.phi, self.ro)
         t2 = time.perf_counter()
-        t_step.append(t1 - t0)
-        t_pseudo.append(t2 - t1)
-    ts, tp = min(t_step), min(t_pseudo)
-    rate = pr.n_dofs * REINIT_EVERY / (REINIT_EVERY * ts + N_PSEUDO * tp)
-    return rate, {"step_s": ts, "pseudo_step_s": tp, "n_dofs": pr.n_dofs}
+        if st != 0:
+            raise RuntimeError(f"oracle reinit failed ({st})")
+        ts, tr = t1 - t0, t2 - t1
+        return self.n_dofs * REINIT_EVERY / (REINIT_EVERY * ts + tr), ts, tr
+
+
+def cpu_sample_text(ts, tr):
+    return (f"CPU FP64 restatement (OpenMP, {os.cpu_count() or 1} threads) on the full 64^3 Q2 mesh "
+            f"(7,077,888 DoFs): per bench step one SSP-RK3 substep ({ts:.3f} s) and one 5-pseudo-step reinit "
+            f"({tr:.3f} s), amortised to the period (10 substeps per reinit)")
 
 
 def run_reference(args):
@@ -169,25 +188,29 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    rates = []
+    cs = CpuSample()
     for _ in range(args.warmup):
-        cpu_rate()
+        cs.step()
+    rates, walls, tss, trs = [], [], [], []
     for _ in range(args.steps):
-        r, info = cpu_rate()
+        t0 = time.perf_counter()
+        r, ts, tr = cs.step()
+        walls.append(time.perf_counter() - t0)
         rates.append(r)
+        tss.append(ts)
+        trs.append(tr)
     value = statistics.median(rates)
-    sample = (f"64x64x16 slab of the 64^3 Q2 mesh (same h, {info['n_dofs']} DoFs): 1 SSP-RK3 step + "
-              f"1 reinit pseudo-step per bench step, amortised to 10 steps + 5 pseudo-steps")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "DoF-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * info["n_dofs"] * REINIT_EVERY / value,
+        # wall time of one bench step as run (the timed sample), not the
+        # amortised period it stands for
+        "ms_per_step": 1e3 * sum(walls) / len(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD.replace("FP32", "FP64 CPU restatement"),
-                                        "mesh": "64^3", "degree": 2, "basis": "Q", "reinit_every": 10,
-                                        "pseudo_steps": 5, "cfl": CFL},
+        "data": "synthetic", "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "DoF-steps/s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": cpu_sample_text(statistics.median(tss), statistics.median(trs)),
+                         "period_s_amortised": cs.n_dofs * REINIT_EVERY / value},
         "e2e": {"value": value, "unit": "DoF-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -281,24 +304,45 @@ def run_ours(args):
         e2e_ms.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
 
-    # FP32 production mode against FP64 on the same periods: L1 interface
-    # difference and area (FP64 device reductions of the FP64 handle)
-    acc64 = None
+    # FP64 mode on the same workload: timed like the FP32 headline, then the
+    # FP32 state against the FP64 state after the same periods (L1
+    # interface difference and area, FP64 device reductions)
+    fp64 = None
     if not args.no_fp64_check:
-        periods = args.warmup + 2 * args.steps
         s32 = pb.get_state()
         mass32 = ls.integrate_mass()
         ls64 = make_problem(abi.FP64, local)
-        ls64.run_steps(periods * REINIT_EVERY)
-        s64 = ls64.problem.get_state()
+        p64 = ls64.problem
+        st64 = torch.cuda.ExternalStream(p64.stream(), device=local)
+        for _ in range(args.warmup):
+            ls64.run_steps(REINIT_EVERY)
+        t64 = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st64)
+            ls64.run_steps(REINIT_EVERY, sync=False)
+            e1.record(st64)
+            e1.synchronize()
+            t64.append(e0.elapsed_time(e1))
+        # the FP32 problem also ran the e2e periods
+        ls64.run_steps(args.steps * REINIT_EVERY)
+        periods = args.warmup + 2 * args.steps
+        s64 = p64.get_state()
         mass64 = ls64.integrate_mass()
-        ls64.problem.set_state(s32)
-        ls64.problem.snapshot()
-        ls64.problem.set_state(s64)
-        acc64 = {"periods": periods, "l1_interface_fp32_vs_fp64": ls64.problem.reduce(abi.RED_L1_INTERFACE),
-                 "area_fp32_vs_fp64_rel": (mass32 - mass64) / mass64,
-                 "max_coeff_diff_rel": float(abs(s32 - s64).max() / abs(s64).max())}
-        ls64.problem.close()
+        p64.set_state(s32)
+        p64.snapshot()
+        p64.set_state(s64)
+        fp64 = {"value": n_dofs * REINIT_EVERY * args.steps / (sum(t64) * 1e-3), "unit": "DoF-steps/s",
+                "ms_per_step": sum(t64) / args.steps, "dtype": "f64",
+                "what": "the same workload and timing in the FP64 (parity) mode",
+                "fp32_vs_fp64": {"periods": periods,
+                                 "l1_interface_fp32_vs_fp64": p64.reduce(abi.RED_L1_INTERFACE),
+                                 "area_fp32_vs_fp64_rel": (mass32 - mass64) / mass64,
+                                 "max_coeff_diff_rel": float(abs(s32 - s64).max() / abs(s64).max())}}
+        p64.close()
 
     # roofline of the dominant kernel (advection stage), events on the library stream
     ms_stage = pb.time_kernel(0, reps=20)
@@ -325,7 +369,10 @@ def run_ours(args):
                 "traffic": (tr or {}).get("adv_stage_bytes_per_launch"),
                 "kernel": "adv_sep_kernel<3,2,float>", "ms_per_launch": ms_stage,
                 "algorithmic_bytes_per_launch": alg_bytes_per_launch, "peak_source": peak_kind,
-                "hj_ms_per_launch": ms_hj}
+                "hj_ms_per_launch": ms_hj, "hj_algorithmic_bytes_per_launch": 3.0 * s * n_dofs,
+                "hj_frac": 3.0 * s * n_dofs / (ms_hj * 1e-3) / 1e9 / peak,
+                "stage_tile": list(tile),
+                "stage_tile_ms": {"x".join(map(str, k)): v for k, v in tile_ms.items()}}
 
     per_step_launches = REINIT_EVERY * 5 + 2 + 3 * N_PSEUDO
     if rank != 0:
@@ -335,31 +382,30 @@ def run_ours(args):
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        rate, info = cpu_rate()
+        cs = CpuSample()
+        rate, t_sub, t_re = cs.step()
         cpu = {"value": rate, "unit": "DoF-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
-               "sample": (f"CPU FP64 restatement, 64x64x16 slab of the 64^3 Q2 mesh ({info['n_dofs']} DoFs): "
-                          f"1 SSP-RK3 step {info['step_s']:.3f}s + 1 pseudo-step {info['pseudo_step_s']:.3f}s, "
-                          f"amortised to 10 steps + 5 pseudo-steps")}
+               "sample": cpu_sample_text(t_sub, t_re)}
+        del cs
 
     line = {
         "metric": METRIC, "value": value, "unit": "DoF-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "mesh": "64^3", "degree": 2, "basis": "Q", "n_dofs": n_dofs,
-                   "velocity": "3D deformation, T=3", "ic": "sphere r=0.15 at (0.35,0.35,0.35)",
-                   "rk": "SSP-RK3", "cfl": CFL, "reinit_every": REINIT_EVERY, "pseudo_steps": N_PSEUDO,
-                   "step": "10 SSP-RK3 substeps + 1 reinit, one CUDA graph",
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "stage_tile": list(tile),
-                   "stage_tile_ms": {"x".join(map(str, k)): v for k, v in tile_ms.items()}},
+        "config": workload_config(), "parallelism": f"replicas x{world}",
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "DoF-steps/s", "h2d_bytes_per_step": 8 * n_dofs,
                 "d2h_bytes_per_step": 8 * n_dofs, "ms_per_step": e2e_total / args.steps},
         "gpu_launches": per_step_launches * args.steps,
         "clocks": clocks,
-        "accuracy": {"area_rel_change": (area1 - area0) / area0, "fp32_vs_fp64": acc64},
+        "fp64": fp64,
+        "accuracy": {"area_rel_change": (area1 - area0) / area0,
+                     "fp32_vs_fp64": (fp64 or {}).get("fp32_vs_fp64")},
     }
+    if world == 1 and not args.no_oracle_checks:
+        line["accuracy"]["sphere_64cubed_vs_oracle"] = sphere_vs_oracle(local)
+        line["accuracy"]["zalesak_128"] = zalesak_accuracy(local)
     if world == 1 and not args.no_learned:
         line["learned_vs_plain"] = learned_comparison()
         line["learned_vs_plain_3d"] = learned_comparison_3d()
@@ -408,6 +454,86 @@ def run_ours(args):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def sphere_vs_oracle(device):
+    """The 3D workload's first reinit period from the projected sphere, FP64
+    and FP32 GPU modes against the oracle (CPU FP64, all host cores) on the
+    full 64^3 mesh."""
+    from oracle import oracle as O
+    from felspa_b200 import abi, fields as F
+    ic = F.sphere((0.35, 0.35, 0.35), 0.15)
+    orc = O.Problem(3, (N_CELLS,) * 3, DEGREE, abi.BASIS_Q)
+    orc.set_velocity(F.deformation_3d())
+    phi = orc.project(ic)
+    ctl = abi.default_ls_opts(reinit_frequency=REINIT_EVERY,
+                              reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=N_PSEUDO))
+    t0 = time.perf_counter()
+    for _ in range(REINIT_EVERY):
+        orc.ls_advance(phi, 1e30, ctl, single_step=True, cfl_max=CFL)
+    cpu_s = time.perf_counter() - t0
+    ref_l1 = orc.reduce(abi.RED_L1_INTERFACE_IC, phi, ic=ic)
+    ref_mass = orc.reduce(abi.RED_MASS, phi)
+    out = {"what": "64^3 Q2, one reinit period (10 SSP-RK3 substeps + 5 pseudo-steps) from the projected sphere; "
+                   "GPU state against the oracle's",
+           "oracle_cpu_s": cpu_s, "oracle_threads": os.cpu_count() or 1,
+           "oracle_l1_interface_vs_ic": ref_l1}
+    for prec, name in ((abi.FP64, "fp64"), (abi.FP32, "fp32")):
+        ls = make_problem(prec, device)
+        ls.run_steps(REINIT_EVERY)
+        got = ls.problem.get_state()
+        # L1 interface difference GPU vs oracle: the oracle's state as the snapshot
+        ls.problem.set_state(phi)
+        ls.problem.snapshot()
+        ls.problem.set_state(got)
+        out[name] = {"time_diff": ls.get_time() - orc.clock.t,
+                     "max_coeff_diff_rel": float(np.abs(got - phi).max() / np.abs(phi).max()),
+                     "l1_interface_vs_oracle": ls.problem.reduce(abi.RED_L1_INTERFACE),
+                     "area_vs_oracle_rel": (ls.integrate_mass() - ref_mass) / ref_mass}
+        ls.problem.close()
+    return out
+
+
+def zalesak_accuracy(device):
+    """The 2D Zalesak workload (128^2, degree 1, Q and P bases, one full
+    revolution, reinit every 10 substeps with 5 pseudo-steps): FP64 and
+    FP32 GPU runs, each with its L1 interface error against the initial
+    shape and its area change; beside them the oracle's full-revolution
+    run of the FP64 mode (frozen in tests/golden, with the CPU time and
+    thread count of the machine that ran it)."""
+    from felspa_b200 import abi
+    from felspa_b200.zalesak import revolution
+    out = {"what": "128^2 degree-1 slotted disk, one CCW revolution (T = 1), SSP-RK3 at CFL 0.1, fixed "
+                   "5-pseudo-step reinit every 10 substeps over every cell; L1 interface error vs the initial "
+                   "shape, area change; LDG viscosity 0 (as the configuration) and 1e-3 (the reference test's)"}
+    for basis, bname in ((abi.BASIS_Q, "q1"), (abi.BASIS_P, "p1")):
+        for nu, nname in ((0.0, "nu0"), (1e-3, "nu1e-3")):
+            key = f"zalesak128_{bname}_{nname}"
+            r64 = revolution(basis, nu, abi.FP64, device=device)
+            r32 = revolution(basis, nu, abi.FP32, device=device)
+            row = {"n_dofs": r64["n_dofs"], "substeps": r64["substeps"], "t_end": r64["t_end"]}
+            for r, nm in ((r64, "gpu_fp64"), (r32, "gpu_fp32")):
+                row[nm] = {k: r[k] for k in ("l1_interface_error", "area_change_rel", "wall_s", "dof_steps_per_s")}
+            row["fp32_vs_fp64_max_coeff_diff_rel"] = float(np.abs(r32["state"] - r64["state"]).max()
+                                                           / np.abs(r64["state"]).max())
+            gpath = os.path.join(ROOT, "tests", "golden", key + ".npz")
+            if os.path.exists(gpath):
+                g = np.load(gpath)
+                row["oracle_fp64"] = {"l1_interface_error": float(g["l1_ic"]),
+                                      "area_change_rel": float((g["area1"] - g["area0"]) / g["area0"]),
+                                      "substeps": int(g["n_substeps"]), "cpu_s": float(g["cpu_s"]),
+                                      "threads": int(g["threads"]),
+                                      "dof_steps_per_s": r64["n_dofs"] * int(g["n_substeps"]) / float(g["cpu_s"])}
+                if "result" in g:
+                    row["gpu_fp64_vs_oracle_max_coeff_diff_rel"] = float(
+                        np.abs(r64["state"] - g["result"]).max() / np.abs(g["result"]).max())
+                else:
+                    nb = 4 if basis == abi.BASIS_Q else 3
+                    row["gpu_fp64_vs_oracle_cell_mean_diff_rel"] = float(
+                        np.abs(r64["state"].reshape(-1, nb)[:, 0] - g["cell_means"]).max()
+                        / np.abs(g["cell_means"]).max())
+            out[key] = row
+    return out
 
 
 def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=0, band_cells=6.0):

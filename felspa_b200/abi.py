@@ -48,6 +48,7 @@ class MeshDesc(C.Structure):
         ("lo", C.c_double * 3),
         ("hi", C.c_double * 3),
         ("host_cell_order", C.POINTER(C.c_int64)),
+        ("boundary_ids", C.POINTER(C.c_int32)),
     ]
 
 
@@ -183,7 +184,7 @@ def default_ls_opts(reinit=None, **kw):
     return o
 
 
-def mesh_desc(dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=None):
+def mesh_desc(dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=None, boundary_ids=None):
     m = MeshDesc()
     m.dim = dim
     n = list(n) + [1] * (3 - len(n))
@@ -194,4 +195,5 @@ def mesh_desc(dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=No
         m.lo[d] = float(lo[d])
         m.hi[d] = float(hi[d])
     m.host_cell_order = host_cell_order
+    m.boundary_ids = boundary_ids
     return m

@@ -73,13 +73,15 @@ __host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms) {
 // Upwind flux through face (E, S) of a cell (S = 1: upper face, outward
 // normal +e_E), projected onto the face modes:
 //   Fm[m] = sum_q w_q v_n(q) phi_hat(q) L_m(q),  v_n = (S ? 1 : -1) u_E,
-//   phi_hat = v_n > 0 ? own trace : neighbour trace (own trace on the
-// boundary: zero-Neumann inflow, advection.implement.h:719-741).
+//   phi_hat = v_n > 0 ? own trace : neighbour trace; on the domain
+// boundary the neighbour trace is the Dirichlet value `gd` where the face
+// carries one (dir), else the own trace (zero-Neumann inflow,
+// advection.implement.h:719-741).
 // vel_e(q0, q1) returns the weighted normal component u_E(q) w_q (w_q > 0,
 // so its sign is the sign of u_E).
 template <int DIM, int P, int E, int S, typename T, typename VelE>
 __device__ __forceinline__ void face_flux(const Tab1D<T>& tb, const T* c, const T* cn, bool has_nb,
-                                          VelE&& vel_e, T* Fm) {
+                                          VelE&& vel_e, T* Fm, bool dir = false, T gd = T(0)) {
   constexpr int N1 = P + 1, NQ = P + 2, NF = ipow(N1, DIM - 1);
   constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
   constexpr int st[3] = {1, N1, N1 * N1};
@@ -95,7 +97,7 @@ __device__ __forceinline__ void face_flux(const Tab1D<T>& tb, const T* c, const 
       if (has_nb) sx += (S ? tb.L0[a] : tb.L1[a]) * cn[base + a * st[E]];
     }
     tin[mf] = si;
-    tex[mf] = has_nb ? sx : si;
+    tex[mf] = has_nb ? sx : (dir ? (mf == 0 ? gd : T(0)) : si);
   }
   if constexpr (DIM == 2) {
 #pragma unroll
@@ -383,8 +385,10 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     const bool has_nb = g[E] + 1 < m.n[E];
     const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
     T Fm[NF];
+    T gd = T(0);
+    const bool dir = !has_nb && bc_dirichlet<DIM>(m, E, 1, g, gd);
     face_flux<DIM, P, E, 1, T>(tb, c, cn, has_nb, face_vel(std::integral_constant<int, E>(),
-                                                          std::integral_constant<int, 1>()), Fm);
+                                                          std::integral_constant<int, 1>()), Fm, dir, gd);
     scatter_face<DIM, P, E, T>(R, tb.L1, Fm, -ih[E]);
     if (has_nb && l[E] + 1 < tl[E]) {
 #pragma unroll
@@ -410,8 +414,10 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
       nl[E] -= 1;
       const bool has_nb = g[E] > 0;
       const T* cn = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
+      T gd = T(0);
+      const bool dir = !has_nb && bc_dirichlet<DIM>(m, E, 0, g, gd);
       face_flux<DIM, P, E, 0, T>(tb, c, cn, has_nb, face_vel(std::integral_constant<int, E>(),
-                                                            std::integral_constant<int, 0>()), Fm);
+                                                            std::integral_constant<int, 0>()), Fm, dir, gd);
       scatter_face<DIM, P, E, T>(R, tb.L0, Fm, -ih[E]);
     }
   };

@@ -15,8 +15,9 @@
 //     F = c g_EE (A_Et0 (x) A_Et1) (T- + T+)/2
 //       + |c g_EE| (B_Et0 (x) B_Et1) (T- - T+)/2,   B_de = A_de with |g_de|
 //   (|u_E| = |c g_EE| |g_Et0| |g_Et1| is separable too; on the domain
-//   boundary T+ = T- (own trace, zero-Neumann inflow), so the second term
-//   vanishes); R- -= L(1) F / h_E, R+ += L(0) F / h_E.
+//   boundary the missing trace is the Dirichlet value of the face, or the
+//   own trace (zero-Neumann inflow), when the second term vanishes);
+//   R- -= L(1) F / h_E, R+ += L(0) F / h_E.
 //
 // The CTA's halo box (one bulk copy per row of cells, each row keeping its
 // 16-byte phase from HBM so that 27-value cells need no splitting) and its
@@ -367,11 +368,12 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
 
   // flux through the face normal to E in +e_E between the lower cell (L1
   // trace of the box copy cm) and the upper cell (L0 trace of the box copy
-  // cp); a missing side takes
-  // the other side's trace (domain boundary: own trace).  Tangential
-  // operator rows at local coordinates lc, g_EE at the face = fe.
+  // cp); on the domain boundary the missing side's trace is the Dirichlet
+  // value gd (constant mode only) where the face carries one (dir), else
+  // the other side's (own) trace, zero-Neumann.  Tangential operator rows
+  // at local coordinates lc, g_EE at the face = fe.
   auto face_flux_sep = [&](auto EC, const T* cm, const T* cp, bool has_m, bool has_p, const int* lc,
-                           T fe, T* F) {
+                           T fe, T* F, bool dir, T gd) {
     constexpr int E = decltype(EC)::value;
     constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
     // traces straight from the box copies (Q layout), or through the
@@ -393,10 +395,16 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
     const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
     if (sigma != T(0)) {
       // upwind side: the lower cell where u_E > 0; a missing side takes the
-      // other (domain boundary: own trace)
-      const bool up_m = (s1 * sigma > T(0)) ? has_m : !has_p;
+      // Dirichlet value or, without one, the other side (own trace)
+      const bool flow_up = s1 * sigma > T(0);
       T W[NF];
-      trace(up_m ? cm : cp, up_m ? tb.L1 : tb.L0, W);
+      if (dir && !(flow_up ? has_m : has_p)) {
+#pragma unroll
+        for (int mf = 0; mf < NF; ++mf) W[mf] = mf == 0 ? gd : T(0);
+      } else {
+        const bool up_m = flow_up ? has_m : !has_p;
+        trace(up_m ? cm : cp, up_m ? tb.L1 : tb.L0, W);
+      }
       face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
       return;
     }
@@ -405,11 +413,12 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
     if (has_p) trace(cp, tb.L0, D);
 #pragma unroll
     for (int mf = 0; mf < NF; ++mf) {
-      const T tm = has_m ? S[mf] : D[mf], tp = has_p ? D[mf] : S[mf];
+      const T ghost = dir ? (mf == 0 ? gd : T(0)) : T(0);
+      const T tm = has_m ? S[mf] : (dir ? ghost : D[mf]), tp = has_p ? D[mf] : (dir ? ghost : S[mf]);
       S[mf] = T(0.5) * (tm + tp);
       D[mf] = T(0.5) * (tm - tp);
     }
-    face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, has_m && has_p, F);
+    face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, (has_m && has_p) || dir, F);
   };
 
   T R[NM];
@@ -439,7 +448,9 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
       const bool has_nb = g[E] + 1 < m.n[E];
       const T* cn = cellp(nl[0], nl[1], nl[2]);
       T F[NF];
-      face_flux_sep(EC, cme, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F);
+      T gd = T(0);
+      const bool dir = !has_nb && bc_dirichlet<DIM>(m, E, 1, g, gd);
+      face_flux_sep(EC, cme, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F, dir, gd);
       scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
       const int sl = slot(EC, nl);
 #pragma unroll
@@ -476,7 +487,9 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
         const T* cp = cellp(lc[0], lc[1], lc[2]);
         const T* cm = cellp(ll[0], ll[1], ll[2]);
         T F[NF];
-        face_flux_sep(EC, cm, cp, has_m, true, lc, rowp(E, E, 0)[BOFF], F);
+        T gd = T(0);
+        const bool dir = !has_m && bc_dirichlet<DIM>(m, E, 0, gc, gd);
+        face_flux_sep(EC, cm, cp, has_m, true, lc, rowp(E, E, 0)[BOFF], F, dir, gd);
         const int sl = slot(EC, lc);
 #pragma unroll
         for (int mf = 0; mf < NF; ++mf) flux_at(EC, mf, sl) = F[mf];

@@ -159,6 +159,14 @@ struct flsp_handle {
   int* nb_counts = nullptr;   // their device counts
   bool nb_use[3] = {false, false, false};   // lists in force for the launches
   std::map<unsigned long long, GraphEntry> graphs;
+  unsigned long long gen = 0;     // bumped whenever captured graphs go stale
+  // boundary conditions: id of every domain-boundary face (empty: all 0),
+  // Dirichlet value per id, and the per-face values on the device
+  std::vector<int32_t> bid;
+  std::map<int, double> dirichlet;
+  double* bc_dev = nullptr;
+  long long nbf = 0;
+  bool batch_member = false;      // owned by a batch (no Dirichlet conditions)
   // exported files (PVDCollector: time and VTU name of every export)
   std::vector<std::pair<double, std::string>> pvd;
   // last curvature estimate (host DoF order, FP64) and the time it belongs to
@@ -207,6 +215,33 @@ void clear_graphs(flsp_handle* h) {
   for (auto& kv : h->graphs)
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   h->graphs.clear();
+  h->gen++;
+}
+
+// per-face Dirichlet values from the face ids and the conditions (NaN: none)
+int rebuild_bc(flsp_handle* h) {
+  std::vector<double> v((size_t)h->nbf, std::nan(""));
+  bool any = false;
+  for (long long k = 0; k < h->nbf; ++k) {
+    const int id = h->bid.empty() ? 0 : h->bid[k];
+    if (id <= 0) continue;
+    auto it = h->dirichlet.find(id);
+    if (it == h->dirichlet.end()) continue;
+    v[k] = it->second;
+    any = true;
+  }
+  CU(cudaSetDevice(h->dev));
+  CU(cudaStreamSynchronize(h->stream));
+  if (any) {
+    if (!h->bc_dev && cudaMalloc(&h->bc_dev, sizeof(double) * (size_t)h->nbf) != cudaSuccess) {
+      h->bc_dev = nullptr;
+      return fail(FLSP_ERR_OOM, "boundary values allocation failed");
+    }
+    CU(cudaMemcpy(h->bc_dev, v.data(), sizeof(double) * (size_t)h->nbf, cudaMemcpyHostToDevice));
+  }
+  h->m.bc_face = any ? h->bc_dev : nullptr;
+  clear_graphs(h);
+  return FLSP_OK;
 }
 
 int ensure_partial(flsp_handle* h, int n) {
@@ -839,6 +874,17 @@ int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts, flsp_handl
       return cleanup_fail(fail(FLSP_ERR_OOM, "allocation failed"));
     cudaMemcpy(h->perm, mesh->host_cell_order, sizeof(int64_t) * ncell, cudaMemcpyHostToDevice);
   }
+  for (int d = 0; d < h->dim; ++d) {
+    long long side = 1;
+    for (int e = 0; e < h->dim; ++e)
+      if (e != d) side *= h->m.n[e];
+    h->nbf += 2 * side;
+  }
+  if (mesh->boundary_ids) {
+    h->bid.assign(mesh->boundary_ids, mesh->boundary_ids + h->nbf);
+    for (int32_t id : h->bid)
+      if (id < 0) return cleanup_fail(fail(FLSP_ERR_BAD_MESH, "negative boundary id"));
+  }
   std::memset(&h->vel, 0, sizeof(h->vel));
   std::memset(&h->vel_dev, 0, sizeof(h->vel_dev));
   {
@@ -873,6 +919,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->clk_host) cudaFreeHost(h->clk_host);
   if (h->perm) cudaFree(h->perm);
   if (h->curv) cudaFree(h->curv);
+  if (h->bc_dev) cudaFree(h->bc_dev);
   if (h->stage64) cudaFree(h->stage64);
   if (h->partial) cudaFree(h->partial);
   if (h->red_out) cudaFree(h->red_out);
@@ -1046,6 +1093,31 @@ int flsp_get_time(const flsp_handle* hc, double* t) {
   CU(cudaSetDevice(h->dev));
   ST(sync_clock(h));
   *t = h->clk_host->t;
+  return FLSP_OK;
+}
+
+int flsp_set_dirichlet(flsp_handle* h, int boundary_id, double value) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  if (boundary_id <= 0)
+    return fail(FLSP_ERR_BAD_ARG, "Dirichlet conditions need a boundary id > 0 (id 0 never takes one)");
+  if (!std::isfinite(value)) return fail(FLSP_ERR_BAD_ARG, "non-finite boundary value");
+  if (h->batch_member) return fail(FLSP_ERR_UNSUPPORTED, "Dirichlet conditions on a batch member");
+  h->dirichlet[boundary_id] = value;
+  return rebuild_bc(h);
+}
+
+int flsp_clear_dirichlet(flsp_handle* h) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  h->dirichlet.clear();
+  return rebuild_bc(h);
+}
+
+int flsp_get_step_count(const flsp_handle* hc, int64_t* n_substeps) {
+  flsp_handle* h = const_cast<flsp_handle*>(hc);
+  if (!h || !n_substeps) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  CU(cudaSetDevice(h->dev));
+  ST(sync_clock(h));
+  *n_substeps = h->clk_host->n_substeps;
   return FLSP_OK;
 }
 
@@ -1834,6 +1906,7 @@ int flsp_batch_create(int n, const flsp_mesh_desc* meshes, const flsp_dg_opts* o
       flsp_batch_destroy(b);
       return st;
     }
+    h->batch_member = true;
     b->h.push_back(h);
   }
   if (cudaSetDevice(b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -2096,7 +2169,10 @@ int group_run(flsp_group* g, const GroupMode& gm, int n_periods) {
       const unsigned char* b = (const unsigned char*)p;
       for (size_t i = 0; i < nb; ++i) { key ^= b[i]; key *= 1099511628211ull; }
     };
-    for (flsp_handle* h : g->h) mix(&h->cur, sizeof(h->cur));
+    for (flsp_handle* h : g->h) {
+      mix(&h->cur, sizeof(h->cur));
+      mix(&h->gen, sizeof(h->gen));   // a member's velocity or conditions changed
+    }
     mix(&gm.freq, sizeof(gm.freq));
     if (gm.ro) mix(gm.ro, sizeof(*gm.ro));
     if (gm.net) {

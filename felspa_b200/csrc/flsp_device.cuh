@@ -164,7 +164,40 @@ struct MeshArgs {
   // at or past *n_tiles have no tile (null: block b serves tile b)
   const int* tiles;
   const int* n_tiles;
+  // Dirichlet value of every domain-boundary face (NaN: none, the face
+  // keeps the zero-Neumann interior trace); null: no Dirichlet face.
+  // Faces side by side (x-, x+, y-, y+, z-, z+), each side's faces
+  // lexicographic in the other axes (lower axis fastest).
+  const double* bc_face;
 };
+
+// boundary faces on the sides before side (E, S) and within it
+template <int DIM>
+__host__ __device__ __forceinline__ long long bc_side_faces(const MeshArgs& m, int E) {
+  const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  return (long long)m.n[t0] * (DIM > 2 ? m.n[t1] : 1);
+}
+
+// Dirichlet value g on the domain-boundary face on side S (0: lower, 1:
+// upper) of axis E of the cell at lattice position c, when the face's
+// boundary id carries one: the exterior trace there is the constant g, a
+// face polynomial with g in the constant mode and zeros elsewhere
+// (inflow of advection.implement.h:719-741; LDG left / right gradients,
+// ldg.cc:551-620 and :686-740).  False: zero-Neumann (interior trace).
+template <int DIM, typename T>
+__device__ __forceinline__ bool bc_dirichlet(const MeshArgs& m, int E, int S, const int* c, T& g) {
+  if (!m.bc_face) return false;
+  long long off = 0;
+#pragma unroll
+  for (int e = 0; e < DIM; ++e)
+    if (e < E) off += 2 * bc_side_faces<DIM>(m, e);
+  const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  off += S * bc_side_faces<DIM>(m, E) + c[t0] + (DIM > 2 ? (long long)m.n[t0] * c[t1] : 0);
+  const double v = m.bc_face[off];
+  if (v != v) return false;   // NaN: no Dirichlet value on this face
+  g = T(v);
+  return true;
+}
 
 // separable velocity: vtab[((k*3 + axis) * nmax + i) * npt + j]
 // j < NQ: Gauss (p+2) point j of cell i; j == NQ: xi = 0; j == NQ+1: xi = 1

@@ -123,6 +123,9 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
       nl[e] -= 1;
       nu[e] += 1;
       const bool has_lo = gg[e] > 0, has_hi = gg[e] + 1 < m.n[e];
+      T glo = T(0), ghi = T(0);
+      const bool dlo = !has_lo && bc_dirichlet<DIM>(m, e, 0, gg, glo);
+      const bool dhi = !has_hi && bc_dirichlet<DIM>(m, e, 1, gg, ghi);
       const T* cL = box + (size_t)box_index(m, DIM, nl[0], nl[1], nl[2]) * NM;
       const T* cU = box + (size_t)box_index(m, DIM, nu[0], nu[1], nu[2]) * NM;
       T gl[NM], gr[NM];
@@ -144,8 +147,10 @@ __global__ void __launch_bounds__(256) hj_kernel(const HJArgs<T> a) {
           if (has_lo) tnl += tb.L1[b] * cL[base + b * st[e]];
           if (has_hi) tnu += tb.L0[b] * cU[base + b * st[e]];
         }
-        if (!has_lo) tnl = tlo;
-        if (!has_hi) tnu = tup;
+        // domain boundary: the Dirichlet value of the face (constant mode
+        // only) where it carries one, else the interior trace
+        if (!has_lo) tnl = dlo ? (li == 0 ? glo : T(0)) : tlo;
+        if (!has_hi) tnu = dhi ? (li == 0 ? ghi : T(0)) : tup;
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa) {
           T bs = T(0);

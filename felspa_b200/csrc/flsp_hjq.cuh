@@ -146,6 +146,9 @@ __device__ __forceinline__ void hjq_tile(const HJArgs<T>& a, int slot) {
       ll[d] -= 1;
       lu[d] += 1;
       const bool has_lo = g[d] > 0, has_hi = g[d] + 1 < m.n[d];
+      T glo = T(0), ghi = T(0);
+      const bool dlo = !has_lo && bc_dirichlet<DIM>(m, d, 0, g, glo);
+      const bool dhi = !has_hi && bc_dirichlet<DIM>(m, d, 1, g, ghi);
       const T* cL = box + (size_t)box_index(m, DIM, ll[0], ll[1], ll[2]) * NM;
       const T* cU = box + (size_t)box_index(m, DIM, lu[0], lu[1], lu[2]) * NM;
       T jlo[NF], jhi[NF];
@@ -162,8 +165,10 @@ __device__ __forceinline__ void hjq_tile(const HJArgs<T>& a, int slot) {
           if (has_lo) tnl += tb.L1[b] * cL[base + b * st[d]];
           if (has_hi) tnu += tb.L0[b] * cU[base + b * st[d]];
         }
-        jlo[mf] = has_lo ? tlo - tnl : T(0);
-        jhi[mf] = has_hi ? tnu - tup : T(0);
+        // domain boundary: jump to the Dirichlet value of the face (constant
+        // mode only) where it carries one, else zero (interior trace)
+        jlo[mf] = has_lo ? tlo - tnl : (dlo ? tlo - (mf == 0 ? glo : T(0)) : T(0));
+        jhi[mf] = has_hi ? tnu - tup : (dhi ? (mf == 0 ? ghi : T(0)) - tup : T(0));
       }
 #pragma unroll
       for (int side = 0; side < 2; ++side) {

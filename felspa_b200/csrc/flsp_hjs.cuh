@@ -104,7 +104,30 @@ __device__ __forceinline__ void hjs_face(const MeshArgs& m, const CellP& cellp, 
   ll[E] = f - 1;
   const bool inside = o[E] + f - 1 >= 0 && o[E] + f < m.n[E];
   T J[NF];
-  if (inside) {
+  // a domain-boundary face with a Dirichlet value: the missing side's trace
+  // is that constant (LDG left / right boundary terms, ldg.cc:551-620,
+  // :686-740); without one the jump is zero (interior trace)
+  T gd = T(0);
+  bool dir = false;
+  if (!inside && (o[E] + f == 0 || o[E] + f == m.n[E])) {
+    int gcell[3] = {o[0] + lu[0], o[1] + lu[1], o[2] + lu[2]};
+    gcell[E] = o[E] + f == 0 ? 0 : m.n[E] - 1;
+    dir = bc_dirichlet<DIM>(m, E, o[E] + f == 0 ? 0 : 1, gcell, gd);
+  }
+  if (dir) {
+    const bool lower = o[E] + f == 0;   // the domain's lower side: the cell is above the face
+    const T* cc = lower ? cellp(lu[0], lu[1], lu[2]) : cellp(ll[0], ll[1], ll[2]);
+#pragma unroll
+    for (int mf = 0; mf < NF; ++mf) {
+      const int m0 = mf % N1, m1 = mf / N1;
+      const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
+      T tr = T(0);
+#pragma unroll
+      for (int b = 0; b < N1; ++b) tr += (lower ? tb.L0[b] : tb.L1[b]) * cc[base + b * st[E]];
+      const T ghost = mf == 0 ? gd : T(0);
+      J[mf] = lower ? tr - ghost : ghost - tr;
+    }
+  } else if (inside) {
     const T* cu = cellp(lu[0], lu[1], lu[2]);
     const T* cd = cellp(ll[0], ll[1], ll[2]);
 #pragma unroll

@@ -50,17 +50,39 @@ def dealii_hypercube_order(dim, n_subdiv, n_refine):
     return np.asarray(order, dtype=np.int64)
 
 
+def boundary_face_count(dim, n):
+    """domain-boundary faces of an n[0] x .. box: 2 sum_d prod_{e != d} n[e]"""
+    return int(sum(2 * np.prod([n[e] for e in range(dim) if e != d]) for d in range(dim)))
+
+
+def colorized_boundary_ids(dim, n):
+    """boundary ids of deal.II's colorized hyper_rectangle: side s (x-, x+,
+    y-, y+, z-, z+) has id s, in flsp_mesh_desc's face order"""
+    ids = []
+    for d in range(dim):
+        side = int(np.prod([n[e] for e in range(dim) if e != d]))
+        ids += [2 * d] * side + [2 * d + 1] * side
+    return np.asarray(ids, dtype=np.int32)
+
+
 class Mesh:
     """Uniform Cartesian mesh of a box (the part of dealii::Triangulation the
-    hot path needs): cells per axis, corners, optional host cell order."""
+    hot path needs): cells per axis, corners, optional host cell order and
+    boundary ids of the boundary faces (flsp_mesh_desc's order)."""
 
-    def __init__(self, dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=None):
+    def __init__(self, dim, n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), host_cell_order=None,
+                 boundary_ids=None):
         self.dim = dim
         self.n = tuple(int(v) for v in n[:dim])
         self.lo = tuple(float(v) for v in lo[:dim])
         self.hi = tuple(float(v) for v in hi[:dim])
         self.host_cell_order = None if host_cell_order is None else np.ascontiguousarray(
             host_cell_order, dtype=np.int64)
+        self.boundary_ids = None
+        if boundary_ids is not None:
+            self.boundary_ids = np.ascontiguousarray(boundary_ids, dtype=np.int32)
+            if self.boundary_ids.size != boundary_face_count(dim, self.n):
+                raise ValueError("boundary_ids must hold one id per boundary face")
 
     @property
     def n_cells(self):
@@ -75,7 +97,10 @@ class Mesh:
         order = None
         if self.host_cell_order is not None:
             order = self.host_cell_order.ctypes.data_as(C.POINTER(C.c_int64))
-        return abi.mesh_desc(self.dim, self.n, self.lo, self.hi, order)
+        bids = None
+        if self.boundary_ids is not None:
+            bids = self.boundary_ids.ctypes.data_as(C.POINTER(C.c_int32))
+        return abi.mesh_desc(self.dim, self.n, self.lo, self.hi, order, bids)
 
 
 # ----------------------------------------------------------------------
@@ -167,11 +192,24 @@ class Problem:
         check(load().flsp_get_time(self.h, C.byref(t)))
         return t.value
 
+    def get_step_count(self):
+        """advection substeps executed so far"""
+        n = C.c_int64(0)
+        check(load().flsp_get_step_count(self.h, C.byref(n)))
+        return n.value
+
     def set_time(self, t):
         check(load().flsp_set_time(self.h, float(t)))
 
     def snapshot(self):
         check(load().flsp_snapshot(self.h))
+
+    def set_dirichlet(self, boundary_id, value):
+        """a Dirichlet condition of constant value on the faces of id boundary_id (> 0)"""
+        check(load().flsp_set_dirichlet(self.h, int(boundary_id), float(value)))
+
+    def clear_dirichlet(self):
+        check(load().flsp_clear_dirichlet(self.h))
 
     def sync(self):
         check(load().flsp_sync(self.h))
@@ -301,6 +339,12 @@ class AdvectSimulator:
 
     def get_solution_vector(self):
         return self.problem.get_state()
+
+    def append_boundary_condition(self, boundary_id, dirichlet_value):
+        """append_boundary_condition(bc) for a Dirichlet condition of
+        constant value on the faces of id boundary_id (> 0); the level set's
+        advection and reinitialisation share it (level_set.implement.h:384-392)"""
+        self.problem.set_dirichlet(boundary_id, dirichlet_value)
 
     def export_solutions(self, path, label=None):
         """SimulatorBase::export_solutions(path): the solution's cell-corner

@@ -35,7 +35,10 @@ PROTOTYPES = {
     "flsp_get_state": (C.c_int, [_vp, _dp, C.c_int64]),
     "flsp_set_time": (C.c_int, [_vp, C.c_double]),
     "flsp_get_time": (C.c_int, [_vp, _dp]),
+    "flsp_get_step_count": (C.c_int, [_vp, _i64p]),
     "flsp_snapshot": (C.c_int, [_vp]),
+    "flsp_set_dirichlet": (C.c_int, [_vp, C.c_int, C.c_double]),
+    "flsp_clear_dirichlet": (C.c_int, [_vp]),
     "flsp_advect_rhs": (C.c_int, [_vp, C.c_double, _dp, C.c_int64]),
     "flsp_advance": (C.c_int, [_vp, C.c_double, C.c_int, _dp]),
     "flsp_advance_steps": (C.c_int, [_vp, C.c_int, C.c_double]),

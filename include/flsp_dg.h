@@ -91,6 +91,13 @@ typedef struct flsp_mesh_desc {
      cell order of a refined deal.II hyper cube).  NULL = lexicographic.
      Must be a permutation of 0..n_cells-1 (checked at create).          */
   const int64_t* host_cell_order;
+  /* Optional boundary ids (deal.II types::boundary_id, >= 0) of the
+     domain-boundary faces: side by side in the order x-, x+, y-, y+
+     (, z-, z+), each side's faces lexicographic in the other axes (lower
+     axis fastest), 2 * sum_d prod_{e != d} n[e] entries.  NULL = every
+     boundary face has id 0, as deal.II's hyper_cube without colorize
+     (with colorize the sides carry ids 0..2 dim-1 in this order).       */
+  const int32_t* boundary_ids;
 } flsp_mesh_desc;
 
 typedef struct flsp_dg_opts {
@@ -248,6 +255,20 @@ int flsp_get_time(const flsp_handle* h, double* t);
 int flsp_get_step_count(const flsp_handle* h, int64_t* n_substeps);
 /* save the current state as the comparison snapshot of the reductions */
 int flsp_snapshot(flsp_handle* h);
+
+/* boundary conditions ------------------------------------------------ */
+/* LevelSetSurface::append_boundary_condition (level_set.implement.h:
+   384-392) with a Dirichlet condition of constant value: on every
+   boundary face of id `boundary_id` (> 0; id 0 never takes a condition,
+   advection.implement.h:723, ldg.cc:588) the advection inflow
+   (advection.implement.h:719-741) and the reinitialisation's LDG left /
+   right gradients (ldg.cc:551-620, :686-740) take `value` as the exterior
+   trace; the other boundary faces keep the zero-Neumann interior trace.
+   Setting an id again replaces its value.  Not supported for members of
+   a batch (flsp_batch_run_steps fails).                                */
+int flsp_set_dirichlet(flsp_handle* h, int boundary_id, double value);
+/* remove every Dirichlet condition                                    */
+int flsp_clear_dirichlet(flsp_handle* h);
 
 /* advection ---------------------------------------------------------- */
 /* phidot = M^-1 R(phi, t) of the current state, in host DoF order */

@@ -41,12 +41,14 @@ struct Mesh {
   int n[3] = {1, 1, 1};
   double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
   std::vector<int64_t> host_cell_order;   // empty = lexicographic
+  std::vector<int32_t> boundary_ids;      // per boundary face (flsp_mesh_desc order); empty = all 0
 
   flsp_mesh_desc desc() const {
     flsp_mesh_desc d;
     d.dim = dim;
     for (int i = 0; i < 3; ++i) { d.n[i] = n[i]; d.lo[i] = lo[i]; d.hi[i] = hi[i]; }
     d.host_cell_order = host_cell_order.empty() ? nullptr : host_cell_order.data();
+    d.boundary_ids = boundary_ids.empty() ? nullptr : boundary_ids.data();
     return d;
   }
 };
@@ -106,6 +108,12 @@ class AdvectSimulator {
     std::vector<double> out(problem_.n_dofs());
     check(flsp_get_state(h(), out.data(), (int64_t)out.size()), "flsp_get_state");
     return out;
+  }
+  // append_boundary_condition(bc) for a Dirichlet condition of constant
+  // value on the boundary faces of id boundary_id (> 0); a level set's
+  // advection and reinitialisation share it (level_set.implement.h:384-392)
+  void append_boundary_condition(int boundary_id, double dirichlet_value) {
+    check(flsp_set_dirichlet(h(), boundary_id, dirichlet_value), "flsp_set_dirichlet");
   }
   void set_solution_vector(const std::vector<double>& v) {
     check(flsp_set_state(h(), v.data(), (int64_t)v.size()), "flsp_set_state");

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -130,6 +131,38 @@ struct orc_problem {
     int I[3];
     ijk(c, I);
     for (int d = 0; d < 3; ++d) X[d] = d < dim ? lo[d] + I[d] * h[d] : 0.0;
+  }
+  // boundary conditions: id of every boundary face (empty: all 0, deal.II's
+  // default), the Dirichlet value of each id
+  std::vector<int> bid;
+  std::map<int, double> dirichlet;
+  long side_faces(int ax) const {
+    long s = 1;
+    for (int e = 0; e < dim; ++e)
+      if (e != ax) s *= n[e];
+    return s;
+  }
+  // Dirichlet value on the boundary face f = 2*axis + side of cell c, NaN
+  // if none (id 0 or no condition for its id: zero-Neumann).  Faces side by
+  // side (x-, x+, y-, y+, z-, z+), each side lexicographic in the other axes.
+  double bc_value(long c, int f) const {
+    if (dirichlet.empty()) return std::nan("");
+    int I[3];
+    ijk(c, I);
+    const int ax = f / 2, s = f % 2;
+    long k = 0;
+    for (int e = 0; e < ax; ++e) k += 2 * side_faces(e);
+    k += s * side_faces(ax);
+    long in_side = 0, stride = 1;
+    for (int e = 0; e < dim; ++e) {
+      if (e == ax) continue;
+      in_side += stride * I[e];
+      stride *= n[e];
+    }
+    const int id = bid.empty() ? 0 : bid[k + in_side];
+    if (id <= 0) return std::nan("");
+    auto it = dirichlet.find(id);
+    return it == dirichlet.end() ? std::nan("") : it->second;
   }
 };
 
@@ -398,6 +431,16 @@ void orc_legendre(int n, double x, double* v, double* d, double* dd) {
   legendre(n, x, v, d, dd);
 }
 
+int orc_set_dirichlet(orc_problem* pr, int boundary_id, double value) {
+  if (!pr || boundary_id <= 0 || !std::isfinite(value)) return FLSP_ERR_BAD_ARG;
+  pr->dirichlet[boundary_id] = value;
+  return FLSP_OK;
+}
+
+void orc_clear_dirichlet(orc_problem* pr) {
+  if (pr) pr->dirichlet.clear();
+}
+
 int orc_create(const flsp_mesh_desc* mesh, int degree, int basis,
                orc_problem** out) {
   if (!mesh || !out || mesh->dim < 2 || mesh->dim > 3 || degree < 0 || degree > 4)
@@ -422,6 +465,11 @@ int orc_create(const flsp_mesh_desc* mesh, int degree, int basis,
     } else {
       pr->h[d] = 1.0;
     }
+  }
+  if (mesh->boundary_ids) {
+    long nbf = 0;
+    for (int e = 0; e < pr->dim; ++e) nbf += 2 * pr->side_faces(e);
+    pr->bid.assign(mesh->boundary_ids, mesh->boundary_ids + nbf);
   }
   // cell diameter = longest diagonal (mesh/src/mesh.implement.h:60-71)
   pr->diam = std::sqrt(d2);
@@ -555,18 +603,20 @@ int orc_advect_rhs(orc_problem* pr, const double* phi, double t, double* phidot)
     for (int f = 0; f < 2 * dim; ++f) {
       int ax = f / 2, s = f % 2;
       long nbc = pr->neighbor(c, f);
+      const double gbc = nbc < 0 ? pr->bc_value(c, f) : std::nan("");
       const FaceQuad& fq = pr->fc[f];
       const std::vector<double>& vin = pr->vfc[f];
       const std::vector<double>& vex = pr->vfc[f ^ 1];
       double area = pr->vol / pr->h[ax];
       for (int q = 0; q < fq.np; ++q) {
         double pin = eval_at(pc, vin, nb, fq.np, q);
-        double pex = nbc >= 0 ? eval_at(phi + nbc * nb, vex, nb, fq.np, q) : pin;
+        // boundary: the face's Dirichlet value, or without one zero-Neumann
+        // (interior trace) (:719-741)
+        double pex = nbc >= 0 ? eval_at(phi + nbc * nb, vex, nb, fq.np, q) : (std::isnan(gbc) ? pin : gbc);
         double x[3], u[3];
         for (int d = 0; d < 3; ++d) x[d] = X0[d] + pr->h[d] * fq.xi[q][d];
         velocity(pr, x, t, u);
         double vn = s ? u[ax] : -u[ax];
-        // boundary without a Dirichlet BC: zero-Neumann -> interior trace
         double up = vn > 0.0 ? pin : pex;
         double jxw = fq.w[q] * area;
         for (int i = 0; i < nb; ++i) R[i] -= vn * vin[(size_t)i * fq.np + q] * up * jxw;
@@ -677,16 +727,19 @@ int orc_hj_gradients(orc_problem* pr, const double* phi, double* gl, double* gr)
       for (int s = 0; s < 2; ++s) {
         int f = 2 * e + s;
         long nbc = pr->neighbor(c, f);
+        const double gbc = nbc < 0 ? pr->bc_value(c, f) : std::nan("");
         const FaceQuad& fq = pr->fl[f];
         const std::vector<double>& vin = pr->vfl[f];
         const std::vector<double>& vex = pr->vfl[f ^ 1];
         double nrm = s ? 1.0 : -1.0;
         for (int q = 0; q < fq.np; ++q) {
           double pin = eval_at(pc, vin, nb, fq.np, q);
-          double pex = nbc >= 0 ? eval_at(phi + nbc * nb, vex, nb, fq.np, q) : pin;
+          double pex = nbc >= 0 ? eval_at(phi + nbc * nb, vex, nb, fq.np, q) : (std::isnan(gbc) ? pin : gbc);
           double jxw = fq.w[q] * area;
           // left flux: trace of the lower cell; right: of the upper cell;
-          // boundary (no Dirichlet BC): interior trace
+          // boundary: the face's Dirichlet value on the side the flux takes
+          // (left: lower faces, n_d < 0, ldg.cc:574-601; right: upper faces,
+          // n_d >= 0, :711-735), else the interior trace
           double hl = (nrm < 0.0) ? pex : pin;
           double hr = (nrm < 0.0) ? pin : pex;
           for (int i = 0; i < nb; ++i) {

@@ -45,6 +45,11 @@ typedef struct orc_clock {
 int orc_create(const flsp_mesh_desc* mesh, int degree, int basis,
                orc_problem** out);
 void orc_destroy(orc_problem* pr);
+/* LevelSetSurface::append_boundary_condition with a Dirichlet condition of
+   constant value on the boundary faces of id boundary_id (> 0), as
+   flsp_set_dirichlet                                                  */
+int orc_set_dirichlet(orc_problem* pr, int boundary_id, double value);
+void orc_clear_dirichlet(orc_problem* pr);
 long orc_n_dofs(const orc_problem* pr);
 int orc_dofs_per_cell(const orc_problem* pr);
 void orc_set_threads(int n);

@@ -37,6 +37,8 @@ def lib():
         L = C.CDLL(_LIB_PATH)
         L.orc_create.argtypes = [C.POINTER(abi.MeshDesc), C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_set_dirichlet.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.orc_clear_dirichlet.argtypes = [C.c_void_p]
         L.orc_n_dofs.argtypes = [C.c_void_p]
         L.orc_n_dofs.restype = C.c_long
         L.orc_dofs_per_cell.argtypes = [C.c_void_p]
@@ -108,11 +110,15 @@ def eval_ic(ic, dim, x):
 class Problem:
     """One level-set problem on the CPU: mesh, DG space, velocity."""
 
-    def __init__(self, dim, n, degree, basis=abi.BASIS_Q, lo=(0, 0, 0), hi=(1, 1, 1)):
+    def __init__(self, dim, n, degree, basis=abi.BASIS_Q, lo=(0, 0, 0), hi=(1, 1, 1), boundary_ids=None):
         self.dim = dim
         self.degree = degree
         self.basis = basis
-        self.mesh = abi.mesh_desc(dim, n, lo, hi)
+        self._bids = None
+        if boundary_ids is not None:
+            self._bids = np.ascontiguousarray(boundary_ids, dtype=np.int32)
+        self.mesh = abi.mesh_desc(dim, n, lo, hi, None,
+                                  self._bids.ctypes.data_as(C.POINTER(C.c_int32)) if self._bids is not None else None)
         h = C.c_void_p()
         _check(lib().orc_create(C.byref(self.mesh), degree, basis, C.byref(h)), "create")
         self.h = h
@@ -125,6 +131,12 @@ class Problem:
         if getattr(self, "h", None) and _lib is not None:
             _lib.orc_destroy(self.h)
             self.h = None
+
+    def set_dirichlet(self, boundary_id, value):
+        _check(lib().orc_set_dirichlet(self.h, int(boundary_id), float(value)), "set_dirichlet")
+
+    def clear_dirichlet(self):
+        lib().orc_clear_dirichlet(self.h)
 
     def set_velocity(self, field):
         self.velocity = field

@@ -65,6 +65,50 @@ def compute(name, spec):
     return out
 
 
+def revolution_cases():
+    """The Zalesak slotted disk of the 2D configuration: 128^2 cells of the
+    unit square, degree 1 (Q and P), counter-clockwise rotation
+    u = 2 pi (0.5 - y, x - 0.5), one revolution (T = 1), SSP-RK3 at CFL
+    0.1, a fixed 5-pseudo-step reinit over every cell each 10 substeps
+    (band 6 cells), without and with the reference test's LDG viscosity
+    1e-3 (tests/test_zalesak_disk.cc:252,256).
+    name -> (basis, viscosity, keep the full final state)"""
+    return {
+        "zalesak128_q1_nu0": (abi.BASIS_Q, 0.0, False),
+        "zalesak128_p1_nu0": (abi.BASIS_P, 0.0, False),
+        "zalesak128_q1_nu1e-3": (abi.BASIS_Q, 1e-3, True),
+        "zalesak128_p1_nu1e-3": (abi.BASIS_P, 1e-3, True),
+    }
+
+
+def revolution_opts(viscosity):
+    ro = abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=5, band_width_coeff=6.0,
+                                 viscosity=viscosity)
+    return abi.default_ls_opts(reinit_frequency=10, reinit=ro)
+
+
+def compute_revolution(basis, viscosity, keep_state):
+    import time
+    ic = F.zalesak_disk()
+    pr = O.Problem(2, (128, 128), 1, basis)
+    pr.set_velocity(F.ccw_rotation())
+    phi = pr.project(ic)
+    area0 = pr.reduce(abi.RED_MASS, phi)
+    t0 = time.perf_counter()
+    pr.ls_advance(phi, 1.0, revolution_opts(viscosity), single_step=False, rk_order=3, cfl_max=0.1)
+    cpu_s = time.perf_counter() - t0
+    nb = pr.nb
+    out = {"t_end": np.array(pr.clock.t), "n_substeps": np.array(pr.clock.n_substeps),
+           "area0": np.array(area0), "area1": np.array(pr.reduce(abi.RED_MASS, phi)),
+           "l1_ic": np.array(pr.reduce(abi.RED_L1_INTERFACE_IC, phi, ic=ic)),
+           "max_abs": np.array(np.abs(phi).max()),
+           "cell_means": phi.reshape(-1, nb)[:, 0].copy(),
+           "cpu_s": np.array(cpu_s), "threads": np.array(os.cpu_count() or 1)}
+    if keep_state:
+        out["result"] = phi
+    return out
+
+
 def main(names=None):
     for name, spec in cases().items():
         if names and name not in names:
@@ -72,6 +116,13 @@ def main(names=None):
         out = compute(name, spec)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(name, {k: v.shape for k, v in out.items()})
+    # full revolutions take minutes each: only when named
+    for name, spec in revolution_cases().items():
+        if not names or name not in names:
+            continue
+        out = compute_revolution(*spec)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, {k: (v.shape if v.ndim else float(v)) for k, v in out.items()}, flush=True)
 
 
 if __name__ == "__main__":

@@ -256,3 +256,104 @@ def test_golden(oracle, name):
     for k in ref.files:
         scale = max(np.max(np.abs(ref[k])), 1e-300)
         assert np.max(np.abs(out[k] - ref[k])) <= 1e-13 * scale, k
+
+
+# ----------------------------------------------------------------------
+# Dirichlet boundary conditions
+# ----------------------------------------------------------------------
+def dof_modes(dim, p, basis):
+    """(a, b, c) Legendre degrees of the in-cell DoFs in deal.II order:
+    FE_DGQLegendre lexicographic, FE_DGP PolynomialSpace (c, b outer)"""
+    cz = p if dim == 3 else 0
+    out = []
+    for c in range(cz + 1):
+        for b in range(p + 1):
+            for a in range(p + 1):
+                if basis == abi.BASIS_P and a + b + c > p:
+                    continue
+                out.append((a, b, c))
+    return out
+
+
+def side_ids(dim, n, per_side):
+    """boundary ids in flsp_mesh_desc's face order from one id per side"""
+    from felspa_b200.level_set import colorized_boundary_ids
+    col = colorized_boundary_ids(dim, n)
+    return np.asarray([per_side[s] for s in col], dtype=np.int32)
+
+
+@pytest.mark.parametrize("p,basis", [(1, abi.BASIS_Q), (2, abi.BASIS_P), (3, abi.BASIS_Q)])
+def test_dirichlet_inflow_rhs_known_answer(oracle, p, basis):
+    """phi = 0, u = (1, 0), Dirichlet g on the inflow side x-: the inflow
+    flux -v_n psi_i g (advection.implement.h:719-741) is the only term, so
+    phidot of the cells at x = 0 is g L_a(0) / h on the modes constant in
+    y, L_a(0) = sqrt(2a+1) (-1)^a, and zero everywhere else; a Dirichlet
+    value on the outflow side x+ changes nothing."""
+    n, g = 8, 0.75
+    h = 1.0 / n
+    pr = oracle.Problem(2, (n, n), p, basis, boundary_ids=side_ids(2, (n, n), [7, 9, 0, 0]))
+    pr.set_velocity(F.constant((1.0, 0.0)))
+    pr.set_dirichlet(7, g)
+    pr.set_dirichlet(9, -3.0)
+    rhs = pr.advect_rhs(np.zeros(pr.n_dofs), 0.0).reshape(n, n, -1)   # [iy][ix][dof]
+    want = np.zeros_like(rhs)
+    for k, (a, b, c) in enumerate(dof_modes(2, p, basis)):
+        if b == 0:
+            want[:, 0, k] = g * math.sqrt(2 * a + 1) * (-1) ** a / h
+    assert np.max(np.abs(rhs - want)) < 1e-12 * max(1.0, np.abs(want).max())
+
+
+def test_dirichlet_ldg_gradients_known_answer(oracle):
+    """phi = 0 with Dirichlet values on x- (g0) and x+ (g1): the left
+    gradient takes the value on faces with n_x < 0 (ldg.cc:574-601), the
+    right gradient on faces with n_x >= 0 (:711-735): left_x = -g0 L_a(0)/h
+    at x = 0, right_x = g1 L_a(1)/h at x = 1, every other entry zero."""
+    n, p, g0, g1 = 6, 2, 0.4, -1.1
+    h = 1.0 / n
+    pr = oracle.Problem(2, (n, n), p, abi.BASIS_Q, boundary_ids=side_ids(2, (n, n), [1, 2, 0, 0]))
+    pr.set_velocity(F.constant((1.0, 0.0)))
+    pr.set_dirichlet(1, g0)
+    pr.set_dirichlet(2, g1)
+    gl, gr = pr.hj_gradients(np.zeros(pr.n_dofs))
+    wl, wr = np.zeros((2, n, n, 9)), np.zeros((2, n, n, 9))
+    for k, (a, b, c) in enumerate(dof_modes(2, p, abi.BASIS_Q)):
+        if b == 0:
+            wl[0, :, 0, k] = -g0 * math.sqrt(2 * a + 1) * (-1) ** a / h
+            wr[0, :, n - 1, k] = g1 * math.sqrt(2 * a + 1) / h
+    assert np.max(np.abs(gl.reshape(2, n, n, 9) - wl)) < 1e-12 / h
+    assert np.max(np.abs(gr.reshape(2, n, n, 9) - wr)) < 1e-12 / h
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_dirichlet_free_stream(oracle, dim):
+    """a constant field with the same constant as Dirichlet value on every
+    face stays constant under any velocity: RHS and LDG gradients vanish"""
+    n = (6,) * dim
+    pr = oracle.Problem(dim, n, 2, abi.BASIS_Q, boundary_ids=side_ids(dim, n, [1] * (2 * dim)))
+    pr.set_velocity(F.constant((0.8, -0.6, 0.3)[:dim]))
+    pr.set_dirichlet(1, 0.35)
+    phi = np.zeros(pr.n_dofs)
+    phi[::pr.nb] = 0.35
+    assert np.max(np.abs(pr.advect_rhs(phi, 0.0))) < 1e-12
+    gl, gr = pr.hj_gradients(phi)
+    assert np.max(np.abs(gl)) < 1e-11 and np.max(np.abs(gr)) < 1e-11
+    # without the condition the inflow is zero-Neumann: still constant
+    pr.clear_dirichlet()
+    assert np.max(np.abs(pr.advect_rhs(phi, 0.0))) < 1e-12
+
+
+def test_dirichlet_id_zero_and_unset_ids_are_neumann(oracle):
+    """faces of id 0 never take a condition (advection.implement.h:723),
+    and ids without a condition stay zero-Neumann: setting conditions on
+    other ids leaves the RHS unchanged"""
+    n = (8, 8)
+    ic, vel = F.zalesak_disk(), F.ccw_rotation()
+    ref = oracle.Problem(2, n, 1, abi.BASIS_Q)
+    ref.set_velocity(vel)
+    phi = ref.project(ic)
+    pr = oracle.Problem(2, n, 1, abi.BASIS_Q, boundary_ids=side_ids(2, n, [0, 0, 4, 4]))
+    pr.set_velocity(vel)
+    pr.set_dirichlet(5, 1.0)
+    assert np.array_equal(pr.advect_rhs(phi, 0.1), ref.advect_rhs(phi, 0.1))
+    with pytest.raises(RuntimeError):
+        pr.set_dirichlet(0, 1.0)
