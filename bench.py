@@ -505,9 +505,10 @@ def zalesak_accuracy(device):
     from felspa_b200.zalesak import revolution
     out = {"what": "128^2 degree-1 slotted disk, one CCW revolution (T = 1), SSP-RK3 at CFL 0.1, fixed "
                    "5-pseudo-step reinit every 10 substeps over every cell; L1 interface error vs the initial "
-                   "shape, area change; LDG viscosity 0 (as the configuration) and 1e-3 (the reference test's)"}
+                   "shape, area change; LDG viscosity 0 (as the configuration), 6.28e-5 (the reference test's 1e-3 "
+                   "on its [-50,50]^2 domain with period 628, rescaled to the unit square with period 1) and 1e-3"}
     for basis, bname in ((abi.BASIS_Q, "q1"), (abi.BASIS_P, "p1")):
-        for nu, nname in ((0.0, "nu0"), (1e-3, "nu1e-3")):
+        for nu, nname in ((0.0, "nu0"), (6.28e-5, "nu6.28e-5"), (1e-3, "nu1e-3")):
             key = f"zalesak128_{bname}_{nname}"
             r64 = revolution(basis, nu, abi.FP64, device=device)
             r32 = revolution(basis, nu, abi.FP32, device=device)

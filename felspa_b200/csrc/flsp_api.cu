@@ -149,6 +149,7 @@ struct flsp_handle {
   int* lrn_cells = nullptr;   // band cells (ncell)
   int* lrn_count = nullptr;   // [0] band cells, [1] fallback cells
   int* lrn_count_host = nullptr;   // pinned mirror
+  unsigned long long* lrn_tot = nullptr;   // running totals: band cells, fallback cells
   void* lrn_save = nullptr;   // one state vector
   float* lrn_feat = nullptr;  // band patch features
   int64_t lrn_feat_cap = 0;
@@ -432,8 +433,9 @@ int ensure_band_buffers(flsp_handle* h) {
   return FLSP_OK;
 }
 
-// (buffers allocated beforehand by ensure_band_buffers)
-int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter) {
+// (buffers allocated beforehand by ensure_band_buffers); with a gate (a
+// device count), every tile list is emptied when the count is zero
+int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter, const int* gate = nullptr) {
   Ctx c = h->ctx();
   ST(launch_band_flags(c, h->buf[phi0], o->band_cells * h->m.min_diam, h->nb_flags));
   const int margin = 2;
@@ -451,6 +453,7 @@ int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter
                          h->nb_counts + kNbWeno));
     h->nb_use[kNbWeno] = true;
   }
+  if (gate) ST(launch_band_gate(h->stream, h->nb_counts, 3, gate));
   for (int i = 0; i < 3; ++i)
     if (i != phi0)
       CU(cudaMemcpyAsync(h->buf[i], h->buf[phi0], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
@@ -462,8 +465,10 @@ int band_end(flsp_handle* h, int phi0) {
   return launch_band_restore(h->ctx(), h->buf[phi0], h->buf[h->cur], h->nb_flags);
 }
 
-// ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637)
-int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
+// ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637);
+// a narrow-band sweep with a gate (device count) sweeps nothing when the
+// count is zero
+int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter, const int* gate = nullptr) {
   ST(validate_reinit(h, o));
   if (o->viscosity > 0.0) ST(ensure_ldg_buffers(h));
   const bool limiter = reinit_limiter(h, o);
@@ -471,7 +476,7 @@ int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter) {
   const bool narrow = o->narrow_band != 0;
   if (narrow) {
     ST(ensure_band_buffers(h));
-    const int st = band_begin(h, o, phi0, limiter);
+    const int st = band_begin(h, o, phi0, limiter, gate);
     if (st) {
       for (int k = 0; k < 3; ++k) h->nb_use[k] = false;
       return st;
@@ -694,6 +699,8 @@ int ensure_learned_buffers(flsp_handle* h, int64_t nfeat) {
     CU(cudaMalloc(&h->lrn_work, (size_t)(2 * nblk + 2) * sizeof(int)));
     CU(cudaMalloc(&h->lrn_cells, (size_t)ncell * sizeof(int)));
     CU(cudaMalloc(&h->lrn_count, 2 * sizeof(int)));
+    CU(cudaMalloc(&h->lrn_tot, 2 * sizeof(unsigned long long)));
+    CU(cudaMemsetAsync(h->lrn_tot, 0, 2 * sizeof(unsigned long long), h->stream));
     CU(cudaMallocHost(&h->lrn_count_host, 4 * sizeof(int)));
     CU(cudaEventCreateWithFlags(&h->lrn_ev, cudaEventDisableTiming));
     CU(cudaMalloc(&h->lrn_save, (size_t)h->ndofs * h->tsize + kStatePad));
@@ -730,8 +737,56 @@ int enqueue_learned(flsp_handle* h, flsp_mlp* net, double band_cells, int pre, i
   const cudaError_t e2 = cudaStreamWaitEvent(h->stream, h->lrn_ev, 0);
   ST(st);
   if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(FLSP_ERR_CUDA, "learned reinit: stream join failed");
-  return launch_apply_delta(h->stream, h->prec, h->m.nb, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells,
-                            ncell, nband, net->y, net->y_ld);
+  ST(launch_apply_delta(h->stream, h->prec, h->m.nb, h->buf[pre], h->buf[out], h->ndofs, hh, h->lrn_cells,
+                        ncell, nband, net->y, net->y_ld));
+  // the network's next pass (another handle's, in a group) overwrites its
+  // output: it waits until this apply has read it
+  CU(cudaEventRecord(h->lrn_ev, h->stream));
+  CU(cudaStreamWaitEvent(net->stream, h->lrn_ev, 0));
+  return FLSP_OK;
+}
+
+// A learned reinitialisation with its residual fallback, enqueued without
+// a host wait (graph-capturable): the network's result from buf[cur], the
+// band cells whose mean ||grad phi| - 1| exceeds o->max_residual, the
+// narrow-band HJ sweep (o->fallback, fixed count) from buf[cur] gated on
+// that device-side count (its launches find no tile when no cell failed),
+// and the network's result everywhere but the failed cells, which take the
+// sweep's.  The operations of flsp_reinit_learned, whose host loop decides
+// the same on the host; h->cur ends on the result.  Band, learned and LDG
+// buffers are allocated beforehand.
+int enqueue_learned_fallback(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o) {
+  const int64_t ncell = h->m.ncell;
+  const int pre = h->cur, out = other(pre, -1);
+  ST(enqueue_learned(h, net, o->band_cells, pre, out));
+  ST(launch_residual_flags(h->stream, h->prec, h->dim, h->buf[out], h->m.h[0], h->lrn_cells, ncell,
+                           h->lrn_count, o->max_residual, h->lrn_flags, h->lrn_count + 1));
+  CU(cudaMemcpyAsync(h->lrn_save, h->buf[out], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  h->cur = pre;
+  int nit = 0;
+  ST(run_reinit(h, &o->fallback, &nit, h->lrn_count + 1));
+  const int hj = h->cur, res = other(hj, -1);
+  CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
+  ST(launch_merge_cells(h->stream, h->prec, h->m.nb, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, ncell,
+                        h->lrn_count));
+  ST(launch_learned_totals(h->stream, h->lrn_count, h->lrn_tot, 1));
+  h->cur = res;
+  return FLSP_OK;
+}
+
+// a fallback that graph-replayed periods can carry: enabled by a finite
+// positive max_residual, a fixed-count narrow-band sweep (the other modes
+// need host decisions)
+int learned_graph_fallback(flsp_handle* h, const flsp_learned_opts* o, bool* on) {
+  *on = std::isfinite(o->max_residual) && o->max_residual > 0.0;
+  if (!*on) return FLSP_OK;
+  ST(validate_reinit(h, &o->fallback));
+  if (o->fallback.mode != FLSP_REINIT_FIXED || !o->fallback.narrow_band)
+    return fail(FLSP_ERR_BAD_ARG, "graph-replayed learned periods need a fixed-count narrow-band fallback sweep "
+                                  "(or max_residual = infinity for none)");
+  ST(ensure_band_buffers(h));
+  if (o->fallback.viscosity > 0.0) ST(ensure_ldg_buffers(h));
+  return FLSP_OK;
 }
 
 // band cells of the current state: |mean phi| <= band_cells * h; returns the count
@@ -909,7 +964,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
   if (h->optab) cudaFree(h->optab);
-  void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_save, h->lrn_feat,
+  void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_tot, h->lrn_save, h->lrn_feat,
                  h->nb_flags, h->nb_lists, h->nb_counts};
   for (void* q : lrn)
     if (q) cudaFree(q);
@@ -1546,6 +1601,7 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   // band cells whose result is not distance-like enough take the HJ sweep
   ST(launch_residual_flags(h->stream, h->prec, h->dim, h->buf[out], hh, h->lrn_cells, ncell, nband,
                            o->max_residual, h->lrn_flags, h->lrn_count + 1));
+  ST(launch_learned_totals(h->stream, h->lrn_count, h->lrn_tot, 1));
   CU(cudaMemcpyAsync(h->lrn_count_host, h->lrn_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(h->lrn_count_host + 2, net->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -1574,6 +1630,20 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
   return FLSP_OK;
 }
 
+int flsp_learned_totals(flsp_handle* h, int64_t* n_band, int64_t* n_fallback, int reset) {
+  if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+  CU(cudaSetDevice(h->dev));
+  unsigned long long t[2] = {0, 0};
+  if (h->lrn_tot) {
+    CU(cudaMemcpyAsync(t, h->lrn_tot, sizeof(t), cudaMemcpyDeviceToHost, h->stream));
+    if (reset) CU(cudaMemsetAsync(h->lrn_tot, 0, sizeof(t), h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+  }
+  if (n_band) *n_band = (int64_t)t[0];
+  if (n_fallback) *n_fallback = (int64_t)t[1];
+  return FLSP_OK;
+}
+
 int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o, int reinit_frequency,
                               int n_steps) {
   if (!h || !net || !o) return fail(FLSP_ERR_BAD_ARG, "null argument");
@@ -1585,6 +1655,8 @@ int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_
   // buffers and attributes before any capture
   ST(ensure_learned_buffers(h, h->m.ncell));
   ST(mlp_ensure_cap(net, h->m.ncell));
+  bool fb = false;
+  ST(learned_graph_fallback(h, o, &fb));
   ST(launch_adv_clock_horizon(h->stream, h->clk, INFINITY));
   int done = 0;
   while (done < n_steps) {
@@ -1603,6 +1675,11 @@ int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_
       mix(&o->band_cells, sizeof(o->band_cells));
       mix(&net->uid, sizeof(net->uid));
       mix(&net->cap, sizeof(net->cap));
+      mix(&fb, sizeof(fb));
+      if (fb) {
+        mix(&o->max_residual, sizeof(o->max_residual));
+        mix(&o->fallback, sizeof(o->fallback));
+      }
       auto it = h->graphs.find(key);
       if (it == h->graphs.end()) {
         const int cur0 = h->cur;
@@ -1610,9 +1687,12 @@ int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_
         CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
         int st = FLSP_OK;
         for (int s = 0; s < to_reinit && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
-        if (st == FLSP_OK) {
+        if (st == FLSP_OK && fb) {
+          st = enqueue_learned_fallback(h, net, o);
+        } else if (st == FLSP_OK) {
           const int pre = h->cur, out = other(pre, -1);
           st = enqueue_learned(h, net, o->band_cells, pre, out);
+          if (st == FLSP_OK) st = launch_learned_totals(h->stream, h->lrn_count, h->lrn_tot, 0);
           if (st == FLSP_OK) h->cur = out;
         }
         cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
@@ -2154,6 +2234,7 @@ struct GroupMode {
   const flsp_reinit_opts* ro = nullptr;
   flsp_mlp* net = nullptr;
   const flsp_learned_opts* lo = nullptr;
+  bool fallback = false;   // learned with its residual fallback
 };
 
 int group_run(flsp_group* g, const GroupMode& gm, int n_periods) {
@@ -2179,6 +2260,11 @@ int group_run(flsp_group* g, const GroupMode& gm, int n_periods) {
       mix(&gm.net->uid, sizeof(gm.net->uid));
       mix(&gm.net->cap, sizeof(gm.net->cap));
       mix(&gm.lo->band_cells, sizeof(gm.lo->band_cells));
+      mix(&gm.fallback, sizeof(gm.fallback));
+      if (gm.fallback) {
+        mix(&gm.lo->max_residual, sizeof(gm.lo->max_residual));
+        mix(&gm.lo->fallback, sizeof(gm.lo->fallback));
+      }
     }
     auto gi = g->graphs.find(key);
     if (gi == g->graphs.end()) {
@@ -2197,9 +2283,12 @@ int group_run(flsp_group* g, const GroupMode& gm, int n_periods) {
             // the members' network passes share the network's buffers: they
             // follow one another on its stream (member order)
             for (int s = 0; s < gm.freq && st == FLSP_OK; ++s) st = enqueue_adv_step(h);
-            if (st == FLSP_OK) {
+            if (st == FLSP_OK && gm.fallback) {
+              st = enqueue_learned_fallback(h, gm.net, gm.lo);
+            } else if (st == FLSP_OK) {
               const int pre = h->cur, out = other(pre, -1);
               st = enqueue_learned(h, gm.net, gm.lo->band_cells, pre, out);
+              if (st == FLSP_OK) st = launch_learned_totals(h->stream, h->lrn_count, h->lrn_tot, 0);
               if (st == FLSP_OK) h->cur = out;
             }
           } else {
@@ -2265,11 +2354,13 @@ int flsp_group_run_periods_learned(flsp_group* g, flsp_mlp* net, const flsp_lear
   if (!(o->band_cells > 0.0)) return fail(FLSP_ERR_BAD_ARG, "bad learned options");
   CU(cudaSetDevice(g->dev));
   int64_t max_cells = 0;
+  bool fb = false;
   for (flsp_handle* h : g->h) {
     if (!h->has_vel) return fail(FLSP_ERR_BAD_ARG, "velocity not set");
     if (h->n_since_reinit != 0) return fail(FLSP_ERR_BAD_ARG, "a group member is inside a reinit period");
     ST(learned_check(h, net));
     ST(ensure_learned_buffers(h, h->m.ncell));
+    ST(learned_graph_fallback(h, o, &fb));
     max_cells = std::max<int64_t>(max_cells, h->m.ncell);
   }
   ST(mlp_ensure_cap(net, max_cells));
@@ -2277,6 +2368,7 @@ int flsp_group_run_periods_learned(flsp_group* g, flsp_mlp* net, const flsp_lear
   gm.freq = reinit_frequency;
   gm.net = net;
   gm.lo = o;
+  gm.fallback = fb;
   return group_run(g, gm, n_periods);
 }
 

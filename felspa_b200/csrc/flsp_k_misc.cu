@@ -419,6 +419,33 @@ int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margi
   return launch_status("band_tiles_kernel");
 }
 
+namespace {
+// no tile for any band kernel family when the gate count is zero
+__global__ void band_gate_kernel(int* counts, int n, const int* gate) {
+  if (threadIdx.x < n && *gate == 0) counts[threadIdx.x] = 0;
+}
+}  // namespace
+
+namespace {
+// running totals of the learned reinitialisation: band cells, and fallback
+// cells when `with_fallback`
+__global__ void learned_totals_kernel(const int* counts, unsigned long long* tot, int with_fallback) {
+  if (threadIdx.x != 0) return;
+  tot[0] += (unsigned long long)counts[0];
+  if (with_fallback) tot[1] += (unsigned long long)counts[1];
+}
+}  // namespace
+
+int launch_learned_totals(cudaStream_t s, const int* counts, unsigned long long* tot, int with_fallback) {
+  learned_totals_kernel<<<1, 32, 0, s>>>(counts, tot, with_fallback);
+  return launch_status("learned_totals_kernel");
+}
+
+int launch_band_gate(cudaStream_t s, int* counts, int n, const int* gate) {
+  band_gate_kernel<<<1, 32, 0, s>>>(counts, n, gate);
+  return launch_status("band_gate_kernel");
+}
+
 int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags) {
   const int blocks = grid_for(c.m.ncell * c.m.nb);
   if (c.prec == FLSP_FP64)

@@ -276,6 +276,73 @@ def zalesak_run(method, net=None, n=128, every=40, T=1.0, plain=None, max_residu
 zalesak_run.steps_to_T = {}
 
 
+def interface_run(method, net=None, velocity=None, ic=None, t_end=1.0, n=256, every=40, plain=None,
+                  max_residual=0.05, steps=None, precision=abi.FP32):
+    """One run of a 2D degree-2 Q level set (FP32, CFL 0.1) from the
+    projected `ic` under `velocity` to `t_end` (or for `steps` substeps),
+    reinitialised every `every` substeps by `method`: "none", "plain" (the
+    fixed-count sweep `plain`, periods replayed from CUDA graphs) or
+    "learned" (the network over the 6-cell band with the residual test and
+    the narrow-band fallback sweep decided on the device; max_residual =
+    inf: no fallback; periods replayed from CUDA graphs).  Device time of
+    the whole run; L1 interface error against the exact solution `ic`
+    (the shape returns at t_end for the periodic and time-reversed flows
+    used here) and area change."""
+    import torch
+    from .level_set import Mesh, Problem
+    L = load()
+    plain = plain if plain is not None else plain_reinit_opts()
+    pb = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=precision, cfl_max=0.1)
+    pb.set_velocity(velocity)
+    pb.project(ic)
+    area0 = pb.reduce(abi.RED_MASS_SHARP)
+    if steps is None:
+        # substep count to t_end: the CFL-limited step sequence depends on
+        # the velocity alone (running-maximum estimate), so a run without
+        # reinitialisation counts it
+        probe = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=precision, cfl_max=0.1)
+        probe.set_velocity(velocity)
+        probe.project(ic)
+        while probe.get_time() < t_end - 1e-12:
+            check(L.flsp_advance_steps(probe.h, 200, float(t_end)))
+        steps = probe.get_step_count()
+        probe.close()
+    lo = default_learned_opts(max_residual=max_residual)
+    lo.fallback = abi.ReinitOpts.from_buffer_copy(plain)
+    lo.fallback.narrow_band = 1
+    lo.fallback.band_cells = lo.band_cells
+    s = torch.cuda.ExternalStream(pb.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    check(L.flsp_sync(pb.h))
+    e0.record(s)
+    if method == "none":
+        check(L.flsp_advance_steps(pb.h, int(steps), float(t_end)))
+    elif method == "plain":
+        ctl = abi.default_ls_opts(reinit_frequency=every, reinit=plain)
+        check(L.flsp_ls_run_steps(pb.h, C.byref(ctl), int(steps)))
+    elif method == "learned":
+        check(L.flsp_ls_run_steps_learned(pb.h, net.h, C.byref(lo), int(every), int(steps)))
+    else:
+        raise ValueError(method)
+    e1.record(s)
+    check(L.flsp_sync(pb.h))
+    ms = e0.elapsed_time(e1)
+    out = {"method": method, "every": every, "steps": int(steps), "t": pb.get_time(), "device_s": ms * 1e-3,
+           "dof_steps_per_s": pb.n_dofs * steps / (ms * 1e-3),
+           "l1_interface_error": pb.reduce(abi.RED_L1_INTERFACE_IC, ic),
+           "area_change": (pb.reduce(abi.RED_MASS_SHARP) - area0) / area0,
+           "grad_deviation": pb.reduce(abi.RED_GRAD_DEVIATION)}
+    if method == "learned":
+        out["max_residual"] = max_residual if np.isfinite(max_residual) else None
+        nb, nf = C.c_int64(0), C.c_int64(0)
+        check(L.flsp_learned_totals(pb.h, C.byref(nb), C.byref(nf), 0))
+        out["band_cells_total"] = nb.value
+        if np.isfinite(max_residual):
+            out["fallback_fraction"] = nf.value / nb.value if nb.value else 0.0
+    pb.close()
+    return out
+
+
 def learned_vs_plain(n=128, instances=24, train_steps=8000, seed=7):
     """Train the network on the plain sweep's pairs (on the GPU), then run
     the slotted-disk revolution with no reinit, the plain sweep (host loop

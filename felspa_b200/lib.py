@@ -79,6 +79,7 @@ PROTOTYPES = {
     "flsp_mlp_eval": (C.c_int, [_vp, _dp]),
     "flsp_reinit_learned": (C.c_int, [_vp, _vp, C.POINTER(abi.LearnedOpts), C.POINTER(abi.LearnedStats)]),
     "flsp_ls_run_steps_learned": (C.c_int, [_vp, _vp, C.POINTER(abi.LearnedOpts), C.c_int, C.c_int]),
+    "flsp_learned_totals": (C.c_int, [_vp, _i64p, _i64p, C.c_int]),
     "flsp_default_train_opts": (None, [C.POINTER(abi.TrainOpts)]),
     "flsp_default_learned_opts": (None, [C.POINTER(abi.LearnedOpts)]),
     "flsp_batch_create": (C.c_int, [C.c_int, C.POINTER(abi.MeshDesc), C.POINTER(abi.DGOpts), C.POINTER(_vp)]),

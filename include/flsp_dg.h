@@ -489,14 +489,23 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
                         flsp_learned_stats* stats);
 /* n_steps advection substeps with a learned reinitialisation every
    reinit_frequency steps, each period replayed from a captured CUDA graph
-   (like flsp_ls_run_steps).  No counterpart in the reference.  The
-   network's result is taken in every band cell: the residual test and the
-   HJ fallback of flsp_reinit_learned need a host decision and are not
-   part of these periods (o->max_residual and o->fallback are not used).
-   Enqueued; flsp_sync waits.  The first period of each buffer role sizes
-   the network's work buffers for every cell of the mesh.               */
+   (like flsp_ls_run_steps).  No counterpart in the reference.  With a
+   finite o->max_residual > 0 each period carries the residual test and
+   the HJ fallback of flsp_reinit_learned, decided on the device: the
+   fallback sweep (o->fallback, which must be a fixed-count narrow-band
+   sweep) is always enqueued and finds no tile to sweep when no band cell
+   failed the test, so the results equal flsp_reinit_learned's.  With
+   o->max_residual = infinity the network's result is taken in every band
+   cell.  Enqueued; flsp_sync waits.  The first period of each buffer role
+   sizes the network's work buffers for every cell of the mesh.         */
 int flsp_ls_run_steps_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o,
                               int reinit_frequency, int n_steps);
+/* running totals over the handle's learned reinitialisations (host loop,
+   graph-replayed periods, groups): band cells the network redistanced
+   and, of those, cells that took the fallback sweep's result (periods
+   without a fallback add to the first only); reset != 0 zeroes them.
+   Synchronises the handle's stream.                                    */
+int flsp_learned_totals(flsp_handle* h, int64_t* n_band, int64_t* n_fallback, int reset);
 void flsp_default_train_opts(flsp_train_opts* o);
 void flsp_default_learned_opts(flsp_learned_opts* o);
 
@@ -552,10 +561,12 @@ typedef struct flsp_group flsp_group;
 int flsp_group_create(flsp_handle* const* handles, int n, flsp_group** out);
 void flsp_group_destroy(flsp_group* g);
 int flsp_group_run_periods(flsp_group* g, const flsp_ls_opts* o, int n_periods);
-/* the same with the learned reinitialisation (no fallback, as in
-   flsp_ls_run_steps_learned): every member advances reinit_frequency
-   substeps and takes the network's result in its band; the members'
-   network passes follow one another on the network's stream             */
+/* the same with the learned reinitialisation, the residual fallback
+   decided on the device as in flsp_ls_run_steps_learned (none for
+   o->max_residual = infinity): every member advances reinit_frequency
+   substeps and takes the network's result in its band, its failed cells
+   the result of its own fallback sweep; the members' network passes
+   follow one another on the network's stream                            */
 int flsp_group_run_periods_learned(flsp_group* g, flsp_mlp* net, const flsp_learned_opts* o,
                                    int reinit_frequency, int n_periods);
 int flsp_group_sync(flsp_group* g);

@@ -78,6 +78,11 @@ def revolution_cases():
         "zalesak128_p1_nu0": (abi.BASIS_P, 0.0, False),
         "zalesak128_q1_nu1e-3": (abi.BASIS_Q, 1e-3, True),
         "zalesak128_p1_nu1e-3": (abi.BASIS_P, 1e-3, True),
+        # the reference test's viscosity 1e-3 on its [-50, 50]^2 domain with
+        # period 628, rescaled to the unit square with period 1:
+        # 1e-3 * 628 / 100^2
+        "zalesak128_q1_nu6.28e-5": (abi.BASIS_Q, 6.28e-5, True),
+        "zalesak128_p1_nu6.28e-5": (abi.BASIS_P, 6.28e-5, True),
     }
 
 

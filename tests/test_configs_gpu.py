@@ -3,7 +3,8 @@ at their own sizes and horizons (FP64 mode):
 
 * the 2D Zalesak slotted disk, 128^2 degree-1 cells (Q and P), one full
   counter-clockwise revolution (17,440 CFL-limited SSP-RK3 substeps, 1,744
-  reinitialisations), without and with the reference test's LDG viscosity,
+  reinitialisations), without LDG viscosity, with the reference test's
+  viscosity rescaled to the unit square (1e-3 * 628 / 100^2) and with 1e-3,
   against full-revolution oracle runs frozen in tests/golden/ (made by
   tests/golden/make_golden.py; the oracle is deterministic for any thread
   count, so the fixture equals a run on this machine);
@@ -51,6 +52,8 @@ def revolution_control(viscosity):
     ("zalesak128_p1_nu1e-3", abi.BASIS_P, 1e-3),
     ("zalesak128_q1_nu0", abi.BASIS_Q, 0.0),
     ("zalesak128_p1_nu0", abi.BASIS_P, 0.0),
+    ("zalesak128_q1_nu6.28e-5", abi.BASIS_Q, 6.28e-5),
+    ("zalesak128_p1_nu6.28e-5", abi.BASIS_P, 6.28e-5),
 ])
 def test_zalesak_revolution(flsp, name, basis, viscosity):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))

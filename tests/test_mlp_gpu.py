@@ -183,3 +183,34 @@ def test_learned_graph_periods_match_host_loop():
     a.close()
     b.close()
     net.close()
+
+
+@pytest.mark.parametrize("max_residual", [1e-12, 0.3, 1e30])
+def test_learned_graph_periods_with_fallback_match_host_loop(max_residual):
+    """learned periods replayed from CUDA graphs with the residual test and
+    the HJ fallback decided on the device equal the host loop (advance,
+    then flsp_reinit_learned, whose host decides) bit for bit: every band
+    cell failing, some failing, none failing (the gated sweep finds no
+    tile)"""
+    import ctypes as C
+    from felspa_b200.lib import check, load
+    net = MLP(device=0, seed=12)    # untrained: many cells fail a moderate bound
+    lo = default_learned_opts(max_residual=max_residual, fallback_pseudo_steps=4)
+    a, b = make_problem(40, 13), make_problem(40, 13)
+    fails = []
+    for _ in range(3):
+        advance(a, 6)
+        st = net.reinit(a, lo)
+        fails.append(st["n_fallback"])
+    check(load().flsp_ls_run_steps_learned(b.h, net.h, C.byref(lo), 6, 3 * 6))
+    check(load().flsp_sync(b.h))
+    if max_residual < 1e-6:
+        assert min(fails) > 0
+    if max_residual > 1e6:
+        assert max(fails) == 0
+    assert a.get_time() == b.get_time()
+    sa, sb = a.get_state(), b.get_state()
+    assert np.all(np.isfinite(sb)) and np.array_equal(sa, sb)
+    a.close()
+    b.close()
+    net.close()
