@@ -35,6 +35,9 @@ CURV_REFERENCE, CURV_NEIGHBOUR = range(2)
 (RED_MASS, RED_MASS_ERROR, RED_L1_INTERFACE, RED_MEAN_ABS_DIFF, RED_GRAD_DEVIATION,
  RED_MAX_ABS, RED_L2_ERROR_IC, RED_L1_INTERFACE_IC, RED_MASS_SHARP) = range(9)
 NOALLOC_MAX_CELLS = 65536 * 128   # flsp_reduce_noalloc scratch limit (cells)
+MAX_MATERIALS = 8                 # level sets of a material stack
+MAX_MIX_QPTS = 8                  # Gauss points per axis of the mixing
+HEAVISIDE_NONE, HEAVISIDE_LINEAR, HEAVISIDE_SINE = 0, 1, 2
 
 MAX_VEL_TERMS = 24
 MAX_IC_NODES = 32

@@ -1055,6 +1055,71 @@ int flsp_eval_patches(flsp_handle* h, int n_sub, double* values, int64_t n) {
   return st;
 }
 
+int flsp_material_mix(flsp_handle* const* ls, int n, const double* values, int nq, int smoothing, double* out,
+                      int64_t n_out) {
+  if (!ls || !values || !out) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (n < 1 || n > FLSP_MAX_MATERIALS) return fail(FLSP_ERR_BAD_ARG, "1..FLSP_MAX_MATERIALS level sets");
+  if (nq < 1 || nq > FLSP_MAX_MIX_QPTS) return fail(FLSP_ERR_BAD_ARG, "n_qpts_1d must be in 1..FLSP_MAX_MIX_QPTS");
+  if (smoothing < FLSP_HEAVISIDE_NONE || smoothing > FLSP_HEAVISIDE_SINE)
+    return fail(FLSP_ERR_BAD_ARG, "bad Heaviside smoothing");
+  const flsp_handle* h0 = ls[0];
+  for (int i = 0; i < n; ++i) {
+    const flsp_handle* h = ls[i];
+    if (!h) return fail(FLSP_ERR_BAD_ARG, "null handle");
+    bool same = h->dim == h0->dim && h->dev == h0->dev;
+    for (int d = 0; d < 3 && same; ++d)
+      same = h->m.n[d] == h0->m.n[d] && h->m.lo[d] == h0->m.lo[d] && h->m.h[d] == h0->m.h[d];
+    if (!same) return fail(FLSP_ERR_BAD_ARG, "the level sets of a material stack must share mesh and device");
+  }
+  for (int i = 0; i <= n; ++i)
+    if (!std::isfinite(values[i])) return fail(FLSP_ERR_BAD_ARG, "non-finite material value");
+  const long long npt = h0->dim == 3 ? (long long)nq * nq * nq : (long long)nq * nq;
+  if (n_out != h0->m.ncell * npt) return fail(FLSP_ERR_BAD_ARG, "size mismatch (n_cells * n_qpts_1d^dim)");
+  CU(cudaSetDevice(h0->dev));
+  MixArgs a;
+  std::memset(&a, 0, sizeof(a));
+  double x[FLSP_MAX_MIX_QPTS], w[FLSP_MAX_MIX_QPTS], v[8], dv[8], ddv[8];
+  gauss_rule(nq, x, w);
+  for (int q = 0; q < nq; ++q) {
+    leg_all(kMaxN1, x[q], v, dv, ddv);
+    for (int k = 0; k < kMaxN1; ++k) a.L[k][q] = v[k];
+  }
+  a.perm = h0->perm;
+  a.ncell = h0->m.ncell;
+  a.n = n;
+  a.dim = h0->dim;
+  a.nq = nq;
+  a.smoothing = smoothing;
+  for (int i = 0; i <= n; ++i) a.value[i] = values[i];
+  // the kernel runs on the first handle's stream, after that handle's
+  // earlier work; the other handles' streams are drained first
+  for (int i = 0; i < n; ++i) {
+    flsp_handle* h = ls[i];
+    MixLevelSet& m = a.ls[i];
+    m.phi = h->buf[h->cur];
+    m.prec = h->prec;
+    m.n1 = h->p + 1;
+    m.nb = h->m.nb;
+    m.eps = 1.5 * h->m.min_diam;
+    std::memcpy(m.q2g, h->m.q2g, sizeof(m.q2g));
+    if (i > 0) CU(cudaStreamSynchronize(h->stream));
+  }
+  // results in the first handle's FP64 staging buffer when it is large
+  // enough (2 dim n_dofs doubles), else in a buffer of their own
+  flsp_handle* hs = ls[0];
+  const bool own = n_out > (long long)hs->ndofs * 2 * hs->dim;
+  double* dev = hs->stage64;
+  if (own) CU(cudaMalloc(&dev, sizeof(double) * (size_t)n_out));
+  int st = launch_material_mix(a, hs->stream, dev);
+  if (st == FLSP_OK) {
+    cudaError_t e = cudaMemcpyAsync(out, dev, sizeof(double) * (size_t)n_out, cudaMemcpyDeviceToHost, hs->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hs->stream);
+    if (e != cudaSuccess) st = fail(FLSP_ERR_CUDA, std::string("material mix copy: ") + cudaGetErrorString(e));
+  }
+  if (own) cudaFree(dev);
+  return st;
+}
+
 int flsp_curvature(flsp_handle* h, int mode, double* kappa, int64_t n) {
   if (!h || !kappa) return fail(FLSP_ERR_BAD_ARG, "null argument");
   if (mode != FLSP_CURV_REFERENCE && mode != FLSP_CURV_NEIGHBOUR) return fail(FLSP_ERR_BAD_ARG, "bad curvature mode");

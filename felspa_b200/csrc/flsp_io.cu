@@ -87,6 +87,75 @@ int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int 
 }
 
 // ---------------------------------------------------------------------
+// MaterialStack mixing, MaterialAccessor<MaterialStack>::reinit +
+// eval_scalars (include/felspa/level_set/src/material_stack.implement.h:
+// 320-470): at every Gauss point of every cell, the level sets in stack
+// order each take the share rest * H(-phi_i) of what the earlier ones left
+// (rest starts at 1; a share or rest of magnitude <= DBL_EPSILON counts as
+// zero, numerics::is_zero), the background material the remaining rest;
+// the mixed scalar is the share-weighted sum of the materials' values.
+// H is LevelSetSurface::domain_identity (level_set.implement.h:356-380):
+// sharp, linear or sine smoothing over eps = 1.5 min_diameter
+// (level_set.implement.h:957-993).  One thread per (cell, point), FP64.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ double mix_heaviside(double y, double eps, int kind) {
+  const double kEpsD = 2.220446049250313e-16;
+  if (kind == FLSP_HEAVISIDE_NONE) return y > 0.0 ? 1.0 : (y < 0.0 ? 0.0 : 0.5);
+  if (y > eps) return 1.0;
+  if (y < -eps) return 0.0;
+  if (kind == FLSP_HEAVISIDE_LINEAR) return 0.5 * (y / eps + 1.0);
+  const double v = 0.5 * (1.0 + y / eps + sin(y * 3.14159265358979323846 / eps) / 3.14159265358979323846);
+  if (fabs(v) < kEpsD) return 0.0;
+  if (fabs(v - 1.0) < kEpsD) return 1.0;
+  return v;
+}
+
+__global__ void __launch_bounds__(256) material_mix_kernel(const MixArgs a, double* __restrict__ out) {
+  const double kEpsD = 2.220446049250313e-16;
+  const int nq = a.nq;
+  const long long npt = a.dim == 3 ? (long long)nq * nq * nq : (long long)nq * nq;
+  const long long total = a.ncell * npt;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long k = idx / npt;
+    const int j = (int)(idx - k * npt);
+    const long long c = a.perm ? a.perm[k] : k;
+    const int qx = j % nq, qy = (j / nq) % nq, qz = a.dim == 3 ? j / (nq * nq) : 0;
+    double rest = 1.0, v = 0.0;
+    for (int i = 0; i < a.n && !(fabs(rest) <= kEpsD); ++i) {
+      const MixLevelSet& ls = a.ls[i];
+      const int n1 = ls.n1, n3 = a.dim == 3 ? n1 : 1;
+      double phi = 0.0;
+      for (int a2 = 0; a2 < n3; ++a2)
+        for (int a1 = 0; a1 < n1; ++a1)
+          for (int a0 = 0; a0 < n1; ++a0) {
+            const int gi = ls.q2g[a0 + n1 * (a1 + n1 * a2)];
+            if (gi < 0) continue;
+            const double cv = ls.prec == FLSP_FP64 ? ((const double*)ls.phi)[c * ls.nb + gi]
+                                                   : (double)((const float*)ls.phi)[c * ls.nb + gi];
+            phi += cv * a.L[a0][qx] * a.L[a1][qy] * (a.dim == 3 ? a.L[a2][qz] : 1.0);
+          }
+      const double H = mix_heaviside(-phi, ls.eps, a.smoothing);
+      if (!(fabs(H) <= kEpsD)) {
+        const double share = rest * H;
+        v += a.value[i] * share;
+        rest -= share;
+      }
+    }
+    if (!(fabs(rest) <= kEpsD)) v += a.value[a.n] * rest;
+    out[idx] = v;
+  }
+}
+
+int launch_material_mix(const MixArgs& a, cudaStream_t s, double* out) {
+  const long long npt = a.dim == 3 ? (long long)a.nq * a.nq * a.nq : (long long)a.nq * a.nq;
+  const long long total = a.ncell * npt;
+  const int grid = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  material_mix_kernel<<<grid, 256, 0, s>>>(a, out);
+  return launch_status("material_mix_kernel");
+}
+
+// ---------------------------------------------------------------------
 // Curvature estimate, LevelSetSurface::CurvatureEstimator::estimate
 // (include/felspa/level_set/src/level_set.implement.h:600-812): the weak
 // divergence of n = grad phi / |grad phi| on QGauss(p+1) cell and face

@@ -192,6 +192,23 @@ int launch_hj_clock_end(cudaStream_t s, DevClock* clk);
 // ---------------- output (flsp_io.cu) ----------------
 // out[k * (n_sub+1)^dim + j] = the state of host cell k at its patch vertex j
 int launch_eval_patches(const Ctx& c, const void* phi, const int64_t* perm, int n_sub, double* out);
+
+// MaterialStack mixing (flsp_io.cu): one level set of the stack
+struct MixLevelSet {
+  const void* phi;        // state, lexicographic cells
+  int prec, n1, nb;
+  double eps;             // Heaviside smoothing width, 1.5 min_diameter
+  signed char q2g[64];    // Q-layout mode -> in-cell DoF (-1: absent)
+};
+struct MixArgs {
+  MixLevelSet ls[FLSP_MAX_MATERIALS];
+  double value[FLSP_MAX_MATERIALS + 1];   // stack entries, then the background
+  double L[kMaxN1][FLSP_MAX_MIX_QPTS];    // Legendre values at the Gauss points
+  const int64_t* perm;                    // output cell order (null: lexicographic)
+  long long ncell;
+  int n, dim, nq, smoothing;
+};
+int launch_material_mix(const MixArgs& a, cudaStream_t s, double* out);
 // values2 / label2 (or NULL): a second point-data array
 int write_vtu_file(const flsp_mesh_desc* mesh, int n_sub, const double* values, const char* label,
                    const char* filename, const double* values2, const char* label2);

@@ -448,3 +448,43 @@ class LevelSetSurface(AdvectSimulator):
 
     def gradient_deviation(self):
         return self.problem.reduce(abi.RED_GRAD_DEVIATION)
+
+
+class MaterialStack:
+    """ls::MaterialStack (include/felspa/level_set/material_stack.h:22) for
+    materials with one constant scalar each: materials pushed with their
+    level sets (LevelSetSurface or Problem, all on one mesh), a background
+    material, and the mixed scalar at the Gauss points of every cell
+    (MaterialAccessor<MaterialStack>::reinit + eval_scalars,
+    material_stack.implement.h:320-470), evaluated on the device."""
+
+    def __init__(self, background_value=None):
+        self.background = background_value
+        self.entries = []
+
+    def set_background_material(self, value):
+        self.background = float(value)
+
+    def push(self, value, level_set):
+        if len(self.entries) >= abi.MAX_MATERIALS:
+            raise ValueError("at most %d level sets" % abi.MAX_MATERIALS)
+        self.entries.append((float(value), getattr(level_set, "problem", level_set)))
+
+    def n_materials(self):
+        return len(self.entries)
+
+    def eval_scalars(self, n_qpts_1d, smoothing=abi.HEAVISIDE_SINE):
+        """mixed scalar, shape (n_cells, n_qpts_1d^dim): host cell order of
+        the first level set, QGauss(n_qpts_1d) points x fastest"""
+        if self.background is None:
+            raise ValueError("the background material must be set first (ExcBackgroundMaterialUndefined)")
+        if not self.entries:
+            raise ValueError("no material pushed")
+        pb0 = self.entries[0][1]
+        n = len(self.entries)
+        hs = (C.c_void_p * n)(*[pb.h for _, pb in self.entries])
+        vals = np.ascontiguousarray([v for v, _ in self.entries] + [self.background], dtype=np.float64)
+        npt = n_qpts_1d ** pb0.mesh.dim
+        out = np.empty(pb0.mesh.n_cells * npt)
+        check(load().flsp_material_mix(hs, n, dp(vals), int(n_qpts_1d), int(smoothing), dp(out), out.size))
+        return out.reshape(pb0.mesh.n_cells, npt)

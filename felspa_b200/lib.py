@@ -54,6 +54,7 @@ PROTOTYPES = {
     "flsp_autotune": (C.c_int, [_vp, C.c_int, _ip, _ip, _dp, _ip]),
     "flsp_stage_tile": (C.c_int, [_vp, _ip]),
     "flsp_curvature": (C.c_int, [_vp, C.c_int, _dp, C.c_int64]),
+    "flsp_material_mix": (C.c_int, [C.POINTER(_vp), C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int64]),
     "flsp_eval_patches": (C.c_int, [_vp, C.c_int, _dp, C.c_int64]),
     "flsp_export_solutions": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
     "flsp_write_vtu": (C.c_int, [C.POINTER(abi.MeshDesc), C.c_int, _dp, C.c_char_p, C.c_char_p]),

@@ -377,6 +377,33 @@ int flsp_write_vtu(const flsp_mesh_desc* mesh, int n_sub, const double* values,
 int flsp_write_pvd(const char* filename, int n, const double* times,
                    const char* const* files);
 
+/* MaterialStack mixing: MaterialAccessor<MaterialStack>::reinit and
+   eval_scalars (include/felspa/level_set/src/material_stack.implement.h:
+   320-470) for materials with one constant scalar each (a viscosity, a
+   density).  At every point of QGauss(n_qpts_1d) of every cell, the level
+   sets level_sets[0..n) in stack order each take the share
+   rest * H(-phi_i) of what the earlier ones left (rest starts at 1), the
+   background material the remaining rest, where H is the level set's
+   domain identity (level_set.implement.h:356-380) with `smoothing`
+   (flsp_heaviside) over eps = 1.5 min_diameter; shares and rests of
+   magnitude <= DBL_EPSILON count as zero (numerics::is_zero).  values[i]
+   is material i's scalar, values[n] the background's.  out[k * npt + j]
+   = the mixed scalar at point j (x fastest) of host cell k (the first
+   handle's cell order), npt = n_qpts_1d^dim.  Every handle must be on the
+   same mesh (dim, cells, box) and device; degrees, bases and precisions
+   may differ.  The reference sums the shares in the order of its
+   material map; here they are summed in stack order, then the
+   background.                                                         */
+#define FLSP_MAX_MATERIALS 8
+#define FLSP_MAX_MIX_QPTS 8
+enum flsp_heaviside {
+  FLSP_HEAVISIDE_NONE = 0,    /* sharp: 1, 0, 1/2 at zero                */
+  FLSP_HEAVISIDE_LINEAR = 1,  /* linear ramp over [-eps, eps]            */
+  FLSP_HEAVISIDE_SINE = 2     /* sine smoothing (LevelSetControl default) */
+};
+int flsp_material_mix(flsp_handle* const* level_sets, int n, const double* values,
+                      int n_qpts_1d, int smoothing, double* out, int64_t n_out);
+
 /* Allocation-free reduction.  No counterpart in the reference: FELSPA
    computes these diagnostics on the host.  Same arithmetic as flsp_reduce,
    but for callers that cannot allocate device memory: host codes that own

@@ -1183,6 +1183,67 @@ static double heaviside_sine(double x, double eps) {
 }
 static double heaviside_sharp(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? 0.0 : 0.5); }
 
+// MaterialStack mixing: MaterialAccessor<MaterialStack>::reinit + eval_scalars
+// (include/felspa/level_set/src/material_stack.implement.h:320-470) with a
+// constant scalar per material.  Per QGauss(nq) point: proportion_sum = 1;
+// for each level set in stack order while proportion_sum is not zero,
+// heaviside = domain_identity(phi) = H(-phi) (level_set.implement.h:356-380,
+// smoothing over 1.5 min_diameter, :957-993); if it is not zero the
+// material takes proportion_sum * heaviside, which is subtracted; the
+// background takes a non-zero remainder; value = sum of value * proportion.
+static double mix_heaviside(double y, double eps, int kind) {
+  if (kind == FLSP_HEAVISIDE_NONE) return y > 0.0 ? 1.0 : (y < 0.0 ? 0.0 : 0.5);
+  if (kind == FLSP_HEAVISIDE_LINEAR) {
+    if (y > eps) return 1.0;
+    if (y < -eps) return 0.0;
+    return 0.5 * (y / eps + 1.0);
+  }
+  return heaviside_sine(y, eps);
+}
+
+int orc_material_mix(int n, orc_problem* const* prs, const double* const* phis, const double* values, int nq,
+                     int smoothing, const int64_t* order, double* out) {
+  if (n < 1 || !prs || !phis || !values || !out || nq < 1 || nq > 8) return FLSP_ERR_BAD_ARG;
+  const orc_problem* p0 = prs[0];
+  const int dim = p0->dim;
+  double xg[8], wg[8];
+  orc_gauss(nq, xg, wg);
+  const int npt = dim == 3 ? nq * nq * nq : nq * nq;
+  // shape values of every level set at the reference Gauss points
+  std::vector<std::vector<double>> sv(n);
+  for (int i = 0; i < n; ++i) {
+    sv[i].resize((size_t)prs[i]->nb * npt);
+    std::vector<double> gtmp((size_t)prs[i]->nb * 3);
+    for (int j = 0; j < npt; ++j) {
+      const double xi[3] = {xg[j % nq], xg[(j / nq) % nq], dim == 3 ? xg[j / (nq * nq)] : 0.0};
+      std::vector<double> val(prs[i]->nb);
+      shape_eval(prs[i], xi, val.data(), gtmp.data(), nullptr);
+      for (int b = 0; b < prs[i]->nb; ++b) sv[i][(size_t)b * npt + j] = val[b];
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (long k = 0; k < p0->ncell; ++k) {
+    const long c = order ? (long)order[k] : k;
+    for (int j = 0; j < npt; ++j) {
+      double rest = 1.0, v = 0.0;
+      for (int i = 0; i < n && !is_zero(rest); ++i) {
+        const orc_problem* pr = prs[i];
+        double phi = 0.0;
+        for (int b = 0; b < pr->nb; ++b) phi += phis[i][c * pr->nb + b] * sv[i][(size_t)b * npt + j];
+        const double H = mix_heaviside(-phi, 1.5 * pr->min_diam, smoothing);
+        if (!is_zero(H)) {
+          const double share = rest * H;
+          v += values[i] * share;
+          rest -= share;
+        }
+      }
+      if (!is_zero(rest)) v += values[n] * rest;
+      out[k * npt + j] = v;
+    }
+  }
+  return FLSP_OK;
+}
+
 int orc_reduce(orc_problem* pr, int which, const double* phi, const double* phi_ref,
                const flsp_ic_desc* ic, double* out) {
   const int nb = pr->nb, dim = pr->dim;

@@ -100,6 +100,11 @@ int orc_ls_advance(orc_problem* pr, double* phi, orc_clock* clk, int rk_order,
                    int single_step, double* advanced);
 
 /* reductions (flsp_reduce_kind) */
+/* MaterialStack mixing of constant material scalars at QGauss(nq) points
+   (as flsp_material_mix): out[k * nq^dim + j], k in the cell order
+   `order` (NULL: lexicographic) */
+int orc_material_mix(int n, orc_problem* const* prs, const double* const* phis, const double* values, int nq,
+                     int smoothing, const int64_t* order, double* out);
 int orc_reduce(orc_problem* pr, int which, const double* phi,
                const double* phi_ref, const flsp_ic_desc* ic, double* out);
 

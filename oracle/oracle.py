@@ -67,6 +67,8 @@ def lib():
         L.orc_ls_advance.argtypes = [C.c_void_p, _dp, C.POINTER(Clock), C.c_int, C.c_double,
                                      C.POINTER(abi.LSOpts), C.c_double, C.c_int, _dp]
         L.orc_reduce.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(abi.ICDesc), _dp]
+        L.orc_material_mix.argtypes = [C.c_int, C.POINTER(C.c_void_p), C.POINTER(_dp), _dp, C.c_int, C.c_int,
+                                       C.c_void_p, _dp]
         L.orc_mlp_forward.argtypes = [C.c_int, _ip, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp, _dp]
         L.orc_mlp_backward.argtypes = [C.c_int, _ip, C.POINTER(_dp), C.POINTER(_dp), C.c_int, _dp,
                                        _dp, C.POINTER(_dp), C.POINTER(_dp)]
@@ -242,6 +244,23 @@ class Problem:
         icd = C.byref(ic.desc()) if ic is not None else None
         _check(lib().orc_reduce(self.h, which, _p(phi), ref, icd, C.byref(out)), "reduce")
         return out.value
+
+
+def material_mix(problems, phis, values, nq, smoothing=abi.HEAVISIDE_SINE, order=None):
+    """MaterialStack mixing of constant scalars (stack order; values[-1] is
+    the background) at QGauss(nq) points: (n_cells, nq^dim)"""
+    n = len(problems)
+    prs = (C.c_void_p * n)(*[pr.h for pr in problems])
+    ph = [np.ascontiguousarray(p, dtype=np.float64) for p in phis]
+    php = (_dp * n)(*[_p(p) for p in ph])
+    vals = np.ascontiguousarray(values, dtype=np.float64)
+    o = np.ascontiguousarray(order, dtype=np.int64) if order is not None else None
+    npt = nq ** problems[0].dim
+    ncell = problems[0].n_dofs // problems[0].nb
+    out = np.zeros(ncell * npt)
+    _check(lib().orc_material_mix(n, prs, php, _p(vals), int(nq), int(smoothing),
+                                  o.ctypes.data_as(C.c_void_p) if o is not None else None, _p(out)), "material_mix")
+    return out.reshape(ncell, npt)
 
 
 def mlp_forward(Ws, bs, x):

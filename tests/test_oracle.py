@@ -357,3 +357,63 @@ def test_dirichlet_id_zero_and_unset_ids_are_neumann(oracle):
     assert np.array_equal(pr.advect_rhs(phi, 0.1), ref.advect_rhs(phi, 0.1))
     with pytest.raises(RuntimeError):
         pr.set_dirichlet(0, 1.0)
+
+
+# ----------------------------------------------------------------------
+# MaterialStack mixing
+# ----------------------------------------------------------------------
+def _gauss_points(oracle, dim, n, nq):
+    """physical coordinates (n_cells, nq^dim, dim) of QGauss(nq) on a
+    lexicographic n^dim mesh of the unit box, points x fastest"""
+    xg, _ = oracle.gauss(nq)
+    h = 1.0 / n
+    pts = []
+    for c in range(n ** dim):
+        I = [c % n, (c // n) % n, c // (n * n)][:dim]
+        cell = []
+        for j in range(nq ** dim):
+            q = [j % nq, (j // nq) % nq, j // (nq * nq)][:dim]
+            cell.append([(I[d] + xg[q[d]]) * h for d in range(dim)])
+        pts.append(cell)
+    return np.asarray(pts)
+
+
+def _hsine(y, eps):
+    return np.where(y > eps, 1.0, np.where(y < -eps, 0.0, 0.5 * (1 + y / eps + np.sin(np.pi * y / eps) / np.pi)))
+
+
+@pytest.mark.parametrize("smoothing", [abi.HEAVISIDE_NONE, abi.HEAVISIDE_LINEAR, abi.HEAVISIDE_SINE])
+def test_material_mix_known_answer(oracle, smoothing):
+    """two planes (exact in the degree-1 space) stacked over a background:
+    material 0 takes H0 = H(-(x - 0.45)), material 1 (1 - H0) H1 with
+    H1 = H(-(y - 0.55)), the background the rest"""
+    n, nq = 8, 3
+    pr0 = oracle.Problem(2, (n, n), 1, abi.BASIS_Q)
+    pr1 = oracle.Problem(2, (n, n), 2, abi.BASIS_P)
+    phi0 = pr0.project(F.height_function(0, 0.45, []))
+    phi1 = pr1.project(F.height_function(1, 0.55, []))
+    got = oracle.material_mix([pr0, pr1], [phi0, phi1], [3.0, -2.0, 0.5], nq, smoothing)
+    X = _gauss_points(oracle, 2, n, nq)
+    eps = 1.5 * math.sqrt(2.0) / n
+
+    def H(y):
+        if smoothing == abi.HEAVISIDE_NONE:
+            return np.where(y > 0, 1.0, np.where(y < 0, 0.0, 0.5))
+        if smoothing == abi.HEAVISIDE_LINEAR:
+            return np.clip(0.5 * (y / eps + 1), 0.0, 1.0)
+        return _hsine(y, eps)
+
+    h0 = H(-(X[..., 0] - 0.45))
+    h1 = H(-(X[..., 1] - 0.55))
+    want = 3.0 * h0 + (-2.0) * (1 - h0) * h1 + 0.5 * (1 - h0) * (1 - h1)
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
+def test_material_mix_partition_of_unity(oracle):
+    """equal values everywhere: the shares sum to one at every point"""
+    n = 10
+    prs = [oracle.Problem(2, (n, n), 2, abi.BASIS_Q) for _ in range(3)]
+    phis = [prs[0].project(F.zalesak_disk()), prs[1].project(F.sphere((0.3, 0.4), 0.2)),
+            prs[2].project(F.sphere((0.6, 0.6), 0.25))]
+    got = oracle.material_mix(prs, phis, [1.0, 1.0, 1.0, 1.0], 4)
+    assert np.max(np.abs(got - 1.0)) < 1e-14
