@@ -428,19 +428,9 @@ def run_ours(args):
                     "planes, seeds 5..13) advanced together, each reinit period (5 SSP-RK3 substeps + a fixed "
                     "5-pseudo-step plain reinit) of all 9 problems replayed from ONE CUDA graph (one branch per "
                     "problem); compared with the same periods replayed problem by problem",
-            **plume_group(periods=4)}
+            **plume_group(periods=40)}
         if not args.no_learned:
-            # the same group with the learned reinit every 5 steps (the 3D patch network)
-            from felspa_b200.learned import MLP, collect_training_pairs_3d
-            net3 = MLP(device=0, seed=7, dim=3)
-            collect_training_pairs_3d(net3, n=24, instances=8)
-            net3.train(steps=3000, batch=8192, lr=1e-3, seed=1)
-            line["variants"]["plume_group_learned"] = {
-                "what": "the plume group with the learned reinit every 5 steps (the 3x3x3-patch network, "
-                        "trained here on 24^3 sphere / plume pairs; no fallback), all 9 problems in one graph per "
-                        "period",
-                **plume_group(periods=4, net=net3)}
-            net3.close()
+            line["variants"]["plume_group_learned"] = plume_group_learned()
     if world == 1 and not args.no_batched:
         from felspa_b200.batch import uneven_batch_benchmark
         r = uneven_batch_benchmark()
@@ -537,6 +527,45 @@ def zalesak_accuracy(device):
     return out
 
 
+def plume_group_learned():
+    """The large 3D production configuration as specified: the 128^3 Q2
+    plume problem with 8 side 64^3 problems in one graph per period, 2000
+    SSP-RK3 steps, the learned reinit (3x3x3-patch network, trained here)
+    every 5 steps with its residual fallback decided on the device; FP32,
+    and the same run in FP64 for its accuracy (L1 interface difference and
+    volume of every problem)."""
+    from felspa_b200 import abi
+    from felspa_b200.batch import plume_group
+    from felspa_b200.learned import MLP, collect_training_pairs_3d
+    from felspa_b200.level_set import Mesh, Problem
+    net3 = MLP(device=0, seed=7, dim=3)
+    collect_training_pairs_3d(net3, n=24, instances=8)
+    net3.train(steps=3000, batch=8192, lr=1e-3, seed=1)
+    r32 = plume_group(periods=400, net=net3, states=True)
+    r64 = plume_group(periods=400, net=net3, precision=abi.FP64, timed=False, states=True)
+    net3.close()
+    s32, s64 = r32.pop("states"), r64.pop("states")
+    l1, dmax = [], []
+    for i, (a, b) in enumerate(zip(s32, s64)):
+        n = 128 if i == 0 else 64
+        pb = Problem(Mesh(3, (n, n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP64)
+        pb.set_state(b)
+        pb.snapshot()
+        pb.set_state(a)
+        l1.append(pb.reduce(abi.RED_L1_INTERFACE))
+        pb.close()
+        dmax.append(float(np.abs(a - b).max() / np.abs(b).max()))
+    return {"what": "the large 3D production configuration: 128^3 Q2 FP32 plume problem + 8 x 64^3 side problems in "
+                    "one graph per period, 2000 SSP-RK3 steps, learned reinit every 5 steps (3x3x3-patch network "
+                    "trained here on 24^3 sphere / plume pairs) with its residual fallback decided on the device",
+            **r32,
+            "fp64": {"dof_steps_per_s": r64["dof_steps_per_s"], "max_volume_change": r64["max_volume_change"],
+                     "fallback_fraction": r64.get("fallback_fraction")},
+            "fp32_vs_fp64": {"l1_interface_diff": l1, "max_coeff_diff_rel": dmax,
+                             "volume_change_fp32_minus_fp64": [x - y for x, y in zip(r32["volume_change"],
+                                                                                      r64["volume_change"])]}}
+
+
 def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=0, band_cells=6.0):
     """DoF-steps/s (device time, CUDA events on the library stream) of `periods`
     reinit periods (10 SSP-RK3 steps + 5 fixed pseudo-steps) of a 3D Q2 problem."""
@@ -571,37 +600,51 @@ def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=
 
 
 def learned_comparison():
-    """Learned (tensor-core MLP) vs plain HJ reinitialisation on the 2D
-    degree-2 slotted-disk revolution; the network is trained here, on the
-    GPU, on pairs produced by the plain sweep."""
-    from felspa_b200.learned import learned_vs_plain
-    r = learned_vs_plain(n=256, instances=32, train_steps=12000)
-    runs = {}
-    for x in r["runs"]:
-        key = x["method"]
-        if key == "plain" and x.get("graph_replay"):
-            key = "plain_graph"
-        elif key == "learned" and x.get("graph_replay"):
-            key = "learned_graph_no_fallback"
-        elif key == "learned" and x.get("max_residual", 0) > 1e6:
-            key = "learned_no_fallback"
-        runs[key] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in x.items()
-                     if k not in ("method", "mesh", "graph_replay")}
-    best_plain = max(runs["plain"]["dof_steps_per_s"], runs["plain_graph"]["dof_steps_per_s"])
-    return {
-        "workload": "2D degree-2 Q slotted disk (centre (0.5,0.75), r 0.15, slot 0.05x0.25), 256^2, one CCW "
-                    "revolution, CFL 0.1, FP32, reinit every 40 steps; L1 interface error and area change vs "
-                    "the initial shape; wall clock of the whole run",
-        "plain_reinit": "reference LF HJ sweep, 5 fixed pseudo-steps, LDG viscosity 1e-3, CFL 0.1",
-        "learned_reinit": "MLP 82-256x4-9 (BF16 tcgen05) over the 6-cell band; fallback = the plain sweep "
-                          "restricted to the band, for cells with mean ||grad phi|-1| > 0.05",
-        "training": {k: (round(v, 8) if isinstance(v, float) else v) for k, v in r["training"].items()},
-        "runs": runs,
-        "learned_vs_best_plain_speed": runs["learned"]["dof_steps_per_s"] / best_plain,
-        "learned_no_fallback_vs_best_plain_speed": runs["learned_no_fallback"]["dof_steps_per_s"] / best_plain,
-        "learned_graph_no_fallback_vs_best_plain_speed":
-            runs["learned_graph_no_fallback"]["dof_steps_per_s"] / best_plain,
+    """Learned (tensor-core MLP) vs plain HJ reinitialisation at equal L1
+    interface error (2D degree-2): the network is trained here, on the GPU,
+    on pairs produced by the plain sweep; then for each workload and reinit
+    interval the plain sweep, the learned reinit with its residual fallback
+    (decided on the device) and without, every run replayed from CUDA
+    graphs; speed-ups read off the (L1, rate) fronts at the plain runs' L1."""
+    import time
+    from felspa_b200 import fields as F
+    from felspa_b200.learned import MLP, collect_training_pairs, equal_l1_study
+    t0 = time.perf_counter()
+    net = MLP(device=0, seed=7)
+    n_pairs = collect_training_pairs(net, n=256, instances=32)
+    t1 = time.perf_counter()
+    loss0 = net.eval()
+    last = net.train(steps=12000, batch=8192, lr=1e-3, seed=1)
+    t2 = time.perf_counter()
+    loss1 = net.eval()
+    workloads = {
+        "zalesak_rotation": (F.ccw_rotation(), F.zalesak_disk(), 1.0),
+        "zalesak_vortex_T2": (F.single_vortex(period=2.0), F.zalesak_disk(), 2.0),
     }
+    study = equal_l1_study(net, workloads, n=256)
+    net.close()
+
+    def slim(r):
+        return {k: (round(v, 6) if isinstance(v, float) else v) for k, v in r.items()
+                if k not in ("method", "t", "device_s", "steps")}
+
+    out = {
+        "workload": "2D degree-2 Q, 256^2, FP32, CFL 0.1: the slotted disk (centre (0.5,0.75), r 0.15, slot "
+                    "0.05x0.25) over one CCW rotation (T = 1) and through the time-reversed single vortex "
+                    "(period 2, t = 2); L1 interface error and area change vs the initial shape; device time",
+        "plain_reinit": "reference LF HJ sweep over every cell, 5 fixed pseudo-steps, LDG viscosity 1e-3, CFL 0.1",
+        "learned_reinit": "MLP 82-256x4-9 (BF16 tcgen05) over the 6-cell band; fallback (max_residual 0.05): cells "
+                          "with mean ||grad phi|-1| > 0.05 take the plain sweep run over them, decided on the device",
+        "training": {"pairs": n_pairs, "collect_s": round(t1 - t0, 3), "steps": 12000, "batch": 8192,
+                     "train_s": round(t2 - t1, 3), "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},
+    }
+    for name, r in study.items():
+        out[name] = {"steps": r["steps"], "none": slim(r["runs"]["none"]),
+                     "plain": [slim(x) for x in r["runs"]["plain"]],
+                     "learned": [slim(x) for x in r["runs"]["learned"]],
+                     "learned_no_fallback": [slim(x) for x in r["runs"]["learned_no_fallback"]],
+                     "equal_l1": r["equal_l1"]}
+    return out
 
 
 def learned_comparison_3d():

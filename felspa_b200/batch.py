@@ -210,26 +210,31 @@ class Group:
         return s.value
 
 
-def plume_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_pseudo=5, degree=2, net=None):
-    """The large 3D configuration's structure: a main n_main^3 Q2 FP32 problem
-    and n_sides n_side^3 side problems (plume rolls u = curl(0, psi, 0),
+def plume_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_pseudo=5, degree=2, net=None,
+                fallback=True, precision=abi.FP32, timed=True, states=False):
+    """The large 3D configuration's structure: a main n_main^3 Q2 problem and
+    n_sides n_side^3 side problems (plume rolls u = curl(0, psi, 0),
     perturbed-plane ICs with seeds 5, 6, ...), one graph per reinit period
     (reinit_every SSP-RK3 substeps + a fixed n_pseudo-step reinit) covering
     every problem.  Returns DoF-steps/s over all problems (device time, CUDA
-    events on the group's stream) and the same periods with each problem
-    replayed alone, one after the other.  With `net` (the 3D patch network)
-    the reinit is the learned one instead (no fallback) and there is no
-    one-by-one comparison; the largest volume change over the problems is
-    reported either way."""
+    events on the group's stream) and, for the plain reinit, the same
+    periods with each problem replayed alone, one after the other.  With
+    `net` (the 3D patch network) the reinit is the learned one, with its
+    residual fallback decided on the device unless fallback=False.  The
+    largest volume change over the problems is reported; states=True also
+    returns every problem's final state (host order, FP64)."""
     import torch
-    from .learned import default_learned_opts
+    from .learned import default_learned_opts, plain_reinit_opts
     ctl = abi.default_ls_opts(reinit_frequency=reinit_every,
                               reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=n_pseudo))
-    lo = default_learned_opts()
+    lo = default_learned_opts(max_residual=0.05 if fallback else float("inf"))
+    lo.fallback = abi.ReinitOpts.from_buffer_copy(plain_reinit_opts())
+    lo.fallback.narrow_band = 1
+    lo.fallback.band_cells = lo.band_cells
     sizes = [n_main] + [n_side] * n_sides
     probs, vol0 = [], []
     for i, n in enumerate(sizes):
-        pb = Problem(Mesh(3, (n, n, n)), degree, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
+        pb = Problem(Mesh(3, (n, n, n)), degree, basis=abi.BASIS_Q, precision=precision, cfl_max=0.1)
         pb.set_velocity(F.plume_3d())
         pb.project(F.perturbed_plane(seed=5 + i))
         vol0.append(pb.reduce(abi.RED_MASS_SHARP))
@@ -242,25 +247,32 @@ def plume_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_p
         else:
             g.run_periods_learned(net, lo, reinit_every, n_periods, sync=sync)
 
-    run(1)                           # warm-up period (captures the graph)
+    run(1)                           # first period (captures the graph)
     s = torch.cuda.ExternalStream(g.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(s)
-    run(periods, sync=False)
+    run(periods - 1, sync=False)
     e1.record(s)
     e1.synchronize()
     ms_group = e0.elapsed_time(e1)
     g.sync()
     finite = all(bool(np.all(np.isfinite(p.get_state()))) for p in probs)
-    dvol = max(abs(p.reduce(abi.RED_MASS_SHARP) - v) / v for p, v in zip(probs, vol0))
+    dvol = [abs(p.reduce(abi.RED_MASS_SHARP) - v) / v for p, v in zip(probs, vol0)]
     n_dofs = g.n_dofs
     g.close()
-    steps = periods * reinit_every
-    out = {"n_dofs": n_dofs, "problems": len(sizes), "periods": periods, "device_ms": ms_group,
+    steps = (periods - 1) * reinit_every
+    out = {"n_dofs": n_dofs, "problems": len(sizes), "periods": periods, "steps": periods * reinit_every,
+           "timed_steps": steps, "device_ms": ms_group,
            "dof_steps_per_s": n_dofs * steps / (ms_group * 1e-3), "finite": finite,
-           "max_volume_change": dvol, "reinit": "learned (no fallback)" if net is not None else "plain"}
-    if net is None:
+           "max_volume_change": max(dvol), "volume_change": dvol,
+           "reinit": ("learned" + (" with the device-side fallback" if fallback else " (no fallback)"))
+           if net is not None else "plain"}
+    if net is not None:
+        tot = [p.learned_totals() for p in probs]
+        nb, nf = sum(t[0] for t in tot), sum(t[1] for t in tot)
+        out["fallback_fraction"] = nf / nb if (nb and fallback) else None
+    if net is None and timed:
         # the same periods, each problem alone (its own graph), one after the other
         ms_alone = 0.0
         for pb in probs:
@@ -269,11 +281,13 @@ def plume_group(n_main=128, n_side=64, n_sides=8, periods=4, reinit_every=5, n_p
             st = torch.cuda.ExternalStream(pb.stream())
             torch.cuda.synchronize()
             e0.record(st)
-            check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), periods * reinit_every))
+            check(load().flsp_ls_run_steps(pb.h, C.byref(ctl), steps))
             e1.record(st)
             e1.synchronize()
             ms_alone += e0.elapsed_time(e1)
         out["one_after_another_dof_steps_per_s"] = n_dofs * steps / (ms_alone * 1e-3)
+    if states:
+        out["states"] = [p.get_state() for p in probs]
     for pb in probs:
         pb.close()
     return out

@@ -21,10 +21,12 @@
 //
 // The CTA's halo box (one bulk copy per row of cells, each row keeping its
 // 16-byte phase from HBM so that 27-value cells need no splitting) and its
-// operator rows arrive by TMA bulk copies on one mbarrier; the RK
-// combination is fused into a coalesced store that prefetches phi^n into
-// registers (float4 rows where FP32 alignment allows).  Tile shapes are
-// compile-time.
+// operator rows arrive by TMA bulk copies on one mbarrier.  Every face of
+// the tile is then one work item of a single routine (runtime axis), its
+// flux kept in shared memory; each cell adds its cell term and lifts its
+// faces' fluxes; the RK combination is fused into a coalesced store that
+// prefetches phi^n into registers (float4 rows where FP32 alignment
+// allows).  Tile shapes are compile-time.
 //
 // The per-axis operators are tabulated once per velocity on the host in
 // FP64 (optab, one row per component d, axis e and cell index i:
@@ -66,33 +68,6 @@ struct AdvSepArgs {
   double ct_explicit;
   double dt_explicit;
 };
-
-// In-cell DoF index (HBM order) of Q-layout mode q (a + N1 b + N1^2 c):
-// itself for FE_DGQLegendre, the PolynomialSpace position (c outer, b,
-// a inner, a + b + c <= P) for FE_DGP, -1 for a mode outside P-space.
-template <int DIM, int P, bool PB>
-__host__ __device__ constexpr int q2g_c(int q) {
-  const int N1 = P + 1;
-  const int a = q % N1, b = (q / N1) % N1, c = DIM > 2 ? q / (N1 * N1) : 0;
-  if (!PB) return q;
-  if (a + b + c > P) return -1;
-  int idx = 0;
-  for (int cc = 0; cc < c; ++cc)
-    for (int bb = 0; bb <= P - cc; ++bb) idx += P - bb - cc + 1;
-  for (int bb = 0; bb < b; ++bb) idx += P - bb - c + 1;
-  return idx + a;
-}
-
-// a cell's coefficients from its box copy (HBM order) in the Q layout
-template <int DIM, int P, bool PB, typename T>
-__device__ __forceinline__ void load_cell(const T* __restrict__ src, T* cq) {
-  constexpr int NM = ipow(P + 1, DIM);
-#pragma unroll
-  for (int q = 0; q < NM; ++q) {
-    const int gi = q2g_c<DIM, P, PB>(q);
-    cq[q] = gi >= 0 ? src[gi] : T(0);
-  }
-}
 
 // Shared-memory plan of the separable stage kernel for a compile-time tile
 // TX x TY x TZ (TZ = 1 in 2D): mbarrier | halo box rows | operator rows |
@@ -146,42 +121,6 @@ __device__ __forceinline__ void load_op(const T* __restrict__ src, T (&M)[N1][N1
   for (int a = 0; a < N1; ++a)
 #pragma unroll
     for (int b = 0; b < N1; ++b) M[a][b] = v[a * N1 + b];
-}
-
-// R += s * (M0 (x) M1 (x) M2) x, Q layout (index a0 + N1 a1 + N1^2 a2),
-// contracted one z-slab of x at a time to keep the partial sums small
-template <int DIM, int N1, typename T>
-__device__ __forceinline__ void apply_sep_acc(const T (&M0)[N1][N1], const T (&M1)[N1][N1],
-                                              const T (&M2)[N1][N1], const T* x, T* R, T s) {
-  constexpr int NZ = DIM > 2 ? N1 : 1;
-#pragma unroll
-  for (int b2 = 0; b2 < NZ; ++b2) {
-    T u[N1][N1];   // [a0][b1]
-#pragma unroll
-    for (int a0 = 0; a0 < N1; ++a0)
-#pragma unroll
-      for (int b1 = 0; b1 < N1; ++b1) {
-        T acc = T(0);
-#pragma unroll
-        for (int b0 = 0; b0 < N1; ++b0) acc += M0[a0][b0] * x[b0 + N1 * (b1 + N1 * b2)];
-        u[a0][b1] = acc;
-      }
-#pragma unroll
-    for (int a1 = 0; a1 < N1; ++a1)
-#pragma unroll
-      for (int a0 = 0; a0 < N1; ++a0) {
-        T acc = T(0);
-#pragma unroll
-        for (int b1 = 0; b1 < N1; ++b1) acc += M1[a1][b1] * u[a0][b1];
-        if constexpr (DIM == 2) {
-          R[a0 + N1 * a1] += s * acc;
-        } else {
-          const T v = s * acc;
-#pragma unroll
-          for (int a2 = 0; a2 < N1; ++a2) R[a0 + N1 * (a1 + N1 * a2)] += M2[a2][b2] * v;
-        }
-      }
-  }
 }
 
 // F = s1 (A0 (x) A1) S + s2 (B0 (x) B1) D on the face modes (m0 + N1 m1);
@@ -245,26 +184,109 @@ __device__ __forceinline__ void face_apply(const T* __restrict__ rowA0, const T*
   (void)NF;
 }
 
-// trace of the cell polynomial on the face normal to E, in face modes
-template <int DIM, int N1, int E, typename T>
-__device__ __forceinline__ void face_trace(const T* c, const T* Lside, T* tr) {
-  constexpr int NF = DIM > 2 ? N1 * N1 : N1;
-  constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-  constexpr int st[3] = {1, N1, N1 * N1};
+// trace of a box cell (HBM order) on its face normal to the runtime axis E
+// (side values Ls = L(0) or L(1)), in face modes; the P basis reads its
+// modes through the Q-layout map
+template <int DIM, int P, bool PB, typename T>
+__device__ __forceinline__ void face_trace_rt(const T* __restrict__ src, int E, const T* Ls,
+                                              const signed char* q2g, T* tr) {
+  constexpr int N1 = P + 1, NF = DIM > 2 ? N1 * N1 : N1;
+  const int sE = E == 0 ? 1 : (E == 1 ? N1 : N1 * N1);   // stride of axis E
+  const int s0 = E == 0 ? N1 : 1;                        // first tangential axis
+  const int s1 = E == 2 ? N1 : N1 * N1;                  // second (3D)
 #pragma unroll
   for (int mf = 0; mf < NF; ++mf) {
     const int m0 = mf % N1, m1 = mf / N1;
-    const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
+    const int base = m0 * s0 + (DIM > 2 ? m1 * s1 : 0);
     T s = T(0);
 #pragma unroll
-    for (int a = 0; a < N1; ++a) s += Lside[a] * c[base + a * st[E]];
+    for (int aa = 0; aa < N1; ++aa) {
+      const int q = base + aa * sE;
+      if constexpr (PB) {
+        const int gi = q2g[q];
+        if (gi >= 0) s += Ls[aa] * src[gi];
+      } else {
+        s += Ls[aa] * src[q];
+      }
+    }
     tr[mf] = s;
   }
 }
 
+// R += s (M0 (x) M1 (x) M2) c with the cell's coefficients read from its
+// box copy one z-slab at a time (Q layout; the P basis through q2g)
+template <int DIM, int P, bool PB, typename T>
+__device__ __forceinline__ void apply_sep_box(const T (&M0)[P + 1][P + 1], const T (&M1)[P + 1][P + 1],
+                                              const T* __restrict__ m2row, const T* __restrict__ src,
+                                              const signed char* q2g, T* R, T s) {
+  constexpr int N1 = P + 1, NZ = DIM > 2 ? N1 : 1;
+#pragma unroll
+  for (int b2 = 0; b2 < NZ; ++b2) {
+    T x[N1][N1];   // [b1][b0]
+#pragma unroll
+    for (int b1 = 0; b1 < N1; ++b1)
+#pragma unroll
+      for (int b0 = 0; b0 < N1; ++b0) {
+        const int q = b0 + N1 * (b1 + N1 * b2);
+        if constexpr (PB) {
+          const int gi = q2g[q];
+          x[b1][b0] = gi >= 0 ? src[gi] : T(0);
+        } else {
+          x[b1][b0] = src[q];
+        }
+      }
+    T u[N1][N1];   // [a0][b1]
+#pragma unroll
+    for (int a0 = 0; a0 < N1; ++a0)
+#pragma unroll
+      for (int b1 = 0; b1 < N1; ++b1) {
+        T acc = T(0);
+#pragma unroll
+        for (int b0 = 0; b0 < N1; ++b0) acc += M0[a0][b0] * x[b1][b0];
+        u[a0][b1] = acc;
+      }
+    T m2c[N1];   // column b2 of M2
+    if constexpr (DIM > 2) {
+#pragma unroll
+      for (int a2 = 0; a2 < N1; ++a2) m2c[a2] = m2row[a2 * N1 + b2];
+    }
+#pragma unroll
+    for (int a1 = 0; a1 < N1; ++a1)
+#pragma unroll
+      for (int a0 = 0; a0 < N1; ++a0) {
+        T acc = T(0);
+#pragma unroll
+        for (int b1 = 0; b1 < N1; ++b1) acc += M1[a1][b1] * u[a0][b1];
+        const T v = s * acc;
+        if constexpr (DIM == 2) {
+          R[a0 + N1 * a1] += v;
+        } else {
+#pragma unroll
+          for (int a2 = 0; a2 < N1; ++a2) R[a0 + N1 * (a1 + N1 * a2)] += m2c[a2] * v;
+        }
+      }
+  }
+}
+
+// Dirichlet value on the domain-boundary face on side S of axis E of the
+// cell (gx, gy, gz) (bc_dirichlet with the coordinates as scalars)
+template <int DIM, typename T>
+__device__ __forceinline__ bool bc_dirichlet_at(const MeshArgs& m, int E, int S, int gx, int gy, int gz, T& g) {
+  const int c[3] = {gx, gy, gz};
+  return bc_dirichlet<DIM>(m, E, S, c, g);
+}
+
 // FP32 tiles fit two CTAs per SM (<= 128 registers); an FP64 tile takes most
-// of an SM's shared memory, so FP64 gets the full register file
-template <int DIM, int P, bool PB, int TX, int TY, int TZ, typename T>
+// of an SM's shared memory, so FP64 gets the full register file.
+//
+// Phases: (1) every face of the tile (interior, tile boundary, domain
+// boundary) is a work item with a runtime axis: traces of its two box
+// cells, the separable upwind flux, written to the face's slot, so each
+// face's flux is computed once per CTA by one routine whatever the tiling;
+// (2) every cell: the cell term (one direction at a time) and the lifting of
+// its 2 dim face fluxes from the slots; (3) the RK combination fused into
+// the coalesced store.  BC: the mesh may carry Dirichlet faces.
+template <int DIM, int P, bool PB, int TX, int TY, int TZ, typename T, bool BC>
 __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
     adv_sep_kernel(const AdvSepArgs<T> a) {
   using PL = SepPlan<DIM, P, PB, TX, TY, TZ, T>;
@@ -272,9 +294,6 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
   constexpr int NBG = PL::NBG;
   constexpr int NT = PL::NT, NMB = PL::NMB, SPAN = PL::SPAN;
   constexpr int TL[3] = {TX, TY, TZ};
-  constexpr int ROFF[3] = {0, TX, TX + TY};            // first row of each axis within a component
-  constexpr int FLO[3] = {0, NF * PL::SL0, NF * (PL::SL0 + PL::SL1)};
-  constexpr int SLN[3] = {PL::SL0, PL::SL1, PL::SL2};
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw);
   unsigned char* boxb = smem_raw + PL::OFF_BOX;
@@ -300,6 +319,11 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
     const unsigned rowcell = (unsigned)m.n[0] * (unsigned)((oy + ly) + m.n[1] * (DIM > 2 ? oz + lz : 0));
     const unsigned phase = ((rowcell + (unsigned)gx0) * (unsigned)NMB) & 15u;
     return reinterpret_cast<const T*>(boxb + (size_t)rr * PL::SLOT + phase + (ox + lx - gx0) * NMB);
+  };
+  // operator row of component d, axis e, tile cell le along e
+  auto rowp = [&](int d, int e, int le) -> const T* {
+    const int roff = e == 0 ? 0 : (e == 1 ? TX : TX + TY);
+    return ops + (size_t)(d * SPAN + roff + le) * OPW;
   };
 
   // ---- staging: box rows and operator rows by bulk copies (warp 0)
@@ -334,9 +358,7 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
         const int o = e == 0 ? ox : (e == 1 ? oy : oz);
         const unsigned nbytes = (unsigned)(TL[e] * OPW * sizeof(T));
         if (pass == 0) bytes += nbytes;
-        else
-          bulk_g2s(ops + (size_t)(d * SPAN + ROFF[e]) * OPW,
-                   a.optab + ((size_t)(d * 3 + e) * a.nmax + o) * OPW, nbytes, bar);
+        else bulk_g2s(const_cast<T*>(rowp(d, e, 0)), a.optab + ((size_t)(d * 3 + e) * a.nmax + o) * OPW, nbytes, bar);
       }
     }
   }
@@ -351,168 +373,113 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
   const int cl = threadIdx.x;
   const T ih[3] = {T(1.0 / m.h[0]), T(1.0 / m.h[1]), T(DIM > 2 ? 1.0 / m.h[2] : 1.0)};
   const bool work = valid && active;
+  constexpr int SL[3] = {PL::SL0, PL::SL1, PL::SL2};
+  constexpr int FLO[3] = {0, NF * PL::SL0, NF * (PL::SL0 + PL::SL1)};
 
-  auto rowp = [&](int d, int e, int le) -> const T* {
-    return ops + (size_t)(d * SPAN + ROFF[e] + le) * OPW;
-  };
-  // face-flux slot of the face below local cell lc along E (lc[E] in [0, TL[E]])
-  auto slot = [&](auto EC, const int* lc) -> int {
-    constexpr int E = decltype(EC)::value;
-    constexpr int e0 = TX + (E == 0), e1 = TY + (E == 1);
-    return lc[0] + e0 * (lc[1] + (DIM > 2 ? e1 * lc[2] : 0));
-  };
-  auto flux_at = [&](auto EC, int mf, int sl) -> T& {
-    constexpr int E = decltype(EC)::value;
-    return fl[FLO[E] + mf * SLN[E] + sl];
-  };
-
-  // flux through the face normal to E in +e_E between the lower cell (L1
-  // trace of the box copy cm) and the upper cell (L0 trace of the box copy
-  // cp); on the domain boundary the missing side's trace is the Dirichlet
-  // value gd (constant mode only) where the face carries one (dir), else
-  // the other side's (own) trace, zero-Neumann.  Tangential operator rows
-  // at local coordinates lc, g_EE at the face = fe.
-  auto face_flux_sep = [&](auto EC, const T* cm, const T* cp, bool has_m, bool has_p, const int* lc,
-                           T fe, T* F, bool dir, T gd) {
-    constexpr int E = decltype(EC)::value;
-    constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-    // traces straight from the box copies (Q layout), or through the
-    // P-space expansion
-    auto trace = [&](const T* src, const T* Ls, T* tr) {
-      if constexpr (PB) {
-        T cq[NM];
-        load_cell<DIM, P, PB, T>(src, cq);
-        face_trace<DIM, N1, E, T>(cq, Ls, tr);
-      } else {
-        face_trace<DIM, N1, E, T>(src, Ls, tr);
-      }
-    };
-    const T s1 = ct * fe;
-    const T* r0 = rowp(E, t0, lc[t0]);
-    const T* r1 = DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr;
-    // tangential factors of one sign over the face: |u_E| = sigma u_E, so
-    // B = sigma A and the flux is u_E times the upwind trace alone
-    const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
-    if (sigma != T(0)) {
-      // upwind side: the lower cell where u_E > 0; a missing side takes the
-      // Dirichlet value or, without one, the other side (own trace)
-      const bool flow_up = s1 * sigma > T(0);
-      T W[NF];
-      if (dir && !(flow_up ? has_m : has_p)) {
-#pragma unroll
-        for (int mf = 0; mf < NF; ++mf) W[mf] = mf == 0 ? gd : T(0);
-      } else {
-        const bool up_m = flow_up ? has_m : !has_p;
-        trace(up_m ? cm : cp, up_m ? tb.L1 : tb.L0, W);
-      }
-      face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
-      return;
-    }
-    T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
-    if (has_m) trace(cm, tb.L1, S);
-    if (has_p) trace(cp, tb.L0, D);
-#pragma unroll
-    for (int mf = 0; mf < NF; ++mf) {
-      const T ghost = dir ? (mf == 0 ? gd : T(0)) : T(0);
-      const T tm = has_m ? S[mf] : (dir ? ghost : D[mf]), tp = has_p ? D[mf] : (dir ? ghost : S[mf]);
-      S[mf] = T(0.5) * (tm + tp);
-      D[mf] = T(0.5) * (tm - tp);
-    }
-    face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, (has_m && has_p) || dir, F);
-  };
-
-  T R[NM];
-#pragma unroll
-  for (int q = 0; q < NM; ++q) R[q] = T(0);
-
-  if (work) {
-    const T* cme = cellp(l[0], l[1], l[2]);
-    {
-      T c[NM];
-      load_cell<DIM, P, PB, T>(cme, c);
-      // ============================ cell term ============================
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        T M0[N1][N1], M1[N1][N1], M2[N1][N1];
-        load_op<N1, T>(rowp(d, 0, l[0]), M0);
-        load_op<N1, T>(rowp(d, 1, l[1]), M1);
-        if constexpr (DIM > 2) load_op<N1, T>(rowp(d, 2, l[2]), M2);
-        apply_sep_acc<DIM, N1, T>(M0, M1, M2, c, R, ct * ih[d]);
-      }
-    }
-    // ===== upper faces: own flux, shared with the upper neighbour via slot l[E] + 1
-    auto do_upper = [&](auto EC) {
-      constexpr int E = decltype(EC)::value;
-      int nl[3] = {l[0], l[1], l[2]};
-      nl[E] += 1;
-      const bool has_nb = g[E] + 1 < m.n[E];
-      const T* cn = cellp(nl[0], nl[1], nl[2]);
-      T F[NF];
-      T gd = T(0);
-      const bool dir = !has_nb && bc_dirichlet<DIM>(m, E, 1, g, gd);
-      face_flux_sep(EC, cme, cn, true, has_nb, l, rowp(E, E, l[E])[BOFF + 1], F, dir, gd);
-      scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
-      const int sl = slot(EC, nl);
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) flux_at(EC, mf, sl) = F[mf];
-    };
-    do_upper(std::integral_constant<int, 0>());
-    do_upper(std::integral_constant<int, 1>());
-    if constexpr (DIM == 3) do_upper(std::integral_constant<int, 2>());
-  }
-
-  // ===== the tile's lower boundary faces (slot 0 of every line), as work
-  // items; axis E's items start at a warp boundary so that a warp serves
-  // one axis
+  // ===== (1) face fluxes, one work item per face of the tile
   if (active) {
-    constexpr int NI0 = NT / TX, NI1 = NT / TY, NI2 = DIM > 2 ? NT / TZ : 0;
-    constexpr int IB1 = (NI0 + 31) & ~31, IB2 = IB1 + ((NI1 + 31) & ~31);
-    constexpr int TOT = IB2 + ((NI2 + 31) & ~31);
-    constexpr int NIT[3] = {NI0, NI1, NI2}, IBS[3] = {0, IB1, IB2};
+    constexpr int TOT = PL::SL0 + PL::SL1 + PL::SL2;
     for (int it = threadIdx.x; it < TOT; it += NT) {
-      auto do_item = [&](auto EC) {
-        constexpr int E = decltype(EC)::value;
-        const int k = it - IBS[E];
-        if (k < 0 || k >= NIT[E]) return;
-        // tile cell with local coordinate 0 along E; the others from k
-        constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-        int lc[3] = {0, 0, 0};
-        lc[t0] = k % TL[t0];
-        if (DIM > 2) lc[t1] = k / TL[t0];
-        const int gc[3] = {ox + lc[0], oy + lc[1], oz + lc[2]};
-        if (gc[0] >= m.n[0] || gc[1] >= m.n[1] || (DIM > 2 && gc[2] >= m.n[2])) return;
-        int ll[3] = {lc[0], lc[1], lc[2]};
-        ll[E] -= 1;
-        const bool has_m = gc[E] > 0;
-        const T* cp = cellp(lc[0], lc[1], lc[2]);
-        const T* cm = cellp(ll[0], ll[1], ll[2]);
-        T F[NF];
-        T gd = T(0);
-        const bool dir = !has_m && bc_dirichlet<DIM>(m, E, 0, gc, gd);
-        face_flux_sep(EC, cm, cp, has_m, true, lc, rowp(E, E, 0)[BOFF], F, dir, gd);
-        const int sl = slot(EC, lc);
+      const int E = it < SL[0] ? 0 : (it < SL[0] + SL[1] ? 1 : 2);
+      const int r = it - (E == 0 ? 0 : (E == 1 ? SL[0] : SL[0] + SL[1]));
+      const int tE = E == 0 ? TX : (E == 1 ? TY : TZ);
+      const int t0l = E == 0 ? TY : TX;   // tile cells along the first tangential axis
+      const int f = r % (tE + 1), rest = r / (tE + 1);
+      const int u0 = rest % t0l, u1 = DIM > 2 ? rest / t0l : 0;
+      // local coordinates of the face's upper cell (f along E)
+      const int lx = E == 0 ? f : u0;
+      const int ly = E == 1 ? f : (E == 0 ? u0 : u1);
+      const int lz = E == 2 ? f : u1;
+      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
+      const int gE = E == 0 ? gx : (E == 1 ? gy : gz);
+      const int nE = m.n[E];
+      if (E != 0 && gx >= m.n[0]) continue;
+      if (E != 1 && gy >= m.n[1]) continue;
+      if (DIM > 2 && E != 2 && gz >= m.n[2]) continue;
+      const bool has_m = gE >= 1 && gE - 1 < nE, has_p = gE < nE;
+      if (!has_m && !has_p) continue;
+      const T* cp = cellp(lx, ly, lz);
+      const T* cm = cellp(lx - (E == 0), ly - (E == 1), lz - (E == 2));
+      T gd = T(0);
+      bool dir = false;
+      if constexpr (BC) {
+        if (!has_m) dir = bc_dirichlet_at<DIM>(m, E, 0, gx, gy, gz, gd);
+        else if (!has_p) dir = bc_dirichlet_at<DIM>(m, E, 1, gx - (E == 0), gy - (E == 1), gz - (E == 2), gd);
+      }
+      // tangential operator rows and the normal factor g_EE at the face
+      // (the upper cell's xi = 0 value, or the last tile cell's xi = 1 one:
+      // the same number, tabulated from one expression)
+      const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+      const T* r0 = rowp(E, t0, u0);
+      const T* r1 = DIM > 2 ? rowp(E, t1, u1) : nullptr;
+      const T fe = f < tE ? rowp(E, E, f)[BOFF] : rowp(E, E, tE - 1)[BOFF + 1];
+      const T s1 = ct * fe;
+      T F[NF];
+      // tangential factors of one sign over the face: |u_E| = sigma u_E, so
+      // the flux is u_E times the upwind trace alone
+      const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
+      if (sigma != T(0)) {
+        const bool flow_up = s1 * sigma > T(0);   // upwind: the lower cell
+        T W[NF];
+        if (dir && !(flow_up ? has_m : has_p)) {
 #pragma unroll
-        for (int mf = 0; mf < NF; ++mf) flux_at(EC, mf, sl) = F[mf];
-      };
-      do_item(std::integral_constant<int, 0>());
-      do_item(std::integral_constant<int, 1>());
-      if constexpr (DIM == 3) do_item(std::integral_constant<int, 2>());
+          for (int mf = 0; mf < NF; ++mf) W[mf] = mf == 0 ? gd : T(0);
+        } else {
+          const bool up_m = flow_up ? has_m : !has_p;
+          face_trace_rt<DIM, P, PB, T>(up_m ? cm : cp, E, up_m ? tb.L1 : tb.L0, m.q2g, W);
+        }
+        face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
+      } else {
+        T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
+        if (has_m) face_trace_rt<DIM, P, PB, T>(cm, E, tb.L1, m.q2g, S);
+        if (has_p) face_trace_rt<DIM, P, PB, T>(cp, E, tb.L0, m.q2g, D);
+#pragma unroll
+        for (int mf = 0; mf < NF; ++mf) {
+          const T ghost = dir ? (mf == 0 ? gd : T(0)) : T(0);
+          const T tm = has_m ? S[mf] : (dir ? ghost : D[mf]), tp = has_p ? D[mf] : (dir ? ghost : S[mf]);
+          S[mf] = T(0.5) * (tm + tp);
+          D[mf] = T(0.5) * (tm - tp);
+        }
+        face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, (has_m && has_p) || dir, F);
+      }
+      const int sl = lx + (TX + (E == 0)) * (ly + (TY + (E == 1)) * lz);
+      const int base = E == 0 ? FLO[0] : (E == 1 ? FLO[1] : FLO[2]);
+      const int sn = E == 0 ? SL[0] : (E == 1 ? SL[1] : SL[2]);
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) fl[base + mf * sn + sl] = F[mf];
     }
   }
   __syncthreads();
-  // ===== lower faces: every cell reads slot l[E]
+
+  // ===== (2) cell term and the lifting of the cell's face fluxes
+  T R[NM];
+#pragma unroll
+  for (int q = 0; q < NM; ++q) R[q] = T(0);
   if (work) {
-    auto do_lower = [&](auto EC) {
+    const T* cme = cellp(l[0], l[1], l[2]);
+#pragma unroll 1
+    for (int d = 0; d < DIM; ++d) {
+      T M0[N1][N1], M1[N1][N1];
+      load_op<N1, T>(rowp(d, 0, l[0]), M0);
+      load_op<N1, T>(rowp(d, 1, l[1]), M1);
+      const T ihd = d == 0 ? ih[0] : (d == 1 ? ih[1] : ih[2]);
+      apply_sep_box<DIM, P, PB, T>(M0, M1, DIM > 2 ? rowp(d, 2, l[2]) : nullptr, cme, m.q2g, R, ct * ihd);
+    }
+    auto lift = [&](auto EC) {
       constexpr int E = decltype(EC)::value;
-      const int sl = slot(EC, l);
+      const int slo = l[0] + (TX + (E == 0)) * (l[1] + (TY + (E == 1)) * l[2]);
+      const int sup = slo + (E == 0 ? 1 : (E == 1 ? TX : (TX * (TY + 0)) ));
       T F[NF];
 #pragma unroll
-      for (int mf = 0; mf < NF; ++mf) F[mf] = flux_at(EC, mf, sl);
+      for (int mf = 0; mf < NF; ++mf) F[mf] = fl[FLO[E] + mf * SL[E] + slo];
       scatter_face<DIM, P, E, T>(R, tb.L0, F, ih[E]);
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) F[mf] = fl[FLO[E] + mf * SL[E] + sup];
+      scatter_face<DIM, P, E, T>(R, tb.L1, F, -ih[E]);
     };
-    do_lower(std::integral_constant<int, 0>());
-    do_lower(std::integral_constant<int, 1>());
-    if constexpr (DIM == 3) do_lower(std::integral_constant<int, 2>());
+    lift(std::integral_constant<int, 0>());
+    lift(std::integral_constant<int, 1>());
+    if constexpr (DIM == 3) lift(std::integral_constant<int, 2>());
   }
   __syncthreads();   // face fluxes consumed: the region now holds R [cell][NM]
   T* rbuf = fl;

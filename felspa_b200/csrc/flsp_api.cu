@@ -433,11 +433,23 @@ int ensure_band_buffers(flsp_handle* h) {
   return FLSP_OK;
 }
 
-// (buffers allocated beforehand by ensure_band_buffers); with a gate (a
-// device count), every tile list is emptied when the count is zero
-int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter, const int* gate = nullptr) {
+// The cells a narrow-band sweep covers, when they are not the band of phi0:
+// the listed cells (cells[i], i < min(n, *n_dev)) whose flag is set.
+struct SweepCells {
+  const int* cells;
+  const int* flags;
+  long long n;
+  const int* n_dev;
+};
+
+// (buffers allocated beforehand by ensure_band_buffers); `only`: the band is
+// that cell list instead of |mean phi0| <= band_cells * min_diam
+int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter, const SweepCells* only = nullptr) {
   Ctx c = h->ctx();
-  ST(launch_band_flags(c, h->buf[phi0], o->band_cells * h->m.min_diam, h->nb_flags));
+  if (only)
+    ST(launch_band_flags_from_list(c, only->cells, only->flags, only->n, only->n_dev, h->nb_flags));
+  else
+    ST(launch_band_flags(c, h->buf[phi0], o->band_cells * h->m.min_diam, h->nb_flags));
   const int margin = 2;
   ST(launch_band_tiles(c, h->nb_flags, h->hj_tile, margin, h->nb_lists, h->nb_counts));
   h->nb_use[kNbHJ] = true;
@@ -453,7 +465,6 @@ int band_begin(flsp_handle* h, const flsp_reinit_opts* o, int phi0, bool limiter
                          h->nb_counts + kNbWeno));
     h->nb_use[kNbWeno] = true;
   }
-  if (gate) ST(launch_band_gate(h->stream, h->nb_counts, 3, gate));
   for (int i = 0; i < 3; ++i)
     if (i != phi0)
       CU(cudaMemcpyAsync(h->buf[i], h->buf[phi0], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
@@ -466,9 +477,8 @@ int band_end(flsp_handle* h, int phi0) {
 }
 
 // ReinitSimulatorLDG::initialize + run_iteration (reinit.cc:386-393, 529-637);
-// a narrow-band sweep with a gate (device count) sweeps nothing when the
-// count is zero
-int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter, const int* gate = nullptr) {
+// a narrow-band sweep given `only` covers those cells (none listed: no tile)
+int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter, const SweepCells* only = nullptr) {
   ST(validate_reinit(h, o));
   if (o->viscosity > 0.0) ST(ensure_ldg_buffers(h));
   const bool limiter = reinit_limiter(h, o);
@@ -476,7 +486,7 @@ int run_reinit(flsp_handle* h, const flsp_reinit_opts* o, int* n_iter, const int
   const bool narrow = o->narrow_band != 0;
   if (narrow) {
     ST(ensure_band_buffers(h));
-    const int st = band_begin(h, o, phi0, limiter, gate);
+    const int st = band_begin(h, o, phi0, limiter, only);
     if (st) {
       for (int k = 0; k < 3; ++k) h->nb_use[k] = false;
       return st;
@@ -643,7 +653,9 @@ int build_vtab(flsp_handle* h) {
           if (ax < dim && i < h->m.n[ax]) {
             const double xi = j < nq ? x[j] : (double)(j - nq);
             const double X0 = h->m.lo[ax] + i * h->m.h[ax];
-            const double xx = X0 + h->m.h[ax] * xi;
+            // a face's coordinate by one expression from both of its cells
+            // (cell i's upper face = cell i + 1's lower face, bit for bit)
+            const double xx = j == nq + 1 ? h->m.lo[ax] + (i + 1) * h->m.h[ax] : X0 + h->m.h[ax] * xi;
             // coefficient folded into the x factor: ((coeff f0) f1) f2
             v = (ax == 0) ? tm.coeff * host_factor(tm.f[0], xx) : host_factor(tm.f[ax], xx);
           }
@@ -749,12 +761,13 @@ int enqueue_learned(flsp_handle* h, flsp_mlp* net, double band_cells, int pre, i
 // A learned reinitialisation with its residual fallback, enqueued without
 // a host wait (graph-capturable): the network's result from buf[cur], the
 // band cells whose mean ||grad phi| - 1| exceeds o->max_residual, the
-// narrow-band HJ sweep (o->fallback, fixed count) from buf[cur] gated on
-// that device-side count (its launches find no tile when no cell failed),
-// and the network's result everywhere but the failed cells, which take the
-// sweep's.  The operations of flsp_reinit_learned, whose host loop decides
-// the same on the host; h->cur ends on the result.  Band, learned and LDG
-// buffers are allocated beforehand.
+// narrow-band HJ sweep (o->fallback, fixed count) from buf[cur] over those
+// failed cells (tiles within the narrow band's margin of them; none failed:
+// no tile, the launches return at once), and the network's result
+// everywhere but the failed cells, which take the sweep's.  The operations
+// of flsp_reinit_learned, whose host decides whether to sweep at all;
+// h->cur ends on the result.  Band, learned and LDG buffers are allocated
+// beforehand.
 int enqueue_learned_fallback(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* o) {
   const int64_t ncell = h->m.ncell;
   const int pre = h->cur, out = other(pre, -1);
@@ -764,7 +777,8 @@ int enqueue_learned_fallback(flsp_handle* h, flsp_mlp* net, const flsp_learned_o
   CU(cudaMemcpyAsync(h->lrn_save, h->buf[out], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
   h->cur = pre;
   int nit = 0;
-  ST(run_reinit(h, &o->fallback, &nit, h->lrn_count + 1));
+  const SweepCells failed = {h->lrn_cells, h->lrn_flags, ncell, h->lrn_count};
+  ST(run_reinit(h, &o->fallback, &nit, &failed));
   const int hj = h->cur, res = other(hj, -1);
   CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
   ST(launch_merge_cells(h->stream, h->prec, h->m.nb, h->buf[hj], h->buf[res], h->lrn_cells, h->lrn_flags, ncell,
@@ -1678,7 +1692,8 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
     CU(cudaMemcpyAsync(h->lrn_save, h->buf[out], (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));
     h->cur = pre;
     int nit = 0;
-    ST(run_reinit(h, &o->fallback, &nit));
+    const SweepCells failed = {h->lrn_cells, h->lrn_flags, stl.n_band, nullptr};
+    ST(run_reinit(h, &o->fallback, &nit, o->fallback.narrow_band ? &failed : nullptr));
     const int hj = h->cur;
     const int res = other(hj, -1);
     CU(cudaMemcpyAsync(h->buf[res], h->lrn_save, (size_t)h->ndofs * h->tsize, cudaMemcpyDeviceToDevice, h->stream));

@@ -420,13 +420,6 @@ int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margi
 }
 
 namespace {
-// no tile for any band kernel family when the gate count is zero
-__global__ void band_gate_kernel(int* counts, int n, const int* gate) {
-  if (threadIdx.x < n && *gate == 0) counts[threadIdx.x] = 0;
-}
-}  // namespace
-
-namespace {
 // running totals of the learned reinitialisation: band cells, and fallback
 // cells when `with_fallback`
 __global__ void learned_totals_kernel(const int* counts, unsigned long long* tot, int with_fallback) {
@@ -441,9 +434,23 @@ int launch_learned_totals(cudaStream_t s, const int* counts, unsigned long long*
   return launch_status("learned_totals_kernel");
 }
 
-int launch_band_gate(cudaStream_t s, int* counts, int n, const int* gate) {
-  band_gate_kernel<<<1, 32, 0, s>>>(counts, n, gate);
-  return launch_status("band_gate_kernel");
+namespace {
+// flags[cells[i]] = list_flags[i] for the listed cells (the others zeroed before)
+__global__ void band_flags_from_list_kernel(const int* __restrict__ cells, const int* __restrict__ list_flags,
+                                            long long n, const int* __restrict__ n_dev, int* __restrict__ flags) {
+  if (n_dev) n = min(n, (long long)*n_dev);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (list_flags[i]) flags[cells[i]] = 1;
+}
+}  // namespace
+
+int launch_band_flags_from_list(const Ctx& c, const int* cells, const int* list_flags, long long n, const int* n_dev,
+                                int* flags) {
+  cudaError_t e = cudaMemsetAsync(flags, 0, (size_t)c.m.ncell * sizeof(int), c.stream);
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("band flags: ") + cudaGetErrorString(e));
+  if (n <= 0) return FLSP_OK;
+  band_flags_from_list_kernel<<<grid_for(n), 256, 0, c.stream>>>(cells, list_flags, n, n_dev, flags);
+  return launch_status("band_flags_from_list_kernel");
 }
 
 int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags) {

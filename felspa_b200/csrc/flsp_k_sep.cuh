@@ -46,16 +46,22 @@ int sep_call(int what, const Ctx& c, const VelDev* v, const int* tile, size_t* b
         return with_sep_tile<DIM>(tile, [&](auto X, auto Y, auto Z) -> int {
           constexpr int TX = decltype(X)::value, TY = decltype(Y)::value, TZ = decltype(Z)::value;
           using PL = SepPlan<DIM, P, PB, TX, TY, TZ, T>;
-          auto kern = adv_sep_kernel<DIM, P, PB, TX, TY, TZ, T>;
+          // with or without Dirichlet faces (the boundary lookup only where
+          // the mesh carries some)
+          auto kern = c.m.bc_face ? adv_sep_kernel<DIM, P, PB, TX, TY, TZ, T, true>
+                                  : adv_sep_kernel<DIM, P, PB, TX, TY, TZ, T, false>;
           if (what == 0) {
             *bytes = PL::BYTES;
             return FLSP_OK;
           }
           if (what == 1) {
             if (PL::BYTES > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "separable tile too large");
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::BYTES);
-            if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("sep attr: ") + cudaGetErrorString(e));
+            for (auto k : {adv_sep_kernel<DIM, P, PB, TX, TY, TZ, T, true>,
+                           adv_sep_kernel<DIM, P, PB, TX, TY, TZ, T, false>}) {
+              cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::BYTES);
+              if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+              if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("sep attr: ") + cudaGetErrorString(e));
+            }
             return FLSP_OK;
           }
           AdvSepArgs<T> b;

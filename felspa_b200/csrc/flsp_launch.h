@@ -39,8 +39,10 @@ int launch_band_flags(const Ctx& c, const void* phi0, double thr, int* flags);
 int launch_band_tiles(const Ctx& c, const int* flags, const int* tile, int margin, int* list, int* count);
 // out[c] = phi0[c] for cells with flags[c] == 0
 int launch_band_restore(const Ctx& c, const void* phi0, void* out, const int* flags);
-// counts[0..n) = 0 when *gate == 0 (a gated sweep then finds no tile)
-int launch_band_gate(cudaStream_t s, int* counts, int n, const int* gate);
+// band flags of the listed cells whose list flag is set (all others 0); the
+// list holds min(n, *n_dev) cells
+int launch_band_flags_from_list(const Ctx& c, const int* cells, const int* list_flags, long long n, const int* n_dev,
+                                int* flags);
 // tot[0] += counts[0] (band cells); tot[1] += counts[1] (fallback cells) if with_fallback
 int launch_learned_totals(cudaStream_t s, const int* counts, unsigned long long* tot, int with_fallback);
 

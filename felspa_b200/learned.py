@@ -468,3 +468,56 @@ def learned_vs_plain_3d(n=48, train_n=24, instances=8, train_steps=3000, seed=7,
     return {"training": {"pairs": n_pairs, "collect_s": t1 - t0, "steps": train_steps, "batch": 8192,
                          "train_s": t2 - t1, "mse_before": loss0, "mse_after": loss1, "last_batch_mse": last},
             "runs": runs}
+
+
+def _rate_at_l1(points, target):
+    """rate of a method at L1 interface error `target`, by linear
+    interpolation in log L1 along its (L1, rate) points ordered by reinit
+    interval; None when the target lies outside the points' L1 range"""
+    pts = sorted(points, key=lambda p: p[0])
+    for (l0, r0), (l1, r1) in zip(pts, pts[1:]):
+        if l0 <= target <= l1:
+            if l1 == l0:
+                return max(r0, r1)
+            w = (np.log(target) - np.log(l0)) / (np.log(l1) - np.log(l0))
+            return float(r0 + w * (r1 - r0))
+    return None
+
+
+def equal_l1_study(net, workloads, n=256, intervals=(20, 40, 80, 160), plain=None, max_residual=0.05):
+    """Learned against plain HJ reinitialisation at equal L1 interface error.
+    For every workload (name -> (velocity, ic, t_end)): a run without
+    reinitialisation, then for every reinit interval the plain sweep (the
+    reference's algorithm over every cell), the learned reinit with its
+    residual fallback decided on the device, and the learned reinit
+    without fallback; every run replayed from CUDA graphs, device time.
+    Each method's runs give an (L1, DoF-steps/s) front over the intervals;
+    at the L1 of every plain run the learned methods' rates are read off
+    their fronts (interpolated in log L1), and their ratio to the plain
+    rate is the speed-up at equal L1."""
+    out = {}
+    for name, (vel, ic, t_end) in workloads.items():
+        none = interface_run("none", velocity=vel, ic=ic, t_end=t_end, n=n, plain=plain)
+        steps = none["steps"]
+        runs = {"none": none, "plain": [], "learned": [], "learned_no_fallback": []}
+        for every in intervals:
+            runs["plain"].append(interface_run("plain", velocity=vel, ic=ic, t_end=t_end, n=n, every=every,
+                                               plain=plain, steps=steps))
+            runs["learned"].append(interface_run("learned", net=net, velocity=vel, ic=ic, t_end=t_end, n=n,
+                                                 every=every, plain=plain, max_residual=max_residual,
+                                                 steps=steps))
+            runs["learned_no_fallback"].append(interface_run("learned", net=net, velocity=vel, ic=ic, t_end=t_end,
+                                                             n=n, every=every, plain=plain,
+                                                             max_residual=float("inf"), steps=steps))
+        fronts = {k: [(r["l1_interface_error"], r["dof_steps_per_s"]) for r in runs[k]]
+                  for k in ("plain", "learned", "learned_no_fallback")}
+        equal = []
+        for r in runs["plain"]:
+            row = {"plain_every": r["every"], "l1": r["l1_interface_error"], "plain_rate": r["dof_steps_per_s"]}
+            for k in ("learned", "learned_no_fallback"):
+                rate = _rate_at_l1(fronts[k], r["l1_interface_error"])
+                row[k + "_rate"] = rate
+                row[k + "_speedup"] = rate / r["dof_steps_per_s"] if rate else None
+            equal.append(row)
+        out[name] = {"steps": steps, "runs": runs, "equal_l1": equal}
+    return out

@@ -204,6 +204,12 @@ class Problem:
     def snapshot(self):
         check(load().flsp_snapshot(self.h))
 
+    def learned_totals(self, reset=False):
+        """(band cells, fallback cells) summed over the learned reinitialisations"""
+        nb, nf = C.c_int64(0), C.c_int64(0)
+        check(load().flsp_learned_totals(self.h, C.byref(nb), C.byref(nf), 1 if reset else 0))
+        return nb.value, nf.value
+
     def set_dirichlet(self, boundary_id, value):
         """a Dirichlet condition of constant value on the faces of id boundary_id (> 0)"""
         check(load().flsp_set_dirichlet(self.h, int(boundary_id), float(value)))

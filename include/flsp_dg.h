@@ -474,7 +474,10 @@ typedef struct flsp_learned_opts {
   double max_residual;     /* a cell whose mean ||grad phi| - 1| after the
                               network exceeds this takes the HJ result
                               (default 0.05)                              */
-  flsp_reinit_opts fallback;   /* the HJ sweep used for those cells     */
+  flsp_reinit_opts fallback;   /* the HJ sweep used for those cells; a
+                              narrow-band sweep covers exactly them (and the
+                              tiles within two cells of them), the rest of
+                              the mesh frozen at the pre-reinit state      */
 } flsp_learned_opts;
 
 typedef struct flsp_learned_stats {
@@ -520,8 +523,9 @@ int flsp_reinit_learned(flsp_handle* h, flsp_mlp* net, const flsp_learned_opts* 
    finite o->max_residual > 0 each period carries the residual test and
    the HJ fallback of flsp_reinit_learned, decided on the device: the
    fallback sweep (o->fallback, which must be a fixed-count narrow-band
-   sweep) is always enqueued and finds no tile to sweep when no band cell
-   failed the test, so the results equal flsp_reinit_learned's.  With
+   sweep) is always enqueued, over the failed cells only, and finds no
+   tile to sweep when no band cell failed the test, so the results equal
+   flsp_reinit_learned's.  With
    o->max_residual = infinity the network's result is taken in every band
    cell.  Enqueued; flsp_sync waits.  The first period of each buffer role
    sizes the network's work buffers for every cell of the mesh.         */

@@ -74,6 +74,10 @@ def revolution_cases():
     1e-3 (tests/test_zalesak_disk.cc:252,256).
     name -> (basis, viscosity, keep the full final state)"""
     return {
+        # the inviscid Q1 sweep is unstable over a revolution (the field
+        # degrades and rounding differences grow without bound): its state
+        # is frozen at T = 0.05 as well
+        "zalesak128_q1_nu0_t0.05": (abi.BASIS_Q, 0.0, True, 0.05),
         "zalesak128_q1_nu0": (abi.BASIS_Q, 0.0, False),
         "zalesak128_p1_nu0": (abi.BASIS_P, 0.0, False),
         "zalesak128_q1_nu1e-3": (abi.BASIS_Q, 1e-3, True),
@@ -92,7 +96,7 @@ def revolution_opts(viscosity):
     return abi.default_ls_opts(reinit_frequency=10, reinit=ro)
 
 
-def compute_revolution(basis, viscosity, keep_state):
+def compute_revolution(basis, viscosity, keep_state, t_end=1.0):
     import time
     ic = F.zalesak_disk()
     pr = O.Problem(2, (128, 128), 1, basis)
@@ -100,7 +104,7 @@ def compute_revolution(basis, viscosity, keep_state):
     phi = pr.project(ic)
     area0 = pr.reduce(abi.RED_MASS, phi)
     t0 = time.perf_counter()
-    pr.ls_advance(phi, 1.0, revolution_opts(viscosity), single_step=False, rk_order=3, cfl_max=0.1)
+    pr.ls_advance(phi, t_end, revolution_opts(viscosity), single_step=False, rk_order=3, cfl_max=0.1)
     cpu_s = time.perf_counter() - t0
     nb = pr.nb
     out = {"t_end": np.array(pr.clock.t), "n_substeps": np.array(pr.clock.n_substeps),

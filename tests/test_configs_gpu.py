@@ -20,9 +20,11 @@ kernels re-associate the same quadrature sums: sum factorisation, exact
 modal identities).  Over a run, every substep feeds those rounding
 differences into the next one and the reinitialisation's nonlinear terms
 (smooth sign, the |.| of the Lax-Friedrichs flux, the minmod switch)
-amplify them: the bar is 1e-11 relative for a few periods; over a full
-revolution the bar is on the run's outputs (time, area, L1 interface
-error, the final state), with the tolerances stated per check below.
+amplify them: the bar is 1e-11 relative for a few periods.  Over a full
+revolution the stable configurations still agree to a few 1e-15 (the bar
+is 1e-12 on the final state, the area and the L1 interface error); the
+inviscid Q1 sweep, which the reference's scheme cannot keep stable, is
+pinned at T = 0.05 and compared over the revolution by its character.
 """
 import os
 
@@ -47,15 +49,16 @@ def revolution_control(viscosity):
     return abi.default_ls_opts(reinit_frequency=10, reinit=ro)
 
 
-@pytest.mark.parametrize("name,basis,viscosity", [
-    ("zalesak128_q1_nu1e-3", abi.BASIS_Q, 1e-3),
-    ("zalesak128_p1_nu1e-3", abi.BASIS_P, 1e-3),
-    ("zalesak128_q1_nu0", abi.BASIS_Q, 0.0),
-    ("zalesak128_p1_nu0", abi.BASIS_P, 0.0),
-    ("zalesak128_q1_nu6.28e-5", abi.BASIS_Q, 6.28e-5),
-    ("zalesak128_p1_nu6.28e-5", abi.BASIS_P, 6.28e-5),
+@pytest.mark.parametrize("name,basis,viscosity,t_end", [
+    ("zalesak128_q1_nu1e-3", abi.BASIS_Q, 1e-3, 1.0),
+    ("zalesak128_p1_nu1e-3", abi.BASIS_P, 1e-3, 1.0),
+    ("zalesak128_q1_nu6.28e-5", abi.BASIS_Q, 6.28e-5, 1.0),
+    ("zalesak128_p1_nu6.28e-5", abi.BASIS_P, 6.28e-5, 1.0),
+    ("zalesak128_p1_nu0", abi.BASIS_P, 0.0, 1.0),
+    ("zalesak128_q1_nu0_t0.05", abi.BASIS_Q, 0.0, 0.05),
+    ("zalesak128_q1_nu0", abi.BASIS_Q, 0.0, 1.0),
 ])
-def test_zalesak_revolution(flsp, name, basis, viscosity):
+def test_zalesak_revolution(flsp, name, basis, viscosity, t_end):
     g = np.load(os.path.join(GOLDEN, name + ".npz"))
     ic = F.zalesak_disk()
     ls = LevelSetSurface(Mesh(2, (128, 128)), 1, basis=basis, precision=abi.FP64, cfl_max=0.1,
@@ -63,27 +66,34 @@ def test_zalesak_revolution(flsp, name, basis, viscosity):
     ls.initialize(ic, F.ccw_rotation())
     area0 = ls.integrate_mass()
     assert abs(area0 - float(g["area0"])) <= 1e-13 * abs(float(g["area0"]))
-    ls.advance_time(1.0)
+    ls.advance_time(t_end)
     assert abs(ls.get_time() - float(g["t_end"])) <= 1e-13
+    assert ls.problem.get_step_count() == int(g["n_substeps"])
     phi = ls.get_solution_vector()
     nb = ls.problem.dofs_per_cell
     area1, l1 = ls.integrate_mass(), ls.interface_error_l1(ic)
-    if "result" in g:
-        # the stable sweep (viscosity): the whole final state
+    if name == "zalesak128_q1_nu0":
+        # the inviscid Q1 sweep is unstable: over a revolution the field
+        # degrades in both runs (the area grows ~3x) and the rounding
+        # differences between them grow with it, so only the run's
+        # character is compared; its state is pinned at T = 0.05 above
+        assert area1 > 2.0 * area0 and float(g["area1"]) > 2.0 * float(g["area0"])
+        assert abs(l1 - float(g["l1_ic"])) <= 0.2 * float(g["l1_ic"])
+    elif "result" in g:
+        # the whole final state, the area and the L1 interface error
+        # (measured: 2e-15 to 4e-15 relative after 17,426 substeps)
         assert rel(phi, g["result"]) <= RUN_TOL, rel(phi, g["result"])
         assert abs(area1 - float(g["area1"])) <= RUN_TOL * abs(float(g["area1"]))
         assert abs(l1 - float(g["l1_ic"])) <= RUN_TOL * max(abs(float(g["l1_ic"])), 1e-3)
     else:
-        # the inviscid sweep decays the field (the reference's LF scheme
-        # without viscosity); the cell means and the run's outputs
-        assert rel(phi.reshape(-1, nb)[:, 0], g["cell_means"]) <= RUN_TOL_INVISCID
-        assert abs(area1 - float(g["area1"])) <= RUN_TOL_INVISCID * abs(float(g["area1"]))
-        assert abs(l1 - float(g["l1_ic"])) <= RUN_TOL_INVISCID * max(abs(float(g["l1_ic"])), 1e-3)
+        # the inviscid P1 sweep stays stable: its cell means
+        assert rel(phi.reshape(-1, nb)[:, 0], g["cell_means"]) <= RUN_TOL
+        assert abs(area1 - float(g["area1"])) <= RUN_TOL * abs(float(g["area1"]))
+        assert abs(l1 - float(g["l1_ic"])) <= RUN_TOL * max(abs(float(g["l1_ic"])), 1e-3)
     ls.problem.close()
 
 
-RUN_TOL = 1e-9
-RUN_TOL_INVISCID = 1e-6
+RUN_TOL = 1e-12
 
 
 def test_sphere_64cubed_first_period(oracle, flsp):

@@ -133,8 +133,10 @@ def test_learned_band_and_forced_fallback():
     load().flsp_default_reinit_opts(C.byref(o))
     o.mode = abi.REINIT_FIXED
     o.n_pseudo_steps = 20
-    o.narrow_band = 1     # the fallback's default: the sweep restricted to the band
-    o.band_cells = 6.0
+    o.narrow_band = 1     # the fallback's default: the sweep restricted to the failed cells,
+    # here every band cell (|mean phi| <= 6 h; the sweep's band is measured
+    # in cell diameters, sqrt(2) h)
+    o.band_cells = 6.0 / np.sqrt(2.0)
     nit = C.c_int(0)
     check(load().flsp_reinit(pb.h, C.byref(o), C.byref(nit)))
     hj = pb.get_state().reshape(-1, 9)
@@ -214,3 +216,33 @@ def test_learned_graph_periods_with_fallback_match_host_loop(max_residual):
     a.close()
     b.close()
     net.close()
+
+
+def test_trained_network_beats_untrained_and_no_reinit_on_held_out_instances():
+    """trained on the plain sweep's pairs of some instances, the network
+    predicts the sweep's change on instances it has not seen with a small
+    fraction of the error of the untrained network and of doing nothing
+    (a zero network: the state left as it is)"""
+    trained, untrained, zero = MLP(device=0, seed=21), MLP(device=0, seed=21), MLP(device=0, seed=22)
+    zero.set_params(np.zeros(zero.n_params, dtype=np.float32))
+    for s in range(6):
+        pb = make_problem(64, 50 + s)
+        for _ in range(3):
+            advance(pb, 20)
+            trained.collect(pb, band_cells=6.0)
+        pb.close()
+    trained.train(steps=800, batch=2048, lr=1e-3, seed=4)
+    mse = {}
+    for name, net in (("trained", trained), ("untrained", untrained), ("zero", zero)):
+        net.clear_pairs()
+        for s in range(3):           # held-out instances: the same pairs for every network
+            pb = make_problem(64, 80 + s)
+            for _ in range(2):
+                advance(pb, 20)
+                net.collect(pb, band_cells=6.0)
+            pb.close()
+        mse[name] = net.eval()
+    assert mse["trained"] < 0.3 * mse["zero"], mse
+    assert mse["trained"] < 0.3 * mse["untrained"], mse
+    for net in (trained, untrained, zero):
+        net.close()
