@@ -69,6 +69,21 @@ struct AdvSepArgs {
   double dt_explicit;
 };
 
+// In-cell DoF index (HBM order) of Q-layout mode q for FE_DGP
+// (PolynomialSpace order: c outer, b, a inner with a + b + c <= P), -1 for a
+// mode outside P-space
+template <int DIM, int P>
+__host__ __device__ constexpr int q2g_ct(int q) {
+  const int N1 = P + 1;
+  const int a = q % N1, b = (q / N1) % N1, c = DIM > 2 ? q / (N1 * N1) : 0;
+  if (a + b + c > P) return -1;
+  int idx = 0;
+  for (int cc = 0; cc < c; ++cc)
+    for (int bb = 0; bb <= P - cc; ++bb) idx += P - bb - cc + 1;
+  for (int bb = 0; bb < b; ++bb) idx += P - bb - c + 1;
+  return idx + a;
+}
+
 // Shared-memory plan of the separable stage kernel for a compile-time tile
 // TX x TY x TZ (TZ = 1 in 2D): mbarrier | halo box rows | operator rows |
 // face fluxes (reused for the tile's R).  Box rows: (TY+2)(TZ+2) slots of
@@ -184,26 +199,24 @@ __device__ __forceinline__ void face_apply(const T* __restrict__ rowA0, const T*
   (void)NF;
 }
 
-// trace of a box cell (HBM order) on its face normal to the runtime axis E
-// (side values Ls = L(0) or L(1)), in face modes; the P basis reads its
-// modes through the Q-layout map
-template <int DIM, int P, bool PB, typename T>
-__device__ __forceinline__ void face_trace_rt(const T* __restrict__ src, int E, const T* Ls,
-                                              const signed char* q2g, T* tr) {
+// trace of a box cell (HBM order) on its face normal to E, in face modes
+// (side values Ls = L(0) or L(1)); the P basis reads its modes through the
+// Q-layout map
+template <int DIM, int P, bool PB, int E, typename T>
+__device__ __forceinline__ void face_trace_ct(const T* __restrict__ src, const T* Ls, T* tr) {
   constexpr int N1 = P + 1, NF = DIM > 2 ? N1 * N1 : N1;
-  const int sE = E == 0 ? 1 : (E == 1 ? N1 : N1 * N1);   // stride of axis E
-  const int s0 = E == 0 ? N1 : 1;                        // first tangential axis
-  const int s1 = E == 2 ? N1 : N1 * N1;                  // second (3D)
+  constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  constexpr int st[3] = {1, N1, N1 * N1};
 #pragma unroll
   for (int mf = 0; mf < NF; ++mf) {
     const int m0 = mf % N1, m1 = mf / N1;
-    const int base = m0 * s0 + (DIM > 2 ? m1 * s1 : 0);
+    const int base = m0 * st[t0] + (DIM > 2 ? m1 * st[t1] : 0);
     T s = T(0);
 #pragma unroll
     for (int aa = 0; aa < N1; ++aa) {
-      const int q = base + aa * sE;
+      const int q = base + aa * st[E];
       if constexpr (PB) {
-        const int gi = q2g[q];
+        const int gi = q2g_ct<DIM, P>(q);
         if (gi >= 0) s += Ls[aa] * src[gi];
       } else {
         s += Ls[aa] * src[q];
@@ -213,28 +226,14 @@ __device__ __forceinline__ void face_trace_rt(const T* __restrict__ src, int E, 
   }
 }
 
-// R += s (M0 (x) M1 (x) M2) c with the cell's coefficients read from its
-// box copy one z-slab at a time (Q layout; the P basis through q2g)
-template <int DIM, int P, bool PB, typename T>
-__device__ __forceinline__ void apply_sep_box(const T (&M0)[P + 1][P + 1], const T (&M1)[P + 1][P + 1],
-                                              const T* __restrict__ m2row, const T* __restrict__ src,
-                                              const signed char* q2g, T* R, T s) {
+// R += s (M0 (x) M1 (x) M2) c (Q layout, index a0 + N1 a1 + N1^2 a2),
+// contracted one z-slab of c at a time; M2 read from its shared-memory row
+template <int DIM, int P, typename T>
+__device__ __forceinline__ void apply_sep_reg(const T (&M0)[P + 1][P + 1], const T (&M1)[P + 1][P + 1],
+                                              const T* __restrict__ m2row, const T* c, T* R, T s) {
   constexpr int N1 = P + 1, NZ = DIM > 2 ? N1 : 1;
 #pragma unroll
   for (int b2 = 0; b2 < NZ; ++b2) {
-    T x[N1][N1];   // [b1][b0]
-#pragma unroll
-    for (int b1 = 0; b1 < N1; ++b1)
-#pragma unroll
-      for (int b0 = 0; b0 < N1; ++b0) {
-        const int q = b0 + N1 * (b1 + N1 * b2);
-        if constexpr (PB) {
-          const int gi = q2g[q];
-          x[b1][b0] = gi >= 0 ? src[gi] : T(0);
-        } else {
-          x[b1][b0] = src[q];
-        }
-      }
     T u[N1][N1];   // [a0][b1]
 #pragma unroll
     for (int a0 = 0; a0 < N1; ++a0)
@@ -242,7 +241,7 @@ __device__ __forceinline__ void apply_sep_box(const T (&M0)[P + 1][P + 1], const
       for (int b1 = 0; b1 < N1; ++b1) {
         T acc = T(0);
 #pragma unroll
-        for (int b0 = 0; b0 < N1; ++b0) acc += M0[a0][b0] * x[b1][b0];
+        for (int b0 = 0; b0 < N1; ++b0) acc += M0[a0][b0] * c[b0 + N1 * (b1 + N1 * b2)];
         u[a0][b1] = acc;
       }
     T m2c[N1];   // column b2 of M2
@@ -268,21 +267,13 @@ __device__ __forceinline__ void apply_sep_box(const T (&M0)[P + 1][P + 1], const
   }
 }
 
-// Dirichlet value on the domain-boundary face on side S of axis E of the
-// cell (gx, gy, gz) (bc_dirichlet with the coordinates as scalars)
-template <int DIM, typename T>
-__device__ __forceinline__ bool bc_dirichlet_at(const MeshArgs& m, int E, int S, int gx, int gy, int gz, T& g) {
-  const int c[3] = {gx, gy, gz};
-  return bc_dirichlet<DIM>(m, E, S, c, g);
-}
-
 // FP32 tiles fit two CTAs per SM (<= 128 registers); an FP64 tile takes most
 // of an SM's shared memory, so FP64 gets the full register file.
 //
 // Phases: (1) every face of the tile (interior, tile boundary, domain
-// boundary) is a work item with a runtime axis: traces of its two box
-// cells, the separable upwind flux, written to the face's slot, so each
-// face's flux is computed once per CTA by one routine whatever the tiling;
+// boundary) is a work item: traces of its two box cells, the separable
+// upwind flux, written to the face's slot, so each face's flux is computed
+// once per CTA by one routine whatever the tiling;
 // (2) every cell: the cell term (one direction at a time) and the lifting of
 // its 2 dim face fluxes from the slots; (3) the RK combination fused into
 // the coalesced store.  BC: the mesh may carry Dirichlet faces.
@@ -376,77 +367,79 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
   constexpr int SL[3] = {PL::SL0, PL::SL1, PL::SL2};
   constexpr int FLO[3] = {0, NF * PL::SL0, NF * (PL::SL0 + PL::SL1)};
 
-  // ===== (1) face fluxes, one work item per face of the tile
+  // ===== (1) face fluxes, one work item per face of the tile.  The faces
+  // normal to E form a block (TX + (E==0)) x (TY + (E==1)) x (TZ + (E==2))
+  // in slot order, x fastest (consecutive lanes read consecutive cells of a
+  // box row); the three blocks start on warp boundaries when their sizes are
+  // multiples of 32, so a warp serves one axis
+  auto face_item = [&](auto EC, int r) {
+    constexpr int E = decltype(EC)::value;
+    constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+    constexpr int EX = TX + (E == 0), EY = TY + (E == 1);
+    const int lx = r % EX, ly = (r / EX) % EY, lz = DIM > 2 ? r / (EX * EY) : 0;
+    const int lc[3] = {lx, ly, lz};
+    const int gc[3] = {ox + lx, oy + ly, oz + lz};
+    if ((E != 0 && gc[0] >= m.n[0]) || (E != 1 && gc[1] >= m.n[1]) || (DIM > 2 && E != 2 && gc[2] >= m.n[2])) return;
+    const int f = lc[E], gE = gc[E];
+    const bool has_m = gE >= 1 && gE - 1 < m.n[E], has_p = gE < m.n[E];
+    if (!has_m && !has_p) return;
+    const T* cp = cellp(lx, ly, lz);
+    const T* cm = cellp(lx - (E == 0), ly - (E == 1), lz - (E == 2));
+    T gd = T(0);
+    bool dir = false;
+    if constexpr (BC) {
+      if (!has_m) dir = bc_dirichlet<DIM>(m, E, 0, gc, gd);
+      else if (!has_p) {
+        const int gl[3] = {gc[0] - (E == 0), gc[1] - (E == 1), gc[2] - (E == 2)};
+        dir = bc_dirichlet<DIM>(m, E, 1, gl, gd);
+      }
+    }
+    // tangential operator rows and the normal factor g_EE at the face: the
+    // upper cell's xi = 0 value where that cell is a tile cell of the mesh,
+    // else the lower cell's xi = 1 value (the same number, tabulated from
+    // one expression; rows past the mesh hold no face values)
+    const T* r0 = rowp(E, t0, lc[t0]);
+    const T* r1 = DIM > 2 ? rowp(E, t1, lc[t1]) : nullptr;
+    const T fe = (f < TL[E] && has_p) ? rowp(E, E, f)[BOFF] : rowp(E, E, f - 1)[BOFF + 1];
+    const T s1 = ct * fe;
+    T F[NF];
+    // tangential factors of one sign over the face: |u_E| = sigma u_E, so
+    // the flux is u_E times the upwind trace alone
+    const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
+    if (sigma != T(0)) {
+      const bool flow_up = s1 * sigma > T(0);   // upwind: the lower cell
+      T W[NF];
+      if (dir && !(flow_up ? has_m : has_p)) {
+#pragma unroll
+        for (int mf = 0; mf < NF; ++mf) W[mf] = mf == 0 ? gd : T(0);
+      } else {
+        const bool up_m = flow_up ? has_m : !has_p;
+        face_trace_ct<DIM, P, PB, E, T>(up_m ? cm : cp, up_m ? tb.L1 : tb.L0, W);
+      }
+      face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
+    } else {
+      T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
+      if (has_m) face_trace_ct<DIM, P, PB, E, T>(cm, tb.L1, S);
+      if (has_p) face_trace_ct<DIM, P, PB, E, T>(cp, tb.L0, D);
+#pragma unroll
+      for (int mf = 0; mf < NF; ++mf) {
+        const T ghost = dir ? (mf == 0 ? gd : T(0)) : T(0);
+        const T tm = has_m ? S[mf] : (dir ? ghost : D[mf]), tp = has_p ? D[mf] : (dir ? ghost : S[mf]);
+        S[mf] = T(0.5) * (tm + tp);
+        D[mf] = T(0.5) * (tm - tp);
+      }
+      face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, (has_m && has_p) || dir, F);
+    }
+    const int sl = lx + EX * (ly + EY * lz);
+#pragma unroll
+    for (int mf = 0; mf < NF; ++mf) fl[FLO[E] + mf * SL[E] + sl] = F[mf];
+  };
   if (active) {
     constexpr int TOT = PL::SL0 + PL::SL1 + PL::SL2;
     for (int it = threadIdx.x; it < TOT; it += NT) {
-      const int E = it < SL[0] ? 0 : (it < SL[0] + SL[1] ? 1 : 2);
-      const int r = it - (E == 0 ? 0 : (E == 1 ? SL[0] : SL[0] + SL[1]));
-      const int tE = E == 0 ? TX : (E == 1 ? TY : TZ);
-      const int t0l = E == 0 ? TY : TX;   // tile cells along the first tangential axis
-      const int f = r % (tE + 1), rest = r / (tE + 1);
-      const int u0 = rest % t0l, u1 = DIM > 2 ? rest / t0l : 0;
-      // local coordinates of the face's upper cell (f along E)
-      const int lx = E == 0 ? f : u0;
-      const int ly = E == 1 ? f : (E == 0 ? u0 : u1);
-      const int lz = E == 2 ? f : u1;
-      const int gx = ox + lx, gy = oy + ly, gz = oz + lz;
-      const int gE = E == 0 ? gx : (E == 1 ? gy : gz);
-      const int nE = m.n[E];
-      if (E != 0 && gx >= m.n[0]) continue;
-      if (E != 1 && gy >= m.n[1]) continue;
-      if (DIM > 2 && E != 2 && gz >= m.n[2]) continue;
-      const bool has_m = gE >= 1 && gE - 1 < nE, has_p = gE < nE;
-      if (!has_m && !has_p) continue;
-      const T* cp = cellp(lx, ly, lz);
-      const T* cm = cellp(lx - (E == 0), ly - (E == 1), lz - (E == 2));
-      T gd = T(0);
-      bool dir = false;
-      if constexpr (BC) {
-        if (!has_m) dir = bc_dirichlet_at<DIM>(m, E, 0, gx, gy, gz, gd);
-        else if (!has_p) dir = bc_dirichlet_at<DIM>(m, E, 1, gx - (E == 0), gy - (E == 1), gz - (E == 2), gd);
-      }
-      // tangential operator rows and the normal factor g_EE at the face
-      // (the upper cell's xi = 0 value, or the last tile cell's xi = 1 one:
-      // the same number, tabulated from one expression)
-      const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-      const T* r0 = rowp(E, t0, u0);
-      const T* r1 = DIM > 2 ? rowp(E, t1, u1) : nullptr;
-      const T fe = f < tE ? rowp(E, E, f)[BOFF] : rowp(E, E, tE - 1)[BOFF + 1];
-      const T s1 = ct * fe;
-      T F[NF];
-      // tangential factors of one sign over the face: |u_E| = sigma u_E, so
-      // the flux is u_E times the upwind trace alone
-      const T sigma = DIM > 2 ? r0[N1 * N1] * r1[N1 * N1] : r0[N1 * N1];
-      if (sigma != T(0)) {
-        const bool flow_up = s1 * sigma > T(0);   // upwind: the lower cell
-        T W[NF];
-        if (dir && !(flow_up ? has_m : has_p)) {
-#pragma unroll
-          for (int mf = 0; mf < NF; ++mf) W[mf] = mf == 0 ? gd : T(0);
-        } else {
-          const bool up_m = flow_up ? has_m : !has_p;
-          face_trace_rt<DIM, P, PB, T>(up_m ? cm : cp, E, up_m ? tb.L1 : tb.L0, m.q2g, W);
-        }
-        face_apply<DIM, N1, BOFF, T>(r0, r1, W, W, s1, T(0), false, F);
-      } else {
-        T S[NF], D[NF];   // traces Tm / Tp, then their mean / half jump in place
-        if (has_m) face_trace_rt<DIM, P, PB, T>(cm, E, tb.L1, m.q2g, S);
-        if (has_p) face_trace_rt<DIM, P, PB, T>(cp, E, tb.L0, m.q2g, D);
-#pragma unroll
-        for (int mf = 0; mf < NF; ++mf) {
-          const T ghost = dir ? (mf == 0 ? gd : T(0)) : T(0);
-          const T tm = has_m ? S[mf] : (dir ? ghost : D[mf]), tp = has_p ? D[mf] : (dir ? ghost : S[mf]);
-          S[mf] = T(0.5) * (tm + tp);
-          D[mf] = T(0.5) * (tm - tp);
-        }
-        face_apply<DIM, N1, BOFF, T>(r0, r1, S, D, s1, s1 < T(0) ? -s1 : s1, (has_m && has_p) || dir, F);
-      }
-      const int sl = lx + (TX + (E == 0)) * (ly + (TY + (E == 1)) * lz);
-      const int base = E == 0 ? FLO[0] : (E == 1 ? FLO[1] : FLO[2]);
-      const int sn = E == 0 ? SL[0] : (E == 1 ? SL[1] : SL[2]);
-#pragma unroll
-      for (int mf = 0; mf < NF; ++mf) fl[base + mf * sn + sl] = F[mf];
+      if (it < SL[0]) face_item(std::integral_constant<int, 0>(), it);
+      else if (it < SL[0] + SL[1]) face_item(std::integral_constant<int, 1>(), it - SL[0]);
+      else if constexpr (DIM > 2) face_item(std::integral_constant<int, 2>(), it - SL[0] - SL[1]);
     }
   }
   __syncthreads();
@@ -456,14 +449,27 @@ __global__ void __launch_bounds__(TX * TY * TZ, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
   for (int q = 0; q < NM; ++q) R[q] = T(0);
   if (work) {
-    const T* cme = cellp(l[0], l[1], l[2]);
+    // the cell's coefficients in registers (Q layout)
+    T c[NM];
+    {
+      const T* cme = cellp(l[0], l[1], l[2]);
+#pragma unroll
+      for (int q = 0; q < NM; ++q) {
+        if constexpr (PB) {
+          const int gi = m.q2g[q];
+          c[q] = gi >= 0 ? cme[gi] : T(0);
+        } else {
+          c[q] = cme[q];
+        }
+      }
+    }
 #pragma unroll 1
     for (int d = 0; d < DIM; ++d) {
       T M0[N1][N1], M1[N1][N1];
       load_op<N1, T>(rowp(d, 0, l[0]), M0);
       load_op<N1, T>(rowp(d, 1, l[1]), M1);
       const T ihd = d == 0 ? ih[0] : (d == 1 ? ih[1] : ih[2]);
-      apply_sep_box<DIM, P, PB, T>(M0, M1, DIM > 2 ? rowp(d, 2, l[2]) : nullptr, cme, m.q2g, R, ct * ihd);
+      apply_sep_reg<DIM, P, T>(M0, M1, DIM > 2 ? rowp(d, 2, l[2]) : nullptr, c, R, ct * ihd);
     }
     auto lift = [&](auto EC) {
       constexpr int E = decltype(EC)::value;

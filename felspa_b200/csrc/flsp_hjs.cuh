@@ -58,8 +58,13 @@ struct HjsPlan {
   static constexpr size_t OFF_BOX = 16;
   static constexpr size_t OFF_JN = OFF_BOX + (size_t)NROWS * SLOT;
   static constexpr size_t OFF_JV = OFF_JN + (size_t)2 * DIM * NQF * TL::N * sizeof(T);
-  static constexpr size_t OFF_UB = OFF_JV + (size_t)2 * DIM * NC * TL::N * sizeof(T);
-  static constexpr size_t OFF_RED = (OFF_UB + (size_t)NQ * NU * TL::N * sizeof(T) + 15) / 16 * 16;
+  // the tile's slice of the sign table (pseudo-steps: staged with the box),
+  // then, once every thread has read its entries, the plane projections
+  static constexpr int NS = ipow(NQ, DIM) + (1 << DIM);
+  static constexpr size_t TAB_BYTES = (size_t)NS * TL::N * sizeof(T);
+  static constexpr size_t UB_BYTES = (size_t)NQ * NU * TL::N * sizeof(T);
+  static constexpr size_t OFF_UB = (OFF_JV + (size_t)2 * DIM * NC * TL::N * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t OFF_RED = (OFF_UB + (TAB_BYTES > UB_BYTES ? TAB_BYTES : UB_BYTES) + 15) / 16 * 16;
   static constexpr size_t BYTES = OFF_RED + 64 * sizeof(double);
 };
 
@@ -302,7 +307,8 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
   unsigned char* boxb = smem_raw + PL::OFF_BOX;
   T* jn = reinterpret_cast<T*>(smem_raw + PL::OFF_JN);   // [2*DIM*NQF][NT]
   T* jv = reinterpret_cast<T*>(smem_raw + PL::OFF_JV);   // [2*DIM*NC][NT]
-  T* ub = reinterpret_cast<T*>(smem_raw + PL::OFF_UB);   // [NQ][NU][NT]
+  T* ub = reinterpret_cast<T*>(smem_raw + PL::OFF_UB);   // [NQ][NU][NT], after the table slice
+  T* stl = ub;                                            // table slice [NS][NT] (pseudo-steps)
   double* red = reinterpret_cast<double*>(smem_raw + PL::OFF_RED);
   const MeshArgs& m = a.m;
   const Tab1D<T>& tb = tab<T>(P);
@@ -316,8 +322,10 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
     o[1] = DIM > 1 ? (b % m.ntile[1]) * TY : 0;
     o[2] = DIM > 2 ? (b / m.ntile[1]) * TZ : 0;
   };
+  const bool step = a.mode == kHJStep;
   // halo box of the tile in launch slot `slot`: rows (ly, lz) of cells
-  // [max(ox - 1, 0), min(ox + TX + 1, n)) by bulk copies (warp 0)
+  // [max(ox - 1, 0), min(ox + TX + 1, n)) by bulk copies (warp 0); for a
+  // pseudo-step also the tile's slice of the sign table (one copy)
   auto issue = [&](int slot) {
     int so[3];
     origin(slot, so);
@@ -344,6 +352,11 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
         const long long a0 = s0 & ~15LL, a1 = (s1 + 15) & ~15LL;
         if (pass == 0) bytes += (unsigned)(a1 - a0);
         else bulk_g2s(boxb + (size_t)rr * PL::SLOT, gsrc + a0, (unsigned)(a1 - a0), bar);
+      }
+      if (step && lane == 0) {
+        const int tl = m.tiles ? m.tiles[slot] : slot;
+        if (pass == 0) bytes += (unsigned)PL::TAB_BYTES;
+        else bulk_g2s(stl, a.stab + (size_t)tl * NS * NT, (unsigned)PL::TAB_BYTES, bar);
       }
     }
   };
@@ -510,7 +523,7 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
         S = val / sqrt(val * val + hmin * hmin * gn * gn);
         srow[(size_t)(NQV + v) * NT] = S;
       } else {
-        S = srow[(size_t)(NQV + v) * NT];
+        S = stl[(size_t)(NQV + v) * NT + cl];
       }
       T gs[DIM];
 #pragma unroll
@@ -580,10 +593,13 @@ __global__ void __launch_bounds__(HjsTile<DIM>::N * (P + 2)) hjs_kernel(const HJ
     for (int d = 0; d < DIM; ++d) H += T(0.5) * fabs(S) * (lft[d] - rgt[d]);
     return H;
   };
+  T Sq[NQF];
   if (valid) {
-    T Sq[NQF];
 #pragma unroll
-    for (int j = 0; j < NQF; ++j) Sq[j] = srow[(size_t)(k * NQF + j) * NT];
+    for (int j = 0; j < NQF; ++j) Sq[j] = stl[(size_t)(k * NQF + j) * NT + cl];
+  }
+  __syncthreads();   // the table slice is consumed: its region takes the plane projections
+  if (valid) {
     const T K0k = tb.K0q[k], K1k = tb.K1q[k];
     if constexpr (DIM == 2) {
       const int qy = k;

@@ -179,16 +179,18 @@ def slotted_disk(seed):
                           slot_depth=float(r.uniform(0.5, 1.6) * rad))
 
 
-def collect_training_pairs(net, n=128, instances=24, periods=10, every=40, target=None, band_cells=6.0):
-    """Pairs from random instances (unions of circles and slotted disks; the
-    velocity alternates between an 8-mode Fourier stream function, which
-    distorts the level set, and a rigid rotation about a random centre,
-    which keeps it distance-like; seeds 1000 + i): advance `every` steps,
-    record the band patches, reinitialise with `target`."""
+def collect_training_pairs(net, n=128, instances=24, periods=10, every=40, target=None, band_cells=6.0,
+                           first=0):
+    """Pairs from random instances i = first .. first + instances - 1
+    (unions of circles and slotted disks; the velocity alternates between an
+    8-mode Fourier stream function, which distorts the level set, and a
+    rigid rotation about a random centre, which keeps it distance-like;
+    seeds 1000 + i): advance `every` steps, record the band patches,
+    reinitialise with `target`."""
     from . import fields as F
     from .level_set import Mesh, Problem
     target = target if target is not None else plain_reinit_opts()
-    for i in range(instances):
+    for i in range(first, first + instances):
         pb = Problem(Mesh(2, (n, n)), 2, basis=abi.BASIS_Q, precision=abi.FP32, cfl_max=0.1)
         if (i // 2) % 2 == 0:
             pb.set_velocity(F.fourier_stream_2d(seed=1000 + i))

@@ -50,8 +50,8 @@ def test_mix_matches_oracle(oracle, flsp, dim, smoothing):
             phis.append(lex.ravel())
         want = oracle.material_mix(prs, phis, values, nq, smoothing, order=order)
         assert np.max(np.abs(got - want)) <= 1e-13 * 10.0
-        # every value of the stack occurs
-        assert np.isclose(got, values[0]).any() and np.isclose(got, values[-1]).any()
+        # the materials are mixed: the value varies over the points
+        assert np.ptp(got) > 1.0
     for pb in pbs:
         pb.close()
 
