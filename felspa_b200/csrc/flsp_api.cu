@@ -1827,6 +1827,11 @@ struct flsp_batch {
   int deg_grid[3][4] = {};
   bool built = false;
   std::map<unsigned long long, GraphEntry> graphs;
+  // the degrees' launches of a stage run side by side: one stream per
+  // degree, forked from and joined back into the batch stream
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -1958,31 +1963,55 @@ int batch_sync_problems(flsp_batch* b) {
 }
 
 // the stage / reinit step / limiter of every problem: one launch per degree
+// one launch per degree present, side by side when there are several:
+// each degree's launch on its own stream forked from the batch stream and
+// joined back (graph branches under capture), so that one degree's tail
+// overlaps the others' work
+template <typename F>
+int batch_each_degree(flsp_batch* b, int kind, F&& launch) {
+  int n = 0;
+  for (int p = 1; p <= 3; ++p) n += b->deg_cnt[kind][p] > 0;
+  if (n <= 1) {
+    for (int p = 3; p >= 1; --p)
+      if (b->deg_cnt[kind][p] > 0) ST(launch(p, b->stream));
+    return FLSP_OK;
+  }
+  CU(cudaEventRecord(b->ev_fork, b->stream));
+  int st = FLSP_OK;
+  for (int p = 3; p >= 1; --p) {
+    if (b->deg_cnt[kind][p] == 0) continue;
+    cudaStream_t s = b->side[p - 1];
+    CU(cudaStreamWaitEvent(s, b->ev_fork, 0));
+    if (st == FLSP_OK) st = launch(p, s);
+    // join even after a failed launch, so that a capture stays joined
+    CU(cudaEventRecord(b->ev_join[p - 1], s));
+    CU(cudaStreamWaitEvent(b->stream, b->ev_join[p - 1], 0));
+  }
+  return st;
+}
+
 int batch_adv_all(flsp_batch* b, int thr, int in, int pn, int out, int stage, int combine) {
-  for (int p = 3; p >= 1; --p)
-    if (b->deg_cnt[kBatchKindAdv][p] > 0)
-      ST(launch_batch_adv(b->stream, b->prec, p, b->probs, b->items_adv + b->deg_off[kBatchKindAdv][p],
-                          b->deg_cnt[kBatchKindAdv][p], b->deg_grid[kBatchKindAdv][p], thr,
-                          b->deg_smem[kBatchKindAdv][p], in, pn, out, stage, combine));
-  return FLSP_OK;
+  return batch_each_degree(b, kBatchKindAdv, [&](int p, cudaStream_t s) {
+    return launch_batch_adv(s, b->prec, p, b->probs, b->items_adv + b->deg_off[kBatchKindAdv][p],
+                            b->deg_cnt[kBatchKindAdv][p], b->deg_grid[kBatchKindAdv][p], thr,
+                            b->deg_smem[kBatchKindAdv][p], in, pn, out, stage, combine);
+  });
 }
 
 int batch_hj_all(flsp_batch* b, int thr, int src, int phi0, int dst, int mode, int rk) {
-  for (int p = 3; p >= 1; --p)
-    if (b->deg_cnt[kBatchKindHJ][p] > 0)
-      ST(launch_batch_hj(b->stream, b->prec, p, b->probs, b->items_hj + b->deg_off[kBatchKindHJ][p],
-                         b->deg_cnt[kBatchKindHJ][p], b->deg_grid[kBatchKindHJ][p], thr,
-                         b->deg_smem[kBatchKindHJ][p], src, phi0, dst, mode, rk));
-  return FLSP_OK;
+  return batch_each_degree(b, kBatchKindHJ, [&](int p, cudaStream_t s) {
+    return launch_batch_hj(s, b->prec, p, b->probs, b->items_hj + b->deg_off[kBatchKindHJ][p],
+                           b->deg_cnt[kBatchKindHJ][p], b->deg_grid[kBatchKindHJ][p], thr,
+                           b->deg_smem[kBatchKindHJ][p], src, phi0, dst, mode, rk);
+  });
 }
 
 int batch_weno_all(flsp_batch* b, int in, int out) {
-  for (int p = 3; p >= 1; --p)
-    if (b->deg_cnt[kBatchKindWeno][p] > 0)
-      ST(launch_batch_weno(b->stream, b->prec, p, b->probs, b->items_weno + b->deg_off[kBatchKindWeno][p],
-                           b->deg_cnt[kBatchKindWeno][p], b->deg_grid[kBatchKindWeno][p],
-                           kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out));
-  return FLSP_OK;
+  return batch_each_degree(b, kBatchKindWeno, [&](int p, cudaStream_t s) {
+    return launch_batch_weno(s, b->prec, p, b->probs, b->items_weno + b->deg_off[kBatchKindWeno][p],
+                             b->deg_cnt[kBatchKindWeno][p], b->deg_grid[kBatchKindWeno][p],
+                             kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out);
+  });
 }
 
 int batch_enqueue_step(flsp_batch* b) {
@@ -2039,6 +2068,11 @@ void flsp_batch_destroy(flsp_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_free_plan(b);
   for (flsp_handle* h : b->h) flsp_destroy(h);
+  for (int i = 0; i < 3; ++i) {
+    if (b->side[i]) cudaStreamDestroy(b->side[i]);
+    if (b->ev_join[i]) cudaEventDestroy(b->ev_join[i]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -2069,7 +2103,13 @@ int flsp_batch_create(int n, const flsp_mesh_desc* meshes, const flsp_dg_opts* o
     h->batch_member = true;
     b->h.push_back(h);
   }
-  if (cudaSetDevice(b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  bool ok = cudaSetDevice(b->dev) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < 3 && ok; ++i)
+    ok = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
     flsp_batch_destroy(b);
     return fail(FLSP_ERR_CUDA, "batch stream creation failed");
   }
