@@ -543,6 +543,7 @@ def plume_group_learned():
     net3.train(steps=3000, batch=8192, lr=1e-3, seed=1)
     r32 = plume_group(periods=400, net=net3, states=True)
     r64 = plume_group(periods=400, net=net3, precision=abi.FP64, timed=False, states=True)
+    nofb = plume_group(periods=40, net=net3, fallback=False)
     net3.close()
     s32, s64 = r32.pop("states"), r64.pop("states")
     l1, dmax = [], []
@@ -559,6 +560,7 @@ def plume_group_learned():
                     "one graph per period, 2000 SSP-RK3 steps, learned reinit every 5 steps (3x3x3-patch network "
                     "trained here on 24^3 sphere / plume pairs) with its residual fallback decided on the device",
             **r32,
+            "no_fallback_200_steps": {k: nofb[k] for k in ("dof_steps_per_s", "max_volume_change", "steps")},
             "fp64": {"dof_steps_per_s": r64["dof_steps_per_s"], "max_volume_change": r64["max_volume_change"],
                      "fallback_fraction": r64.get("fallback_fraction")},
             "fp32_vs_fp64": {"l1_interface_diff": l1, "max_coeff_diff_rel": dmax,

@@ -98,12 +98,15 @@ def make_batch(instances, precision=abi.FP32, cfl_max=0.1):
     return b
 
 
-def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, compare_problems=32, compare_steps=50):
+def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=5, compare_problems=256,
+                           compare_steps=100):
     """Batched configuration: DoF-steps/s of the whole batch (device time of
     `steps` steps with a reinit every `reinit_every`, CUDA events on the batch
-    stream) and the autotuner's report; on a subset, for comparison, the same
-    problems issued one after the other, each in its own graph-replayed run
-    on its own stream (so that they overlap on the GPU)."""
+    stream) and the autotuner's report; for comparison, on `compare_problems`
+    of the problems (all of them by default), the same problems issued one
+    after the other, each in its own graph-replayed run on its own stream (so
+    that they overlap on the GPU), against the batched launches, both by wall
+    clock over `compare_steps` steps."""
     import time
     import torch
     from .lib import check, load
@@ -127,7 +130,7 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
     finite = all(np.all(np.isfinite(p.get_state())) for p in b.problems[:16])
     n_dofs = b.n_dofs
     b.close()
-    # the same problems one by one (subset), each its own graph-replayed run
+    # the same problems one by one, each its own graph-replayed run on its own stream
     sub = inst[:compare_problems]
     singles = []
     for d in sub:
@@ -157,7 +160,7 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
     return {"problems": n_problems, "n_dofs": n_dofs, "steps": steps, "reinit_every": reinit_every,
             "pseudo_steps": n_pseudo, "device_ms": ms, "dof_steps_per_s": n_dofs * steps / (ms * 1e-3),
             "autotune": tune, "autotune_s": t_tune, "finite": bool(finite),
-            "subset_one_by_one": {"problems": compare_problems, "steps": compare_steps,
+            "streams_vs_batched": {"problems": compare_problems, "steps": compare_steps,
                                   "one_by_one_s": t_single, "batched_s": t_batch_sub,
                                   "one_by_one_dof_steps_per_s": sub_dofs * compare_steps / t_single,
                                   "batched_dof_steps_per_s": sub_dofs * compare_steps / t_batch_sub}}
