@@ -422,6 +422,12 @@ def run_ours(args):
                         "16 cosine modes; plain full-sweep reinit",
                 **variant_rate(abi.FP32, local, 128, F.plume_3d(), F.perturbed_plane(seed=5), 4)},
         }
+        line["variants"]["fe_velocity_64cubed"] = {
+            "what": "the headline workload with the velocity of a coupled FE simulator: the deformation field at "
+                    "t = 0 as a continuous Q2 nodal field on the Gauss-Lobatto lattice (flsp_set_velocity_fe, "
+                    "constant in time), evaluated per cell at the quadrature points by the point-wise stage kernel",
+            **variant_rate(abi.FP32, local, N_CELLS, F.deformation_3d(), F.sphere((0.35, 0.35, 0.35), 0.15), 10,
+                           fe_degree=2)}
         from felspa_b200.batch import plume_group
         line["variants"]["plume_group"] = {
             "what": "a large 3D run with side problems: the 128^3 Q2 FP32 plume problem and 8 side 64^3 problems (perturbed "
@@ -568,9 +574,11 @@ def plume_group_learned():
                                                                                       r64["volume_change"])]}}
 
 
-def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=0, band_cells=6.0):
+def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=0, band_cells=6.0, fe_degree=0):
     """DoF-steps/s (device time, CUDA events on the library stream) of `periods`
-    reinit periods (10 SSP-RK3 steps + 5 fixed pseudo-steps) of a 3D Q2 problem."""
+    reinit periods (10 SSP-RK3 steps + 5 fixed pseudo-steps) of a 3D Q2 problem.
+    fe_degree > 0: the velocity is the field at t = 0 sampled on the FE lattice
+    of that degree (flsp_set_velocity_fe), constant in time."""
     import torch
     from felspa_b200 import abi
     from felspa_b200.level_set import LevelSetSurface, Mesh
@@ -584,6 +592,9 @@ def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=
     # artificial viscosity
     ls.problem.set_velocity(velocity)
     ls.problem.project(ic)
+    if fe_degree:
+        from felspa_b200 import fields as F
+        ls.problem.set_velocity_fe(fe_degree, F.fe_lattice(lambda x: velocity(x, 0.0), (n_cells,) * 3, fe_degree))
     a0 = ls.integrate_mass()
     ls.run_steps(REINIT_EVERY)   # warm-up, graph capture
     s = torch.cuda.ExternalStream(ls.problem.stream(), device=device)
@@ -597,6 +608,12 @@ def variant_rate(precision, device, n_cells, velocity, ic, periods, narrow_band=
     out = {"n_dofs": ls.problem.n_dofs, "periods": periods, "device_ms": ms,
            "dof_steps_per_s": ls.problem.n_dofs * periods * REINIT_EVERY / (ms * 1e-3),
            "area_rel_change": (ls.integrate_mass() - a0) / a0}
+    if fe_degree:
+        ms_stage = ls.problem.time_kernel(0, reps=20)
+        s_b = 4 if precision == abi.FP32 else 8
+        out["stage_ms_per_launch"] = ms_stage
+        out["stage_algorithmic_bytes_per_launch"] = (8.0 / 3.0) * s_b * ls.problem.n_dofs
+        out["velocity_bytes_per_launch"] = 3 * (fe_degree * n_cells + 1) ** 3 * s_b
     ls.problem.close()
     return out
 

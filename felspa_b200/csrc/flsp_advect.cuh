@@ -59,13 +59,22 @@ __device__ __forceinline__ T term_val(const T* __restrict__ vx, const T* __restr
 // shared-memory footprint of the stage kernel: tile box with face halo,
 // velocity-table rows of the tile, upper-face fluxes shared with the
 // upper neighbours
+// nodes of a tile's block of an FE velocity lattice of degree pv, per component
+template <int DIM>
+__host__ __device__ inline int fe_block_nodes(const int* tile, int pv) {
+  return (pv * tile[0] + 1) * (pv * tile[1] + 1) * (DIM > 2 ? pv * tile[2] + 1 : 1);
+}
+
+// fe_pv > 0: the velocity rows are replaced by the tile's block of the FE
+// velocity lattice (every component)
 template <int DIM, int P, typename T>
-__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms) {
+__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms, int fe_pv = 0) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
   const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
-  size_t vt = (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
+  size_t vt = fe_pv > 0 ? (size_t)DIM * fe_block_nodes<DIM>(tile, fe_pv) * sizeof(T)
+                        : (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
   size_t fl = (size_t)DIM * NF * nt * sizeof(T);
   return box + vt + fl;
 }
@@ -182,9 +191,15 @@ __device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T c
 }
 
 // General velocity: a runtime sum of separable terms per component.  (A
-// velocity whose components are single terms takes adv_sep_kernel.)
+// velocity whose components are single terms takes adv_sep_kernel.)  FE:
+// the velocity of a coupled FE simulator, a continuous nodal field on the
+// Gauss-Lobatto lattice (VelArgs::fe_u), evaluated in every cell from the
+// cell's own nodes at the same quadrature points (advection.implement.h:
+// 891-905).  The basis is exactly 1 / 0 at a face's own / other nodes, so a
+// face's velocity from either of its cells is the same sum of the same
+// products of its shared nodes, bit for bit.
 // one tile of a stage (launch slot `slot`); a plain launch serves slot blockIdx.x
-template <int DIM, int P, typename T>
+template <int DIM, int P, typename T, bool FE = false>
 __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -196,12 +211,27 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   const int nterm = a.v.n_terms;
   const int span = tx + ty + (DIM > 2 ? tz : 0);
   T* vt = box + (size_t)nboxc * NM;
-  T* fl = vt + (size_t)max(nterm, 1) * span * NPT;   // [DIM][NF][nt]
+  const int pv = FE ? a.v.fe_pv : 0;
+  const int LX = pv * tx + 1, LY = pv * ty + 1, LZ = DIM > 2 ? pv * tz + 1 : 1;
+  T* fl = vt + (FE ? (size_t)DIM * LX * LY * LZ : (size_t)max(nterm, 1) * span * NPT);   // [DIM][NF][nt]
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM, slot);
 
-  // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
-  {
+  if constexpr (FE) {
+    // ---- stage the tile's block of the velocity lattice: vt[(comp*LZ + z)*LY + y)*LX + x]
+    // (nodes past the mesh, in a partial tile, repeat the last node)
+    const int lb = LX * LY * LZ;
+    const int total = DIM * lb;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int comp = e / lb, r = e % lb;
+      const int ix = r % LX, iy = (r / LX) % LY, iz = r / (LX * LY);
+      const int gx = min(pv * tc.ox + ix, a.v.fe_nx - 1);
+      const int gy = min(pv * tc.oy + iy, a.v.fe_ny - 1);
+      const int gz = DIM > 2 ? min(pv * tc.oz + iz, a.v.fe_nz - 1) : 0;
+      vt[e] = a.v.fe_u[(((size_t)comp * a.v.fe_nz + gz) * a.v.fe_ny + gy) * a.v.fe_nx + gx];
+    }
+  } else {
+    // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
     const int total = nterm * span * NPT;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       const int j = e % NPT;
@@ -245,6 +275,61 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     const int li = axis == 0 ? tc.lx : (axis == 1 ? tx + tc.ly : tx + ty + tc.lz);
     return vt + (size_t)(k * span + li) * NPT;
   };
+  // FE: the cell's first node in the staged lattice block, component stride
+  const int fe0 = pv * (tc.lx + LX * (tc.ly + LY * tc.lz));
+  const int lbn = LX * LY * LZ;
+  constexpr int NV = kMaxFeVel + 1;
+  // FE, cell term: the x-line of the cell's nodes contracted over y (and
+  // z) at table columns (jy, jz): ln[d][cx] = sum_cz sum_cy node * b_cy(jy)
+  // b_cz(jz); then u_d(jx, jy, jz) = sum_cx b_cx(jx) ln[d][cx]
+  auto fe_line = [&](int jy, int jz, T (&ln)[3][NV]) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int cx = 0; cx < NV; ++cx) ln[d][cx] = T(0);
+#pragma unroll 1
+    for (int cz = 0; cz <= (DIM > 2 ? pv : 0); ++cz)
+#pragma unroll 1
+      for (int cy = 0; cy <= pv; ++cy) {
+        T byz = a.v.fe_b[cy][jy];
+        if constexpr (DIM > 2) byz = byz * a.v.fe_b[cz][jz];
+        const T* row = vt + fe0 + LX * (cy + LY * cz);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+          for (int cx = 0; cx < NV; ++cx)
+            if (cx <= pv) ln[d][cx] += row[(size_t)d * lbn + cx] * byz;
+      }
+  };
+  auto fe_point = [&](const T (&ln)[3][NV], int jx, T* u) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      T s = T(0);
+#pragma unroll
+      for (int cx = 0; cx < NV; ++cx)
+        if (cx <= pv) s += a.v.fe_b[cx][jx] * ln[d][cx];
+      u[d] = s * ct;
+    }
+  };
+  // FE, faces: component E on face (E, S) at tangential columns (q0, q1),
+  // a sum over the face's own nodes only (the basis of the others is 0
+  // there), in one order from either cell: the same value bit for bit
+  auto fe_face = [&](auto EC, int S, int q0, int q1) -> T {
+    constexpr int E = decltype(EC)::value;
+    constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+    const int st[3] = {1, LX, LX * LY};
+    const T* base = vt + (size_t)E * lbn + fe0 + (S ? pv : 0) * st[E];
+    T u = T(0);
+#pragma unroll 1
+    for (int c1 = 0; c1 <= (DIM > 2 ? pv : 0); ++c1)
+#pragma unroll 1
+      for (int c0 = 0; c0 <= pv; ++c0) {
+        T b = a.v.fe_b[c0][q0];
+        if constexpr (DIM > 2) b = b * a.v.fe_b[c1][q1];
+        u += base[c0 * st[t0] + (DIM > 2 ? c1 * st[t1] : 0)] * b;
+      }
+    return u * ct;
+  };
   // velocity component `comp` (times the time factor) at table columns
   auto vel = [&](int comp, int jx, int jy, int jz) -> T {
     T u = T(0);
@@ -255,12 +340,14 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     }
     return u * ct;
   };
+  T fln[3][NV];   // FE: the current x-line (cell term)
 
   if (work) {
     // ============================ cell term ============================
     if constexpr (DIM == 2) {
 #pragma unroll 1
       for (int qy = 0; qy < NQ; ++qy) {
+        if constexpr (FE) fe_line(qy, 0, fln);
         T Py[N1];
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa) {
@@ -277,7 +364,10 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
           T phi = T(0);
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
-          const T u0 = vel(0, qx, qy, 0), u1 = vel(1, qx, qy, 0);
+          T uq[2];
+          if constexpr (FE) fe_point(fln, qx, uq);
+          else { uq[0] = vel(0, qx, qy, 0); uq[1] = vel(1, qx, qy, 0); }
+          const T u0 = uq[0], u1 = uq[1];
           const T w = tb.wq[qx] * tb.wq[qy] * phi;
           const T fx = w * u0 * ih[0];
           const T fy = w * u1 * ih[1];
@@ -313,6 +403,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
           for (int b = 0; b < N1; ++b) { U1[aa][b] = T(0); U3[aa][b] = T(0); }
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
+          if constexpr (FE) fe_line(qy, qz, fln);
           T Py[N1];
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) {
@@ -329,7 +420,10 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
             T phi = T(0);
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
-            const T u0 = vel(0, qx, qy, qz), u1 = vel(1, qx, qy, qz), u2 = vel(2, qx, qy, qz);
+            T uq[3];
+            if constexpr (FE) fe_point(fln, qx, uq);
+            else { uq[0] = vel(0, qx, qy, qz); uq[1] = vel(1, qx, qy, qz); uq[2] = vel(2, qx, qy, qz); }
+            const T u0 = uq[0], u1 = uq[1], u2 = uq[2];
             const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
             const T fx = w * u0 * ih[0];
             const T fy = w * u1 * ih[1];
@@ -372,7 +466,8 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
       if (DIM > 2) j[t1] = q1;
       T w = tb.wq[q0];
       if constexpr (DIM > 2) w = w * tb.wq[q1];
-      return vel(E, j[0], j[1], j[2]) * w;
+      if constexpr (FE) return fe_face(std::integral_constant<int, E>(), S, q0, q1) * w;
+      else return vel(E, j[0], j[1], j[2]) * w;
     };
   };
 
@@ -450,9 +545,9 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   store_tile<DIM, NM>(m, stage_buf, a.out, tc.ox, tc.oy, tc.oz);
 }
 
-template <int DIM, int P, typename T>
+template <int DIM, int P, typename T, bool FE>
 __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
-  adv_stage_tile<DIM, P, T>(a, (int)blockIdx.x);
+  adv_stage_tile<DIM, P, T, FE>(a, (int)blockIdx.x);
 }
 
 }  // namespace flsp

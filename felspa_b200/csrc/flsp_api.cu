@@ -127,6 +127,12 @@ struct flsp_handle {
   bool has_vel = false;
   flsp_velocity_desc vel;
   int nmax = 1, npt = 1;
+  // velocity of a coupled FE simulator (fe_pv > 0): nodal lattice in FP64
+  // (CFL) and in the state precision (fe_u == fe_u64 in FP64 mode)
+  int fe_pv = 0;
+  double* fe_u64 = nullptr;
+  void* fe_u = nullptr;
+  double fe_b[kMaxFeVel + 1][kMaxNQ + 2];
   DevClock* clk = nullptr;
   DevClock* clk_host = nullptr;   // pinned mirror
   int64_t* perm = nullptr;
@@ -206,6 +212,13 @@ struct flsp_handle {
     v.optab = v.sep1 ? optab : nullptr;
     v.opstride = opstride;
     v.err = clk ? &clk->err : nullptr;
+    if (fe_pv > 0) {
+      v.sep1 = false;
+      v.optab = nullptr;
+      v.fe_u = fe_u;
+      v.fe_pv = fe_pv;
+      std::memcpy(v.fe_b, fe_b, sizeof(fe_b));
+    }
     return v;
   }
 };
@@ -633,6 +646,38 @@ int build_optab(flsp_handle* h, const std::vector<double>& tabd) {
   return FLSP_OK;
 }
 
+// Gauss-Lobatto points of degree pv on [0, 1] (the support points of FE_Q(pv))
+void gauss_lobatto01(int pv, double* x) {
+  x[0] = 0.0;
+  x[pv] = 1.0;
+  if (pv == 2) x[1] = 0.5;
+  if (pv == 3) {
+    const double r = 0.5 / std::sqrt(5.0);
+    x[1] = 0.5 - r;
+    x[2] = 0.5 + r;
+  }
+}
+
+// Lagrange basis a of the nodes x[0..pv] at t; exactly 1 / 0 at the nodes
+// (numerator and denominator are the same products there)
+double lagrange(int pv, const double* x, int a, double t) {
+  double num = 1.0, den = 1.0;
+  for (int b = 0; b <= pv; ++b) {
+    if (b == a) continue;
+    num *= t - x[b];
+    den *= x[a] - x[b];
+  }
+  return num / den;
+}
+
+void free_fe_velocity(flsp_handle* h) {
+  if (h->fe_u && h->fe_u != h->fe_u64) cudaFree(h->fe_u);
+  if (h->fe_u64) cudaFree(h->fe_u64);
+  h->fe_u = nullptr;
+  h->fe_u64 = nullptr;
+  h->fe_pv = 0;
+}
+
 int build_vtab(flsp_handle* h) {
   const int dim = h->dim;
   layout_velocity(h);
@@ -977,6 +1022,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->hj_stab) cudaFree(h->hj_stab);
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
+  free_fe_velocity(h);
   if (h->optab) cudaFree(h->optab);
   void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_tot, h->lrn_save, h->lrn_feat,
                  h->nb_flags, h->nb_lists, h->nb_counts};
@@ -1021,9 +1067,57 @@ int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v) {
   }
   if (v->time_kind < 0 || v->time_kind > FLSP_T_ONE_MINUS_EXP) return fail(FLSP_ERR_BAD_ARG, "bad time kind");
   CU(cudaSetDevice(h->dev));
+  CU(cudaStreamSynchronize(h->stream));
+  free_fe_velocity(h);
   h->vel = *v;
   ST(build_vtab(h));
   h->has_vel = true;
+  clear_graphs(h);
+  return prepare_kernels(h);
+}
+
+int flsp_set_velocity_fe(flsp_handle* h, int degree, const double* values, int64_t n) {
+  if (!h || !values) return fail(FLSP_ERR_BAD_ARG, "null argument");
+  if (degree < 1 || degree > FLSP_MAX_FE_VEL_DEGREE) return fail(FLSP_ERR_BAD_ARG, "FE velocity degree out of range");
+  if (h->batch_member) return fail(FLSP_ERR_UNSUPPORTED, "FE velocity on a batch member");
+  long long nn = 1;
+  for (int d = 0; d < h->dim; ++d) nn *= (long long)degree * h->m.n[d] + 1;
+  if (n != (int64_t)h->dim * nn) return fail(FLSP_ERR_BAD_ARG, "FE velocity size mismatch");
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(values[i])) return fail(FLSP_ERR_BAD_ARG, "non-finite FE velocity value");
+  CU(cudaSetDevice(h->dev));
+  const bool same = h->fe_pv == degree && h->fe_u64 != nullptr;
+  if (!same) {
+    // an FE field has no analytic terms: zero tables, time factor 1
+    CU(cudaStreamSynchronize(h->stream));
+    free_fe_velocity(h);
+    std::memset(&h->vel, 0, sizeof(h->vel));
+    h->vel.time_kind = FLSP_T_ONE;
+    ST(build_vtab(h));
+    CU(cudaMalloc(&h->fe_u64, (size_t)n * sizeof(double)));
+    if (h->prec == FLSP_FP64) h->fe_u = h->fe_u64;
+    else CU(cudaMalloc(&h->fe_u, (size_t)n * sizeof(float)));
+    double gl[kMaxFeVel + 1], xq[8], wq[8];
+    gauss_lobatto01(degree, gl);
+    const int nq = h->p + 2;
+    gauss_rule(nq, xq, wq);
+    std::memset(h->fe_b, 0, sizeof(h->fe_b));
+    for (int a = 0; a <= degree; ++a) {
+      for (int j = 0; j < nq; ++j) h->fe_b[a][j] = lagrange(degree, gl, a, xq[j]);
+      h->fe_b[a][nq] = lagrange(degree, gl, a, 0.0);
+      h->fe_b[a][nq + 1] = lagrange(degree, gl, a, 1.0);
+    }
+    h->fe_pv = degree;
+  }
+  // in place: ordered after the work already queued on the problem's stream
+  CU(cudaMemcpyAsync(h->fe_u64, values, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  Ctx c = h->ctx();
+  if (h->prec != FLSP_FP64) ST(launch_to_float(c, h->fe_u64, static_cast<float*>(h->fe_u), n));
+  CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
+  ST(launch_fe_static_cfl(c, h->fe_u64, degree, h->clk));
+  CU(cudaStreamSynchronize(h->stream));
+  h->has_vel = true;
+  if (same) return FLSP_OK;
   clear_graphs(h);
   return prepare_kernels(h);
 }

@@ -18,6 +18,7 @@ constexpr int kMaxP = 3;
 constexpr int kMaxN1 = kMaxP + 1;   // modes per axis
 constexpr int kMaxNQ = kMaxP + 2;   // Gauss points per axis (p+2 rule)
 constexpr int kMaxTerms = 24;
+constexpr int kMaxFeVel = 3;        // largest degree of an FE velocity field
 
 __host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 
@@ -209,6 +210,13 @@ struct VelArgs {
   int npt;
   int comp[kMaxTerms];
   int cstart[4];   // terms of component c: [cstart[c], cstart[c+1]) (terms sorted by component)
+  // velocity of a coupled FE simulator (fe_pv > 0, no terms): the continuous
+  // nodal field of degree fe_pv on the mesh's Gauss-Lobatto lattice,
+  // fe_u[((comp * fe_nz + z) * fe_ny + y) * fe_nx + x], fe_n* = fe_pv * n + 1
+  const T* fe_u;
+  int fe_pv;
+  int fe_nx, fe_ny, fe_nz;
+  T fe_b[kMaxFeVel + 1][kMaxNQ + 2];   // Lagrange basis a at Gauss point j, j = NQ: xi = 0, NQ + 1: xi = 1
 };
 
 // first term of each component in a component-sorted term list

@@ -88,6 +88,23 @@ int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int
   return launch_status("static_cfl_kernel");
 }
 
+int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk) {
+  const int nx = pv * c.m.n[0] + 1, ny = pv * c.m.n[1] + 1, nz = c.dim > 2 ? pv * c.m.n[2] + 1 : 1;
+  const int threads = 256;
+  const int blocks = (int)((c.m.ncell + threads - 1) / threads);
+  if (c.dim == 2) fe_static_cfl_kernel<2><<<blocks, threads, 0, c.stream>>>(c.m, u64, pv, nx, ny, nz, clk);
+  else fe_static_cfl_kernel<3><<<blocks, threads, 0, c.stream>>>(c.m, u64, pv, nx, ny, nz, clk);
+  return launch_status("fe_static_cfl_kernel");
+}
+
+int launch_to_float(const Ctx& c, const double* x, float* y, long long n) {
+  const int threads = 256;
+  const long long want = (n + threads - 1) / threads;
+  const int blocks = (int)std::max<long long>(1, std::min<long long>(want, 148LL * 16));
+  to_float_kernel<<<blocks, threads, 0, c.stream>>>(x, y, n);
+  return launch_status("to_float_kernel");
+}
+
 int reduce_blocks(const Ctx& c) { return (int)((c.m.ncell + 127) / 128); }
 
 int launch_reduce(const Ctx& c, int which, const void* phi, const void* ref,

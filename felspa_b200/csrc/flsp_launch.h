@@ -137,6 +137,10 @@ struct VelDev {
   const void* optab;   // per-axis operator rows of a sep1 velocity (T precision), or null
   int opstride;        // operator rows per (component, axis) in optab
   int* err;            // device error word (DevClock::err)
+  // FE velocity field (fe_pv > 0): T-precision nodal lattice and basis table
+  const void* fe_u;
+  int fe_pv;
+  double fe_b[kMaxFeVel + 1][kMaxNQ + 2];
 };
 // stage kernel of this velocity: separable-operator kernel when optab is set
 inline bool use_sep_kernel(const VelDev& v) { return v.sep1 && v.optab != nullptr; }
@@ -174,6 +178,10 @@ int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count);
 int launch_project_ic(const Ctx& c, const flsp_ic_desc* ic_dev, void* out);
 int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int* comp, int nmax,
                       int npt, DevClock* clk);
+// static CFL part of an FE velocity lattice (FP64, degree pv), max-ed into clk->vd_static
+int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk);
+// y[i] = (float)x[i]
+int launch_to_float(const Ctx& c, const double* x, float* y, long long n);
 // two-level FP64 reduction; partial holds 2 * reduce_blocks(c) doubles,
 // out_dev receives two doubles (sum pair, or max)
 int launch_reduce(const Ctx& c, int which, const void* phi, const void* ref,

@@ -225,6 +225,41 @@ __global__ void static_cfl_kernel(const MeshArgs m, const VelArgs<double> v, Dev
   }
 }
 
+// the same estimate for an FE velocity lattice of degree pv (fe_n* nodes per
+// axis, FP64): a cell's vertex velocities are its corner nodes
+template <int DIM>
+__global__ void fe_static_cfl_kernel(const MeshArgs m, const double* __restrict__ u, int pv, int nx, int ny,
+                                     int nz, DevClock* clk) {
+  __shared__ double red[32];
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double best = 0.0;
+  if (cell < m.ncell) {
+    const int g[3] = {(int)(cell % m.n[0]), (int)((cell / m.n[0]) % m.n[1]),
+                      DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0};
+    const size_t nn = (size_t)nx * ny * nz;
+    for (int vv = 0; vv < (1 << DIM); ++vv) {
+      const int x = pv * (g[0] + (vv & 1)), y = pv * (g[1] + ((vv >> 1) & 1));
+      const int z = DIM > 2 ? pv * (g[2] + ((vv >> 2) & 1)) : 0;
+      const size_t node = ((size_t)z * ny + y) * nx + x;
+      double s = 0.0;
+      for (int d = 0; d < DIM; ++d) s += u[d * nn + node] * u[d * nn + node];
+      best = fmax(best, sqrt(s));
+    }
+    best /= m.diam;
+  }
+  const double bm = block_max(best, red);
+  if (threadIdx.x == 0) {
+    unsigned long long* slot = reinterpret_cast<unsigned long long*>(&clk->vd_static);
+    atomic_max_pos(slot, bm);
+  }
+}
+
+// FP64 -> FP32 copy of a device array
+__global__ void to_float_kernel(const double* __restrict__ x, float* __restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
 // ---------------------------------------------------------------------
 // FP64 reductions (level_set.implement.h:215-295, 356-380, 957-993;
 // advection.cc:452-484; reinit.cc:491-526).  Two levels, fixed order.

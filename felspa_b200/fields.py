@@ -182,6 +182,52 @@ def constant(u):
 
 
 # ----------------------------------------------------------------------
+# velocity of a coupled FE simulator: nodal lattice (flsp_set_velocity_fe)
+# ----------------------------------------------------------------------
+def gauss_lobatto01(degree):
+    """the degree+1 Gauss-Lobatto points on [0, 1] (FE_Q support points)"""
+    if degree == 1:
+        return np.array([0.0, 1.0])
+    if degree == 2:
+        return np.array([0.0, 0.5, 1.0])
+    if degree == 3:
+        r = 0.5 / math.sqrt(5.0)
+        return np.array([0.0, 0.5 - r, 0.5 + r, 1.0])
+    raise ValueError("FE velocity degree must be 1..3")
+
+
+def fe_lattice_coords(n, degree, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """per-axis node coordinates of the lattice: node I of axis e at
+    lo + h (I // degree + x_{I % degree})"""
+    x = gauss_lobatto01(degree)
+    out = []
+    for e, ne in enumerate(n):
+        h = (hi[e] - lo[e]) / ne
+        idx = np.arange(degree * ne + 1)
+        cell = np.minimum(idx // degree, ne - 1)
+        out.append(lo[e] + h * (cell + x[idx - degree * cell]))
+    return out
+
+
+def fe_lattice(fn, n, degree, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """sample fn(x[..., dim]) -> u[..., dim] at the lattice nodes; returns
+    the flsp_set_velocity_fe array (components, then z, y, x)"""
+    dim = len(n)
+    cs = fe_lattice_coords(n, degree, lo, hi)
+    grid = np.meshgrid(*cs[::-1], indexing="ij")[::-1]     # x fastest in memory
+    x = np.stack(grid, axis=-1)
+    u = np.asarray(fn(x), dtype=np.float64)
+    return np.ascontiguousarray(np.moveaxis(u, -1, 0)).reshape((dim,) + x.shape[:-1])
+
+
+def random_fe_lattice(n, degree, seed, scale=1.0):
+    """a continuous field of random node values (any lattice is one)"""
+    rng = np.random.default_rng(seed)
+    shape = (len(n),) + tuple(degree * ne + 1 for ne in n[::-1])
+    return scale * rng.uniform(-1.0, 1.0, size=shape)
+
+
+# ----------------------------------------------------------------------
 # initial conditions
 # ----------------------------------------------------------------------
 class IC:

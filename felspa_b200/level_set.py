@@ -169,6 +169,13 @@ class Problem:
         self._vdesc = field.desc()
         check(load().flsp_set_velocity(self.h, C.byref(self._vdesc)))
 
+    def set_velocity_fe(self, degree, values):
+        """velocity of a coupled FE simulator (flsp_set_velocity_fe): the
+        continuous nodal field of degree 1..3 on the mesh's Gauss-Lobatto
+        lattice, components then z, y, x (fields.fe_lattice samples one)"""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(load().flsp_set_velocity_fe(self.h, int(degree), v.ctypes.data_as(C.POINTER(C.c_double)), v.size))
+
     def project(self, ic):
         self._icdesc = ic.desc()
         check(load().flsp_project_ic(self.h, C.byref(self._icdesc)))

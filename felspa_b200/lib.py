@@ -30,6 +30,7 @@ PROTOTYPES = {
     "flsp_n_dofs": (C.c_int, [_vp, _i64p]),
     "flsp_dofs_per_cell": (C.c_int, [_vp, _ip]),
     "flsp_set_velocity": (C.c_int, [_vp, C.POINTER(abi.VelocityDesc)]),
+    "flsp_set_velocity_fe": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.c_int64]),
     "flsp_project_ic": (C.c_int, [_vp, C.POINTER(abi.ICDesc)]),
     "flsp_set_state": (C.c_int, [_vp, _dp, C.c_int64]),
     "flsp_get_state": (C.c_int, [_vp, _dp, C.c_int64]),

@@ -245,6 +245,28 @@ int flsp_dofs_per_cell(const flsp_handle* h, int* n);
 
 /* state -------------------------------------------------------------- */
 int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v);
+/* Velocity from a coupled finite-element simulator (the advection
+   assembler's simulator branch, advection.implement.h:472-477,891-905;
+   the Stokes extractor, stokes_common.implement.h:583-591): a continuous
+   nodal field of degree `degree` (1..FLSP_MAX_FE_VEL_DEGREE) per axis,
+   the FE_Q field of the coupled simulator on this mesh, evaluated at the
+   advection's own quadrature points in every cell.
+   `values` holds the field at the Gauss-Lobatto support points of every
+   cell (for degree 1 and 2 the equispaced vertices / edge midpoints):
+   on axis e node I sits at lo[e] + h[e]*(I/degree + x_{I%degree}), x the
+   degree+1 Gauss-Lobatto points on [0,1], I = 0..degree*n[e]; nodes x
+   fastest, then y (then z), one block per component: n = dim *
+   prod_e (degree*n[e] + 1).  A face's velocity is the same from both of
+   its cells (the nodes on the face are shared).  The field is constant
+   in time.  The CFL estimate is the largest node |u| at a cell vertex
+   over the cell diameter (CFLEstimator, pde_tools.implement.h:18-67).
+   Setting a field of the same degree again rewrites the device copy in
+   place (on the problem's stream): captured graphs stay valid, so a
+   coupled loop updates the velocity between advance calls without
+   re-capture.  flsp_set_velocity replaces an FE field.  Not supported for
+   members of a batch.                                                    */
+#define FLSP_MAX_FE_VEL_DEGREE 3
+int flsp_set_velocity_fe(flsp_handle* h, int degree, const double* values, int64_t n);
 int flsp_project_ic(flsp_handle* h, const flsp_ic_desc* ic);
 int flsp_set_state(flsp_handle* h, const double* coeffs, int64_t n);
 int flsp_get_state(flsp_handle* h, double* coeffs, int64_t n);

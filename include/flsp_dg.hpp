@@ -92,6 +92,15 @@ class AdvectSimulator {
     check(flsp_set_velocity(h(), &velocity), "flsp_set_velocity");
     set_solution_vector(coeffs);
   }
+  // the simulator velocity branch (VeloFcnType a simulator, e.g. the Stokes
+  // solver of LevelSetStokes): the coupled FE field as nodal values of
+  // degree `degree` on the mesh's Gauss-Lobatto lattice, components then
+  // z, y, x (flsp_set_velocity_fe); call again after every solve of the
+  // coupled simulator
+  void set_velocity_field(int degree, const std::vector<double>& nodal_values) {
+    check(flsp_set_velocity_fe(h(), degree, nodal_values.data(), (int64_t)nodal_values.size()),
+          "flsp_set_velocity_fe");
+  }
   // explicit_time_derivative(t, current solution) = M^-1 R(phi, t)
   std::vector<double> explicit_time_derivative(double current_time) const {
     std::vector<double> out(problem_.n_dofs());

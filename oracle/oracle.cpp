@@ -99,6 +99,11 @@ struct orc_problem {
   std::vector<std::array<int, 3>> modes;
   bool has_vel = false;
   flsp_velocity_desc vel;
+  // velocity of a coupled FE simulator: nodal lattice of degree fe_pv (0: none)
+  int fe_pv = 0;
+  int fe_nn[3] = {1, 1, 1};
+  double fe_x[4];                 // Gauss-Lobatto nodes on [0, 1]
+  std::vector<double> fe_u;       // [comp][z][y][x]
 
   Quad qc, ql;           // QGauss(p+2), QGauss(p+1)
   FaceQuad fc[6], fl[6]; // per face: QGauss<dim-1>(p+2) / (p+1)
@@ -282,6 +287,40 @@ double time_factor(const flsp_velocity_desc& v, double t) {
     case FLSP_T_ONE_MINUS_EXP: return 1.0 - std::exp(-v.ta * t);
   }
   return 1.0;
+}
+
+// Lagrange basis a of the nodes x[0..pv] at t (1 / 0 at the nodes exactly)
+double fe_basis(int pv, const double* x, int a, double t) {
+  double num = 1.0, den = 1.0;
+  for (int b = 0; b <= pv; ++b)
+    if (b != a) {
+      num *= t - x[b];
+      den *= x[a] - x[b];
+    }
+  return num / den;
+}
+
+// The simulator branch of the advection assembler (advection.implement.h:
+// 891-905, stokes_common.implement.h:583-591): the coupled FE field of cell
+// c at reference point xi, sum over the cell's nodes (x fastest) of the
+// node value times the basis products
+void fe_velocity(const orc_problem* pr, long c, const double* xi, double* u) {
+  int I[3];
+  pr->ijk(c, I);
+  const int pv = pr->fe_pv;
+  const size_t nn = (size_t)pr->fe_nn[0] * pr->fe_nn[1] * pr->fe_nn[2];
+  for (int d = 0; d < 3; ++d) u[d] = 0.0;
+  for (int cz = 0; cz <= (pr->dim > 2 ? pv : 0); ++cz)
+    for (int cy = 0; cy <= pv; ++cy) {
+      double byz = fe_basis(pv, pr->fe_x, cy, xi[1]);
+      if (pr->dim > 2) byz *= fe_basis(pv, pr->fe_x, cz, xi[2]);
+      for (int cx = 0; cx <= pv; ++cx) {
+        const double b = fe_basis(pv, pr->fe_x, cx, xi[0]) * byz;
+        const size_t node = ((size_t)(pr->dim > 2 ? pv * I[2] + cz : 0) * pr->fe_nn[1] + pv * I[1] + cy) *
+                                pr->fe_nn[0] + pv * I[0] + cx;
+        for (int d = 0; d < pr->dim; ++d) u[d] += pr->fe_u[d * nn + node] * b;
+      }
+    }
 }
 
 void velocity(const orc_problem* pr, const double* x, double t, double* u) {
@@ -534,6 +573,29 @@ int orc_set_velocity(orc_problem* pr, const flsp_velocity_desc* v) {
   for (int k = 0; k < v->n_terms; ++k)
     if (v->terms[k].comp < 0 || v->terms[k].comp >= pr->dim) return FLSP_ERR_BAD_ARG;
   pr->vel = *v;
+  pr->fe_pv = 0;
+  pr->fe_u.clear();
+  pr->has_vel = true;
+  return FLSP_OK;
+}
+
+int orc_set_velocity_fe(orc_problem* pr, int degree, const double* values, long n) {
+  if (!values || degree < 1 || degree > 3) return FLSP_ERR_BAD_ARG;
+  long nn = 1;
+  for (int d = 0; d < 3; ++d) pr->fe_nn[d] = d < pr->dim ? degree * pr->n[d] + 1 : 1;
+  for (int d = 0; d < pr->dim; ++d) nn *= pr->fe_nn[d];
+  if (n != pr->dim * nn) return FLSP_ERR_BAD_ARG;
+  pr->fe_pv = degree;
+  // Gauss-Lobatto points of degree 1..3 on [0, 1]
+  pr->fe_x[0] = 0.0;
+  pr->fe_x[degree] = 1.0;
+  if (degree == 2) pr->fe_x[1] = 0.5;
+  if (degree == 3) {
+    pr->fe_x[1] = 0.5 - 0.5 / std::sqrt(5.0);
+    pr->fe_x[2] = 0.5 + 0.5 / std::sqrt(5.0);
+  }
+  pr->fe_u.assign(values, values + n);
+  std::memset(&pr->vel, 0, sizeof(pr->vel));   // constant in time
   pr->has_vel = true;
   return FLSP_OK;
 }
@@ -590,7 +652,8 @@ int orc_advect_rhs(orc_problem* pr, const double* phi, double t, double* phidot)
       sq[q] = eval_at(pc, pr->vc, nb, np, q);
       double x[3];
       for (int d = 0; d < 3; ++d) x[d] = X0[d] + pr->h[d] * pr->qc.xi[q][d];
-      velocity(pr, x, t, uq[q]);
+      if (pr->fe_pv) fe_velocity(pr, c, pr->qc.xi[q].data(), uq[q]);
+      else velocity(pr, x, t, uq[q]);
     }
     for (int i = 0; i < nb; ++i)
       for (int q = 0; q < np; ++q) {
@@ -615,7 +678,9 @@ int orc_advect_rhs(orc_problem* pr, const double* phi, double t, double* phidot)
         double pex = nbc >= 0 ? eval_at(phi + nbc * nb, vex, nb, fq.np, q) : (std::isnan(gbc) ? pin : gbc);
         double x[3], u[3];
         for (int d = 0; d < 3; ++d) x[d] = X0[d] + pr->h[d] * fq.xi[q][d];
-        velocity(pr, x, t, u);
+        // FE field: continuous, so the face value is the same from either cell
+        if (pr->fe_pv) fe_velocity(pr, c, fq.xi[q].data(), u);
+        else velocity(pr, x, t, u);
         double vn = s ? u[ax] : -u[ax];
         double up = vn > 0.0 ? pin : pex;
         double jxw = fq.w[q] * area;
@@ -639,7 +704,9 @@ double orc_advect_cfl(orc_problem* pr, double t) {
     for (int v = 0; v < pr->nvert; ++v) {
       double x[3] = {X0[0], X0[1], X0[2]}, u[3];
       for (int d = 0; d < pr->dim; ++d) if ((v >> d) & 1) x[d] += pr->h[d];
-      velocity(pr, x, t, u);
+      const double xi[3] = {(double)(v & 1), (double)((v >> 1) & 1), (double)((v >> 2) & 1)};
+      if (pr->fe_pv) fe_velocity(pr, c, xi, u);
+      else velocity(pr, x, t, u);
       double s = 0.0;
       for (int d = 0; d < pr->dim; ++d) s += u[d] * u[d];
       m = std::max(m, std::sqrt(s));

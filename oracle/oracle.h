@@ -62,6 +62,9 @@ void orc_shape(const orc_problem* pr, int npts, const double* xi,
                double* val, double* grad);
 
 int orc_set_velocity(orc_problem* pr, const flsp_velocity_desc* v);
+/* velocity of a coupled FE simulator: continuous nodal field of degree
+   1..3 on the Gauss-Lobatto lattice (layout of flsp_set_velocity_fe) */
+int orc_set_velocity_fe(orc_problem* pr, int degree, const double* values, long n);
 void orc_eval_velocity(const orc_problem* pr, const double* x, double t,
                        double* u);
 double orc_eval_ic(const flsp_ic_desc* ic, int dim, const double* x);

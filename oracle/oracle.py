@@ -47,6 +47,7 @@ def lib():
         L.orc_legendre.argtypes = [C.c_int, C.c_double, _dp, _dp, _dp]
         L.orc_shape.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp]
         L.orc_set_velocity.argtypes = [C.c_void_p, C.POINTER(abi.VelocityDesc)]
+        L.orc_set_velocity_fe.argtypes = [C.c_void_p, C.c_int, _dp, C.c_long]
         L.orc_eval_velocity.argtypes = [C.c_void_p, _dp, C.c_double, _dp]
         L.orc_eval_ic.argtypes = [C.POINTER(abi.ICDesc), C.c_int, _dp]
         L.orc_eval_ic.restype = C.c_double
@@ -144,6 +145,14 @@ class Problem:
         self.velocity = field
         self._vdesc = field.desc()
         _check(lib().orc_set_velocity(self.h, C.byref(self._vdesc)), "set_velocity")
+
+    def set_velocity_fe(self, degree, values):
+        """velocity of a coupled FE simulator: the nodal lattice of
+        flsp_set_velocity_fe (components, then z, y, x)"""
+        self.velocity = None
+        self._fe_values = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        _check(lib().orc_set_velocity_fe(self.h, int(degree), _p(self._fe_values), self._fe_values.size),
+               "set_velocity_fe")
 
     def eval_velocity(self, x, t=0.0):
         xx = np.zeros(3)
