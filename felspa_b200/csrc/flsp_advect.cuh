@@ -59,22 +59,15 @@ __device__ __forceinline__ T term_val(const T* __restrict__ vx, const T* __restr
 // shared-memory footprint of the stage kernel: tile box with face halo,
 // velocity-table rows of the tile, upper-face fluxes shared with the
 // upper neighbours
-// nodes of a tile's block of an FE velocity lattice of degree pv, per component
-template <int DIM>
-__host__ __device__ inline int fe_block_nodes(const int* tile, int pv) {
-  return (pv * tile[0] + 1) * (pv * tile[1] + 1) * (DIM > 2 ? pv * tile[2] + 1 : 1);
-}
-
-// fe_pv > 0: the velocity rows are replaced by the tile's block of the FE
-// velocity lattice (every component)
+// fe: the velocity is read from the FE tables (VelArgs::fe_q / fe_f), no
+// velocity rows in shared memory
 template <int DIM, int P, typename T>
-__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms, int fe_pv = 0) {
+__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms, bool fe = false) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
   const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
-  size_t vt = fe_pv > 0 ? (size_t)DIM * fe_block_nodes<DIM>(tile, fe_pv) * sizeof(T)
-                        : (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
+  size_t vt = fe ? 0 : (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
   size_t fl = (size_t)DIM * NF * nt * sizeof(T);
   return box + vt + fl;
 }
@@ -141,11 +134,15 @@ __device__ __forceinline__ void face_flux(const Tab1D<T>& tb, const T* c, const 
         Pi[q0][m1] = si;
         Pe[q0][m1] = sx;
       }
-    T G[N1][NQ];
 #pragma unroll
+    for (int mf = 0; mf < NF; ++mf) Fm[mf] = T(0);
+    // one q1 line at a time (not unrolled: the body is inlined for every
+    // face of the cell), Fm[m0 + N1 m1] = sum_q1 G[m0](q1) L_m1(q1)
+#pragma unroll 1
     for (int q1 = 0; q1 < NQ; ++q1) {
+      T G[N1];
 #pragma unroll
-      for (int m0 = 0; m0 < N1; ++m0) G[m0][q1] = T(0);
+      for (int m0 = 0; m0 < N1; ++m0) G[m0] = T(0);
 #pragma unroll
       for (int q0 = 0; q0 < NQ; ++q0) {
         T pin = T(0), pex = T(0);
@@ -159,18 +156,13 @@ __device__ __forceinline__ void face_flux(const Tab1D<T>& tb, const T* c, const 
         const T up = vn > T(0) ? pin : pex;
         const T F = vn * up;
 #pragma unroll
-        for (int m0 = 0; m0 < N1; ++m0) G[m0][q1] += F * tb.Lq[m0][q0];
+        for (int m0 = 0; m0 < N1; ++m0) G[m0] += F * tb.Lq[m0][q0];
       }
+#pragma unroll
+      for (int m1 = 0; m1 < N1; ++m1)
+#pragma unroll
+        for (int m0 = 0; m0 < N1; ++m0) Fm[m0 + N1 * m1] += G[m0] * tb.Lq[m1][q1];
     }
-#pragma unroll
-    for (int m1 = 0; m1 < N1; ++m1)
-#pragma unroll
-      for (int m0 = 0; m0 < N1; ++m0) {
-        T s2 = T(0);
-#pragma unroll
-        for (int q1 = 0; q1 < NQ; ++q1) s2 += G[m0][q1] * tb.Lq[m1][q1];
-        Fm[m0 + N1 * m1] = s2;
-      }
   }
 }
 
@@ -192,12 +184,9 @@ __device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T c
 
 // General velocity: a runtime sum of separable terms per component.  (A
 // velocity whose components are single terms takes adv_sep_kernel.)  FE:
-// the velocity of a coupled FE simulator, a continuous nodal field on the
-// Gauss-Lobatto lattice (VelArgs::fe_u), evaluated in every cell from the
-// cell's own nodes at the same quadrature points (advection.implement.h:
-// 891-905).  The basis is exactly 1 / 0 at a face's own / other nodes, so a
-// face's velocity from either of its cells is the same sum of the same
-// products of its shared nodes, bit for bit.
+// the velocity of a coupled FE simulator, tabulated once per field update
+// (fe_tabulate_*): at every cell's quadrature points and, single-valued, at
+// every face's (advection.implement.h:891-905).
 // one tile of a stage (launch slot `slot`); a plain launch serves slot blockIdx.x
 template <int DIM, int P, typename T, bool FE = false>
 __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
@@ -211,26 +200,11 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   const int nterm = a.v.n_terms;
   const int span = tx + ty + (DIM > 2 ? tz : 0);
   T* vt = box + (size_t)nboxc * NM;
-  const int pv = FE ? a.v.fe_pv : 0;
-  const int LX = pv * tx + 1, LY = pv * ty + 1, LZ = DIM > 2 ? pv * tz + 1 : 1;
-  T* fl = vt + (FE ? (size_t)DIM * LX * LY * LZ : (size_t)max(nterm, 1) * span * NPT);   // [DIM][NF][nt]
+  T* fl = vt + (FE ? 0 : (size_t)max(nterm, 1) * span * NPT);   // [DIM][NF][nt]
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM, slot);
 
-  if constexpr (FE) {
-    // ---- stage the tile's block of the velocity lattice: vt[(comp*LZ + z)*LY + y)*LX + x]
-    // (nodes past the mesh, in a partial tile, repeat the last node)
-    const int lb = LX * LY * LZ;
-    const int total = DIM * lb;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int comp = e / lb, r = e % lb;
-      const int ix = r % LX, iy = (r / LX) % LY, iz = r / (LX * LY);
-      const int gx = min(pv * tc.ox + ix, a.v.fe_nx - 1);
-      const int gy = min(pv * tc.oy + iy, a.v.fe_ny - 1);
-      const int gz = DIM > 2 ? min(pv * tc.oz + iz, a.v.fe_nz - 1) : 0;
-      vt[e] = a.v.fe_u[(((size_t)comp * a.v.fe_nz + gz) * a.v.fe_ny + gy) * a.v.fe_nx + gx];
-    }
-  } else {
+  if constexpr (!FE) {
     // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
     const int total = nterm * span * NPT;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
@@ -275,60 +249,23 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     const int li = axis == 0 ? tc.lx : (axis == 1 ? tx + tc.ly : tx + ty + tc.lz);
     return vt + (size_t)(k * span + li) * NPT;
   };
-  // FE: the cell's first node in the staged lattice block, component stride
-  const int fe0 = pv * (tc.lx + LX * (tc.ly + LY * tc.lz));
-  const int lbn = LX * LY * LZ;
-  constexpr int NV = kMaxFeVel + 1;
-  // FE, cell term: the x-line of the cell's nodes contracted over y (and
-  // z) at table columns (jy, jz): ln[d][cx] = sum_cz sum_cy node * b_cy(jy)
-  // b_cz(jz); then u_d(jx, jy, jz) = sum_cx b_cx(jx) ln[d][cx]
-  auto fe_line = [&](int jy, int jz, T (&ln)[3][NV]) {
+  // FE: the tables at this cell's quadrature points ([comp][point][cell],
+  // cell lexicographic) and at its faces ([E][point][face], face index
+  // lexicographic over n + e_E faces)
+  const long long fe_cell = tc.gx + (long long)m.n[0] * (tc.gy + (long long)m.n[1] * tc.gz);
+  auto fe_point = [&](int qx, int qy, int qz, T* u) {
+    constexpr int NQD = ipow(NQ, DIM);
+    const int q = qx + NQ * (qy + NQ * qz);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d)
-#pragma unroll
-      for (int cx = 0; cx < NV; ++cx) ln[d][cx] = T(0);
-#pragma unroll 1
-    for (int cz = 0; cz <= (DIM > 2 ? pv : 0); ++cz)
-#pragma unroll 1
-      for (int cy = 0; cy <= pv; ++cy) {
-        T byz = a.v.fe_b[cy][jy];
-        if constexpr (DIM > 2) byz = byz * a.v.fe_b[cz][jz];
-        const T* row = vt + fe0 + LX * (cy + LY * cz);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d)
-#pragma unroll
-          for (int cx = 0; cx < NV; ++cx)
-            if (cx <= pv) ln[d][cx] += row[(size_t)d * lbn + cx] * byz;
-      }
+    for (int d = 0; d < DIM; ++d) u[d] = a.v.fe_q[((size_t)d * NQD + q) * m.ncell + fe_cell] * ct;
   };
-  auto fe_point = [&](const T (&ln)[3][NV], int jx, T* u) {
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      T s = T(0);
-#pragma unroll
-      for (int cx = 0; cx < NV; ++cx)
-        if (cx <= pv) s += a.v.fe_b[cx][jx] * ln[d][cx];
-      u[d] = s * ct;
-    }
-  };
-  // FE, faces: component E on face (E, S) at tangential columns (q0, q1),
-  // a sum over the face's own nodes only (the basis of the others is 0
-  // there), in one order from either cell: the same value bit for bit
   auto fe_face = [&](auto EC, int S, int q0, int q1) -> T {
     constexpr int E = decltype(EC)::value;
-    constexpr int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
-    const int st[3] = {1, LX, LX * LY};
-    const T* base = vt + (size_t)E * lbn + fe0 + (S ? pv : 0) * st[E];
-    T u = T(0);
-#pragma unroll 1
-    for (int c1 = 0; c1 <= (DIM > 2 ? pv : 0); ++c1)
-#pragma unroll 1
-      for (int c0 = 0; c0 <= pv; ++c0) {
-        T b = a.v.fe_b[c0][q0];
-        if constexpr (DIM > 2) b = b * a.v.fe_b[c1][q1];
-        u += base[c0 * st[t0] + (DIM > 2 ? c1 * st[t1] : 0)] * b;
-      }
-    return u * ct;
+    int f[3] = {tc.gx, tc.gy, tc.gz};
+    f[E] += S;
+    const long long nf0 = m.n[0] + (E == 0), nf1 = m.n[1] + (E == 1);
+    const long long face = f[0] + nf0 * (f[1] + nf1 * f[2]);
+    return a.v.fe_f[a.v.fe_foff[E] + (size_t)(q0 + NQ * q1) * a.v.fe_nf[E] + face] * ct;
   };
   // velocity component `comp` (times the time factor) at table columns
   auto vel = [&](int comp, int jx, int jy, int jz) -> T {
@@ -340,14 +277,11 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     }
     return u * ct;
   };
-  T fln[3][NV];   // FE: the current x-line (cell term)
-
   if (work) {
     // ============================ cell term ============================
     if constexpr (DIM == 2) {
 #pragma unroll 1
       for (int qy = 0; qy < NQ; ++qy) {
-        if constexpr (FE) fe_line(qy, 0, fln);
         T Py[N1];
 #pragma unroll
         for (int aa = 0; aa < N1; ++aa) {
@@ -365,7 +299,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
           T uq[2];
-          if constexpr (FE) fe_point(fln, qx, uq);
+          if constexpr (FE) fe_point(qx, qy, 0, uq);
           else { uq[0] = vel(0, qx, qy, 0); uq[1] = vel(1, qx, qy, 0); }
           const T u0 = uq[0], u1 = uq[1];
           const T w = tb.wq[qx] * tb.wq[qy] * phi;
@@ -401,9 +335,10 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
         for (int aa = 0; aa < N1; ++aa)
 #pragma unroll
           for (int b = 0; b < N1; ++b) { U1[aa][b] = T(0); U3[aa][b] = T(0); }
-#pragma unroll
+        // qy not unrolled: the instruction footprint of the unrolled 3D
+        // body (every point, every face) misses the instruction cache
+#pragma unroll 1
         for (int qy = 0; qy < NQ; ++qy) {
-          if constexpr (FE) fe_line(qy, qz, fln);
           T Py[N1];
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) {
@@ -421,7 +356,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
             T uq[3];
-            if constexpr (FE) fe_point(fln, qx, uq);
+            if constexpr (FE) fe_point(qx, qy, qz, uq);
             else { uq[0] = vel(0, qx, qy, qz); uq[1] = vel(1, qx, qy, qz); uq[2] = vel(2, qx, qy, qz); }
             const T u0 = uq[0], u1 = uq[1], u2 = uq[2];
             const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;

@@ -127,12 +127,14 @@ struct flsp_handle {
   bool has_vel = false;
   flsp_velocity_desc vel;
   int nmax = 1, npt = 1;
-  // velocity of a coupled FE simulator (fe_pv > 0): nodal lattice in FP64
-  // (CFL) and in the state precision (fe_u == fe_u64 in FP64 mode)
+  // velocity of a coupled FE simulator (fe_pv > 0): the nodal lattice (FP64)
+  // and its tables at the cells' and faces' quadrature points (state
+  // precision; layouts of VelArgs::fe_q / fe_f)
   int fe_pv = 0;
   double* fe_u64 = nullptr;
-  void* fe_u = nullptr;
-  double fe_b[kMaxFeVel + 1][kMaxNQ + 2];
+  void* fe_q = nullptr;
+  void* fe_f = nullptr;
+  long long fe_foff[3] = {0, 0, 0}, fe_nf[3] = {0, 0, 0};
   DevClock* clk = nullptr;
   DevClock* clk_host = nullptr;   // pinned mirror
   int64_t* perm = nullptr;
@@ -215,9 +217,13 @@ struct flsp_handle {
     if (fe_pv > 0) {
       v.sep1 = false;
       v.optab = nullptr;
-      v.fe_u = fe_u;
       v.fe_pv = fe_pv;
-      std::memcpy(v.fe_b, fe_b, sizeof(fe_b));
+      v.fe_q = fe_q;
+      v.fe_f = fe_f;
+      for (int e = 0; e < 3; ++e) {
+        v.fe_foff[e] = fe_foff[e];
+        v.fe_nf[e] = fe_nf[e];
+      }
     }
     return v;
   }
@@ -671,9 +677,10 @@ double lagrange(int pv, const double* x, int a, double t) {
 }
 
 void free_fe_velocity(flsp_handle* h) {
-  if (h->fe_u && h->fe_u != h->fe_u64) cudaFree(h->fe_u);
+  if (h->fe_q) cudaFree(h->fe_q);
+  if (h->fe_f) cudaFree(h->fe_f);
   if (h->fe_u64) cudaFree(h->fe_u64);
-  h->fe_u = nullptr;
+  h->fe_q = h->fe_f = nullptr;
   h->fe_u64 = nullptr;
   h->fe_pv = 0;
 }
@@ -1095,24 +1102,31 @@ int flsp_set_velocity_fe(flsp_handle* h, int degree, const double* values, int64
     h->vel.time_kind = FLSP_T_ONE;
     ST(build_vtab(h));
     CU(cudaMalloc(&h->fe_u64, (size_t)n * sizeof(double)));
-    if (h->prec == FLSP_FP64) h->fe_u = h->fe_u64;
-    else CU(cudaMalloc(&h->fe_u, (size_t)n * sizeof(float)));
-    double gl[kMaxFeVel + 1], xq[8], wq[8];
-    gauss_lobatto01(degree, gl);
     const int nq = h->p + 2;
-    gauss_rule(nq, xq, wq);
-    std::memset(h->fe_b, 0, sizeof(h->fe_b));
-    for (int a = 0; a <= degree; ++a) {
-      for (int j = 0; j < nq; ++j) h->fe_b[a][j] = lagrange(degree, gl, a, xq[j]);
-      h->fe_b[a][nq] = lagrange(degree, gl, a, 0.0);
-      h->fe_b[a][nq + 1] = lagrange(degree, gl, a, 1.0);
+    const long long nqd = h->dim > 2 ? (long long)nq * nq * nq : (long long)nq * nq;
+    const long long nqf = h->dim > 2 ? (long long)nq * nq : nq;
+    long long off = 0;
+    for (int e = 0; e < 3; ++e) {
+      long long nf = e < h->dim ? 1 : 0;
+      for (int d = 0; d < h->dim && e < h->dim; ++d) nf *= h->m.n[d] + (d == e);
+      h->fe_foff[e] = off;
+      h->fe_nf[e] = nf;
+      off += nqf * nf;
     }
+    CU(cudaMalloc(&h->fe_q, (size_t)(h->dim * nqd * h->m.ncell) * h->tsize));
+    CU(cudaMalloc(&h->fe_f, (size_t)off * h->tsize));
     h->fe_pv = degree;
   }
+  double gl[kMaxFeVel + 1], xq[8], wq[8], gb[kMaxFeVel + 1][kMaxNQ + 2];
+  gauss_lobatto01(degree, gl);
+  gauss_rule(h->p + 2, xq, wq);
+  std::memset(gb, 0, sizeof(gb));
+  for (int a = 0; a <= degree; ++a)
+    for (int j = 0; j < h->p + 2; ++j) gb[a][j] = lagrange(degree, gl, a, xq[j]);
   // in place: ordered after the work already queued on the problem's stream
   CU(cudaMemcpyAsync(h->fe_u64, values, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   Ctx c = h->ctx();
-  if (h->prec != FLSP_FP64) ST(launch_to_float(c, h->fe_u64, static_cast<float*>(h->fe_u), n));
+  ST(launch_fe_tabulate(c, h->fe_u64, degree, gb, h->fe_q, h->fe_f, h->fe_foff, h->fe_nf));
   CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
   ST(launch_fe_static_cfl(c, h->fe_u64, degree, h->clk));
   CU(cudaStreamSynchronize(h->stream));

@@ -210,13 +210,13 @@ struct VelArgs {
   int npt;
   int comp[kMaxTerms];
   int cstart[4];   // terms of component c: [cstart[c], cstart[c+1]) (terms sorted by component)
-  // velocity of a coupled FE simulator (fe_pv > 0, no terms): the continuous
-  // nodal field of degree fe_pv on the mesh's Gauss-Lobatto lattice,
-  // fe_u[((comp * fe_nz + z) * fe_ny + y) * fe_nx + x], fe_n* = fe_pv * n + 1
-  const T* fe_u;
-  int fe_pv;
-  int fe_nx, fe_ny, fe_nz;
-  T fe_b[kMaxFeVel + 1][kMaxNQ + 2];   // Lagrange basis a at Gauss point j, j = NQ: xi = 0, NQ + 1: xi = 1
+  // velocity of a coupled FE simulator (no terms), tabulated: fe_q at the
+  // cells' quadrature points [comp][point][cell], fe_f at the faces'
+  // [E][point][face] (block E at fe_foff[E], fe_nf[E] faces normal to E)
+  const T* fe_q;
+  const T* fe_f;
+  long long fe_foff[3];
+  long long fe_nf[3];
 };
 
 // first term of each component in a component-sorted term list

@@ -47,7 +47,7 @@ int adv_default_tile(const Ctx& c, const VelDev& v, int* tile) {
     const int(*cq)[3] = DIM == 2 ? c2 : c3;
     int i = 0;
     for (; i < 3; ++i)
-      if (adv_smem_bytes<DIM, P, T>(cq[i], std::max(v.n_terms, 1), v.fe_pv) <= 200 * 1024) break;
+      if (adv_smem_bytes<DIM, P, T>(cq[i], std::max(v.n_terms, 1), v.fe_pv > 0) <= 200 * 1024) break;
     tile[0] = cq[i][0];
     tile[1] = cq[i][1];
     tile[2] = cq[i][2];
@@ -71,7 +71,7 @@ int adv_prepare(const Ctx& c, const VelDev& v, const int* tile) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
-    const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1), v.fe_pv);
+    const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1), v.fe_pv > 0);
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "advection tile too large for shared memory");
     auto kern = v.fe_pv > 0 ? adv_stage_kernel<DIM, P, T, true> : adv_stage_kernel<DIM, P, T, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -110,13 +110,12 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     for (int k = 0; k < v.n_terms; ++k) a.v.comp[k] = v.comp[k];
     term_ranges(a.v.comp, v.n_terms, a.v.cstart);
     if (v.fe_pv > 0) {
-      a.v.fe_u = reinterpret_cast<const T*>(v.fe_u);
-      a.v.fe_pv = v.fe_pv;
-      a.v.fe_nx = v.fe_pv * c.m.n[0] + 1;
-      a.v.fe_ny = v.fe_pv * c.m.n[1] + 1;
-      a.v.fe_nz = DIM > 2 ? v.fe_pv * c.m.n[2] + 1 : 1;
-      for (int i = 0; i <= kMaxFeVel; ++i)
-        for (int j = 0; j < kMaxNQ + 2; ++j) a.v.fe_b[i][j] = T(v.fe_b[i][j]);
+      a.v.fe_q = reinterpret_cast<const T*>(v.fe_q);
+      a.v.fe_f = reinterpret_cast<const T*>(v.fe_f);
+      for (int e = 0; e < 3; ++e) {
+        a.v.fe_foff[e] = v.fe_foff[e];
+        a.v.fe_nf[e] = v.fe_nf[e];
+      }
     }
     a.phi_s = reinterpret_cast<const T*>(in);
     a.phi_n = reinterpret_cast<const T*>(phin);
@@ -125,7 +124,7 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     a.stage = stage;
     a.combine = combine;
     a.ct_explicit = ct_explicit;
-    const size_t smem = adv_smem_bytes<DIM, P, T>(a.m.tile, std::max(v.n_terms, 1), v.fe_pv);
+    const size_t smem = adv_smem_bytes<DIM, P, T>(a.m.tile, std::max(v.n_terms, 1), v.fe_pv > 0);
     if (v.fe_pv > 0)
       adv_stage_kernel<DIM, P, T, true><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
     else

@@ -97,12 +97,30 @@ int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk)
   return launch_status("fe_static_cfl_kernel");
 }
 
-int launch_to_float(const Ctx& c, const double* x, float* y, long long n) {
+int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* fe_q,
+                       void* fe_f, const long long* foff, const long long* nf) {
+  FeBasis fb;
+  std::memcpy(fb.b, gb, sizeof(fb.b));
+  const int nq = c.p + 2;
   const int threads = 256;
-  const long long want = (n + threads - 1) / threads;
-  const int blocks = (int)std::max<long long>(1, std::min<long long>(want, 148LL * 16));
-  to_float_kernel<<<blocks, threads, 0, c.stream>>>(x, y, n);
-  return launch_status("to_float_kernel");
+  auto grid = [&](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 32)); };
+  const long long nqd = c.dim > 2 ? (long long)nq * nq * nq : (long long)nq * nq;
+  const long long nqf = c.dim > 2 ? (long long)nq * nq : nq;
+  auto run = [&](auto tz) -> int {
+    using T = decltype(tz);
+    T* q = static_cast<T*>(fe_q);
+    T* f = static_cast<T*>(fe_f);
+    if (c.dim == 2) fe_tabulate_cells<2, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, q);
+    else fe_tabulate_cells<3, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, q);
+    for (int e = 0; e < c.dim; ++e) {
+      if (c.dim == 2)
+        fe_tabulate_faces<2, T><<<grid(nqf * nf[e]), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, e, nf[e], f + foff[e]);
+      else
+        fe_tabulate_faces<3, T><<<grid(nqf * nf[e]), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, e, nf[e], f + foff[e]);
+    }
+    return launch_status("fe_tabulate");
+  };
+  return c.prec == FLSP_FP64 ? run(double(0)) : run(float(0));
 }
 
 int reduce_blocks(const Ctx& c) { return (int)((c.m.ncell + 127) / 128); }

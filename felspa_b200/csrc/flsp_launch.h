@@ -137,10 +137,11 @@ struct VelDev {
   const void* optab;   // per-axis operator rows of a sep1 velocity (T precision), or null
   int opstride;        // operator rows per (component, axis) in optab
   int* err;            // device error word (DevClock::err)
-  // FE velocity field (fe_pv > 0): T-precision nodal lattice and basis table
-  const void* fe_u;
+  // FE velocity field (fe_pv > 0): T-precision point and face tables
   int fe_pv;
-  double fe_b[kMaxFeVel + 1][kMaxNQ + 2];
+  const void* fe_q;
+  const void* fe_f;
+  long long fe_foff[3], fe_nf[3];
 };
 // stage kernel of this velocity: separable-operator kernel when optab is set
 inline bool use_sep_kernel(const VelDev& v) { return v.sep1 && v.optab != nullptr; }
@@ -180,8 +181,11 @@ int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int
                       int npt, DevClock* clk);
 // static CFL part of an FE velocity lattice (FP64, degree pv), max-ed into clk->vd_static
 int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk);
-// y[i] = (float)x[i]
-int launch_to_float(const Ctx& c, const double* x, float* y, long long n);
+// the FE velocity lattice (FP64, degree pv) at every cell's QGauss(p+2)
+// points and every face's, in the state precision (layouts of VelArgs::
+// fe_q / fe_f); gb[a][q] = Lagrange basis a at Gauss point q
+int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* fe_q,
+                       void* fe_f, const long long* foff, const long long* nf);
 // two-level FP64 reduction; partial holds 2 * reduce_blocks(c) doubles,
 // out_dev receives two doubles (sum pair, or max)
 int launch_reduce(const Ctx& c, int which, const void* phi, const void* ref,

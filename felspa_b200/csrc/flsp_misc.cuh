@@ -254,10 +254,73 @@ __global__ void fe_static_cfl_kernel(const MeshArgs m, const double* __restrict_
   }
 }
 
-// FP64 -> FP32 copy of a device array
-__global__ void to_float_kernel(const double* __restrict__ x, float* __restrict__ y, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    y[i] = (float)x[i];
+struct FeBasis {
+  double b[kMaxFeVel + 1][kMaxNQ + 2];   // Lagrange basis a at Gauss point q
+};
+
+// FE velocity at every cell's quadrature points: one thread per (point,
+// cell), cell fastest; the cell's nodes times the basis products, summed x
+// fastest, in FP64, stored in T
+template <int DIM, typename T>
+__global__ void fe_tabulate_cells(const MeshArgs m, const double* __restrict__ u, int pv, int nq,
+                                  const FeBasis fb, T* __restrict__ out) {
+  const int nx = pv * m.n[0] + 1, ny = pv * m.n[1] + 1, nz = DIM > 2 ? pv * m.n[2] + 1 : 1;
+  const size_t nn = (size_t)nx * ny * nz;
+  const int nqd = DIM > 2 ? nq * nq * nq : nq * nq;
+  const long long total = (long long)nqd * m.ncell;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long cell = i % m.ncell;
+    const int q = (int)(i / m.ncell);
+    const int qx = q % nq, qy = (q / nq) % nq, qz = DIM > 2 ? q / (nq * nq) : 0;
+    const int gx = (int)(cell % m.n[0]), gy = (int)((cell / m.n[0]) % m.n[1]);
+    const int gz = DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int cz = 0; cz <= (DIM > 2 ? pv : 0); ++cz)
+      for (int cy = 0; cy <= pv; ++cy) {
+        double byz = fb.b[cy][qy];
+        if (DIM > 2) byz *= fb.b[cz][qz];
+        for (int cx = 0; cx <= pv; ++cx) {
+          const double b = fb.b[cx][qx] * byz;
+          const size_t node = ((size_t)(pv * gz + cz) * ny + pv * gy + cy) * nx + pv * gx + cx;
+          for (int d = 0; d < DIM; ++d) acc[d] += u[d * nn + node] * b;
+        }
+      }
+    for (int d = 0; d < DIM; ++d) out[((size_t)d * nqd + q) * m.ncell + cell] = T(acc[d]);
+  }
+}
+
+// the normal component at every face's quadrature points, from the face's
+// own nodes (the basis of the others vanishes on it): one value per face
+template <int DIM, typename T>
+__global__ void fe_tabulate_faces(const MeshArgs m, const double* __restrict__ u, int pv, int nq,
+                                  const FeBasis fb, int E, long long nface, T* __restrict__ out) {
+  const int nx = pv * m.n[0] + 1, ny = pv * m.n[1] + 1, nz = DIM > 2 ? pv * m.n[2] + 1 : 1;
+  const size_t nn = (size_t)nx * ny * nz;
+  const int nqf = DIM > 2 ? nq * nq : nq;
+  const int nf0 = m.n[0] + (E == 0), nf1 = m.n[1] + (E == 1);
+  const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  const long long total = (long long)nqf * nface;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long face = i % nface;
+    const int q = (int)(i / nface);
+    const int q0 = q % nq, q1 = DIM > 2 ? q / nq : 0;
+    const int f[3] = {(int)(face % nf0), (int)((face / nf0) % nf1), DIM > 2 ? (int)(face / ((long long)nf0 * nf1)) : 0};
+    double acc = 0.0;
+    for (int c1 = 0; c1 <= (DIM > 2 ? pv : 0); ++c1)
+      for (int c0 = 0; c0 <= pv; ++c0) {
+        double b = fb.b[c0][q0];
+        if (DIM > 2) b *= fb.b[c1][q1];
+        int node[3];
+        node[E] = pv * f[E];
+        node[t0] = pv * f[t0] + c0;
+        if (DIM > 2) node[t1] = pv * f[t1] + c1;
+        else node[2] = 0;
+        acc += u[E * nn + ((size_t)node[2] * ny + node[1]) * nx + node[0]] * b;
+      }
+    out[(size_t)q * nface + face] = T(acc);
+  }
 }
 
 // ---------------------------------------------------------------------

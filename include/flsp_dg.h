@@ -18,6 +18,8 @@
  *                                  get_solution_vector (advection.implement.h:119-131)
  *   flsp_set_velocity              AdvectSimulator::initialize(..., ptr_velocity_field)
  *                                  (advection.implement.h:86-115)
+ *   flsp_set_velocity_fe           the same with a simulator as the velocity field
+ *                                  (VelocityExtractor, advection.implement.h:472-477,891-905)
  *   flsp_advect_rhs                AdvectSimulator::explicit_time_derivative
  *                                  (src/pde/advection.cc:269-296)
  *   flsp_advance                   AdvectSimulator::advance_time(dt, single)
@@ -257,7 +259,9 @@ int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v);
    degree+1 Gauss-Lobatto points on [0,1], I = 0..degree*n[e]; nodes x
    fastest, then y (then z), one block per component: n = dim *
    prod_e (degree*n[e] + 1).  A face's velocity is the same from both of
-   its cells (the nodes on the face are shared).  The field is constant
+   its cells (the nodes on the face are shared): the call tabulates the
+   field once at every cell's and every face's quadrature points (in the
+   state precision), which the stage kernel reads.  The field is constant
    in time.  The CFL estimate is the largest node |u| at a cell vertex
    over the cell diameter (CFLEstimator, pde_tools.implement.h:18-67).
    Setting a field of the same degree again rewrites the device copy in
