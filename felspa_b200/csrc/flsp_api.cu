@@ -144,6 +144,8 @@ struct flsp_handle {
   double* red_out = nullptr;
   flsp_ic_desc* ic_dev = nullptr;
   unsigned int* flag_dev = nullptr;
+  int2* weno_list = nullptr;      // 2D: troubled cells of a limiter pass
+  unsigned int* weno_n = nullptr;
   int n_since_reinit = 0;
   void* qbuf = nullptr;     // LDG alternating gradient (dim blocks)
   void* rdiff = nullptr;    // LDG diffusion RHS
@@ -381,7 +383,7 @@ int enqueue_hj_step(flsp_handle* h, const flsp_reinit_opts* o, int phi0_idx, boo
   int res = dst;
   if (limiter) {
     const int lim = other(dst, phi0_idx);
-    ST(launch_weno(h->ctx(), h->buf[dst], h->buf[lim], nullptr));
+    ST(launch_weno(h->ctx(), h->buf[dst], h->buf[lim], nullptr, h->weno_list, h->weno_n));
     res = lim;
   }
   h->cur = res;
@@ -982,6 +984,9 @@ int flsp_create(const flsp_mesh_desc* mesh, const flsp_dg_opts* opts, flsp_handl
       cudaMalloc(&h->ic_dev, sizeof(flsp_ic_desc)) != cudaSuccess ||
       cudaMalloc(&h->flag_dev, sizeof(unsigned int)) != cudaSuccess)
     return cleanup_fail(fail(FLSP_ERR_OOM, "allocation failed"));
+  if (h->dim == 2 && (cudaMalloc(&h->weno_list, sizeof(int2) * (size_t)ncell) != cudaSuccess ||
+                      cudaMalloc(&h->weno_n, sizeof(unsigned int)) != cudaSuccess))
+    return cleanup_fail(fail(FLSP_ERR_OOM, "allocation failed"));
   cudaMemset(h->clk, 0, sizeof(DevClock));
   cudaMemset(h->buf[0], 0, h->ndofs * h->tsize);
   if (mesh->host_cell_order) {
@@ -1047,6 +1052,8 @@ void flsp_destroy(flsp_handle* h) {
   if (h->red_out) cudaFree(h->red_out);
   if (h->ic_dev) cudaFree(h->ic_dev);
   if (h->flag_dev) cudaFree(h->flag_dev);
+  if (h->weno_list) cudaFree(h->weno_list);
+  if (h->weno_n) cudaFree(h->weno_n);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1473,7 +1480,7 @@ int flsp_weno_limit(flsp_handle* h, int* n_troubled) {
   CU(cudaSetDevice(h->dev));
   CU(cudaMemsetAsync(h->flag_dev, 0, sizeof(unsigned int), h->stream));
   const int dst = (h->cur + 1) % 3;
-  ST(launch_weno(h->ctx(), h->buf[h->cur], h->buf[dst], h->flag_dev));
+  ST(launch_weno(h->ctx(), h->buf[h->cur], h->buf[dst], h->flag_dev, h->weno_list, h->weno_n));
   unsigned int cnt = 0;
   CU(cudaMemcpyAsync(&cnt, h->flag_dev, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -1940,6 +1947,11 @@ struct flsp_batch {
   cudaStream_t side[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
+  // per degree: the troubled cells of a limiter pass (the cells of the
+  // degree's problems) and their counter (weno_n[p])
+  int2* weno_list[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long deg_cells[4] = {0, 0, 0, 0};
+  unsigned int* weno_n = nullptr;
 };
 
 namespace {
@@ -2118,7 +2130,8 @@ int batch_weno_all(flsp_batch* b, int in, int out) {
   return batch_each_degree(b, kBatchKindWeno, [&](int p, cudaStream_t s) {
     return launch_batch_weno(s, b->prec, p, b->probs, b->items_weno + b->deg_off[kBatchKindWeno][p],
                              b->deg_cnt[kBatchKindWeno][p], b->deg_grid[kBatchKindWeno][p],
-                             kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out);
+                             kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out,
+                             b->weno_list[p], b->weno_n + p, b->deg_cells[p]);
   });
 }
 
@@ -2182,6 +2195,9 @@ void flsp_batch_destroy(flsp_batch* b) {
   }
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->stream) cudaStreamDestroy(b->stream);
+  for (int p = 0; p < 4; ++p)
+    if (b->weno_list[p]) cudaFree(b->weno_list[p]);
+  if (b->weno_n) cudaFree(b->weno_n);
   delete b;
 }
 
@@ -2220,6 +2236,14 @@ int flsp_batch_create(int n, const flsp_mesh_desc* meshes, const flsp_dg_opts* o
   if (!ok) {
     flsp_batch_destroy(b);
     return fail(FLSP_ERR_CUDA, "batch stream creation failed");
+  }
+  for (flsp_handle* h : b->h) b->deg_cells[h->p] += h->m.ncell;
+  ok = cudaMalloc(&b->weno_n, 4 * sizeof(unsigned int)) == cudaSuccess;
+  for (int p = 1; p <= 3 && ok; ++p)
+    if (b->deg_cells[p] > 0) ok = cudaMalloc(&b->weno_list[p], sizeof(int2) * (size_t)b->deg_cells[p]) == cudaSuccess;
+  if (!ok) {
+    flsp_batch_destroy(b);
+    return fail(FLSP_ERR_OOM, "batch allocation failed");
   }
   *out = b;
   return FLSP_OK;

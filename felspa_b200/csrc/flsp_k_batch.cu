@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(128)
 }
 
 template <typename T, int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     batch_weno_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ items, int n_items, int iin,
-                      int iout) {
+                      int iout, int2* list, unsigned int* list_n) {
   __shared__ WenoArgs<T> a;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const int2 w = items[it];
@@ -107,10 +107,31 @@ __global__ void __launch_bounds__(256)
       a.in = reinterpret_cast<const T*>(pr.buf[iin]);
       a.out = reinterpret_cast<T*>(pr.buf[iout]);
       a.count = nullptr;
+      a.list = list;
+      a.list_n = list_n;
+      a.problem = w.x;
     }
     __syncthreads();
     weno_tile<P, T>(a, w.y);
     __syncthreads();
+  }
+}
+
+// the troubled cells of every problem of the launch's degree: a warp each
+template <typename T, int P>
+__global__ void __launch_bounds__(256)
+    batch_weno_fix_kernel(const BatchProb* __restrict__ probs, const int2* __restrict__ list,
+                          const unsigned int* __restrict__ list_n, int iin, int iout) {
+  constexpr int NM = (P + 1) * (P + 1);
+  __shared__ T sh[8][5 * NM];
+  const int wl = threadIdx.x >> 5;
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  const unsigned int n = *list_n;
+  for (unsigned int i = warp; i < n; i += nwarps) {
+    const int2 e = list[i];
+    const BatchProb& pr = probs[e.x];
+    weno_fix<P, T>(pr.m_weno, reinterpret_cast<const T*>(pr.buf[iin]), reinterpret_cast<T*>(pr.buf[iout]), e.y,
+                   sh[wl]);
   }
 }
 
@@ -236,13 +257,20 @@ int launch_batch_hj(cudaStream_t s, int prec, int p, const BatchProb* probs, con
 }
 
 int launch_batch_weno(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
-                      int grid, int threads, size_t smem, int iin, int iout) {
+                      int grid, int threads, size_t smem, int iin, int iout, int2* list, unsigned int* list_n,
+                      long long n_cells) {
+  cudaError_t e = cudaMemsetAsync(list_n, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("batch weno list: ") + cudaGetErrorString(e));
+  const int fix_grid = (int)std::max<long long>(1, std::min<long long>((n_cells + 7) / 8, 148LL * 4));
   return with_degree(p, [&](auto PC) -> int {
     constexpr int P = decltype(PC)::value;
-    if (prec == FLSP_FP64)
-      batch_weno_kernel<double, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
-    else
-      batch_weno_kernel<float, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout);
+    if (prec == FLSP_FP64) {
+      batch_weno_kernel<double, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout, list, list_n);
+      batch_weno_fix_kernel<double, P><<<fix_grid, 256, 0, s>>>(probs, list, list_n, iin, iout);
+    } else {
+      batch_weno_kernel<float, P><<<grid, threads, smem, s>>>(probs, items, n_items, iin, iout, list, list_n);
+      batch_weno_fix_kernel<float, P><<<fix_grid, 256, 0, s>>>(probs, list, list_n, iin, iout);
+    }
     return launch_status("batch_weno_kernel");
   });
 }

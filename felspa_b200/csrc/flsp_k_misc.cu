@@ -38,7 +38,7 @@ int weno_prepare(const Ctx& c) {
   });
 }
 
-int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count) {
+int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count, int2* list, unsigned int* list_n) {
   if (c.dim != 2) return set_error(FLSP_ERR_UNSUPPORTED, "WENO limiter is 2D only (reinit.cc:475-478)");
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int P = decltype(PP)::value;
@@ -54,8 +54,17 @@ int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count) {
       a.in = reinterpret_cast<const T*>(in);
       a.out = reinterpret_cast<T*>(out);
       a.count = count;
+      a.list = list;
+      a.list_n = list_n;
+      a.problem = 0;
+      cudaError_t e = cudaMemsetAsync(list_n, 0, sizeof(unsigned int), c.stream);
+      if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("weno list: ") + cudaGetErrorString(e));
       const size_t smem = weno_smem_bytes<P, T>(a.m.tile);
       weno_kernel<P, T><<<(unsigned)nblocks(a.m), kWenoTile[0] * kWenoTile[1], smem, c.stream>>>(a);
+      // the troubled cells: a warp each, at most one warp per cell
+      const long long want = (c.m.ncell + 7) / 8;
+      const int grid = (int)std::max<long long>(1, std::min<long long>(want, 148LL * 4));
+      weno_fix_kernel<P, T><<<grid, 256, 0, c.stream>>>(a);
       return launch_status("weno_kernel");
     }
   });

@@ -75,7 +75,8 @@ int launch_batch_adv(cudaStream_t s, int prec, int p, const BatchProb* probs, co
 int launch_batch_hj(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
                     int grid, int threads, size_t smem, int isrc, int iphi0, int idst, int mode, int rk);
 int launch_batch_weno(cudaStream_t s, int prec, int p, const BatchProb* probs, const int2* items, int n_items,
-                      int grid, int threads, size_t smem, int iin, int iout);
+                      int grid, int threads, size_t smem, int iin, int iout, int2* list, unsigned int* list_n,
+                      long long n_cells);
 
 // restrict a launch's MeshArgs to the narrow-band tile list of `kind`
 inline void apply_band(const Ctx& c, int kind, MeshArgs& m) {
@@ -175,7 +176,10 @@ int launch_ldg(const Ctx& c, const void* in, void* out, long long block, double 
 
 // ---------------- misc (flsp_k_misc.cu) ----------------
 int weno_prepare(const Ctx& c);
-int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count);
+// detection over the tiles (untroubled cells copied), then the WENO
+// reconstruction of the troubled cells listed in `list` (ncell entries,
+// counter list_n)
+int launch_weno(const Ctx& c, const void* in, void* out, unsigned int* count, int2* list, unsigned int* list_n);
 int launch_project_ic(const Ctx& c, const flsp_ic_desc* ic_dev, void* out);
 int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int* comp, int nmax,
                       int npt, DevClock* clk);
