@@ -44,8 +44,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--profile", action="store_true",
-                    help="short run for ncu: set-up, 2 reinit periods, no timing loops")
+    ap.add_argument("--profile", nargs="?", const="headline", default=None,
+                    choices=["headline", "fe", "batched"],
+                    help="short run for ncu, no timing loops: headline = the 64^3 workload's set-up and 2 reinit "
+                         "periods; fe = the same with the deformation field at t = 0 as a degree-2 FE velocity "
+                         "lattice; batched = the 256-problem batch, autotuned, 2 reinit periods")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP64 run of the same periods (accuracy of the FP32 mode)")
@@ -247,12 +250,25 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
+    if args.profile == "batched":
+        from felspa_b200.batch import make_batch, uneven_batch_instances
+        b = make_batch(uneven_batch_instances(256), precision=abi.FP32)
+        b.autotune()
+        ctl = abi.default_ls_opts(reinit_frequency=REINIT_EVERY,
+                                  reinit=abi.default_reinit_opts(mode=abi.REINIT_FIXED, n_pseudo_steps=N_PSEUDO))
+        b.run_steps(2 * REINIT_EVERY, ctl)
+        print(json.dumps({"profile_run": "batched", "n_dofs": b.n_dofs}), flush=True)
+        b.close()
+        return 0
     ls = make_problem(abi.FP32, local)
     pb = ls.problem
     n_dofs = pb.n_dofs
     if args.profile:
+        if args.profile == "fe":
+            from felspa_b200 import fields as F
+            pb.set_velocity_fe(2, F.fe_lattice(lambda x: F.deformation_3d()(x, 0.0), (N_CELLS,) * 3, 2))
         ls.run_steps(2 * REINIT_EVERY)
-        print(json.dumps({"profile_run": True, "n_dofs": n_dofs}), flush=True)
+        print(json.dumps({"profile_run": args.profile, "n_dofs": n_dofs}), flush=True)
         return 0
 
     # stage-kernel tile from the autotuner (timed on this problem; state kept)

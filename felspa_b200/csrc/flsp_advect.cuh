@@ -59,15 +59,15 @@ __device__ __forceinline__ T term_val(const T* __restrict__ vx, const T* __restr
 // shared-memory footprint of the stage kernel: tile box with face halo,
 // velocity-table rows of the tile, upper-face fluxes shared with the
 // upper neighbours
-// fe: the velocity is read from the FE tables (VelArgs::fe_q / fe_f), no
-// velocity rows in shared memory
+// tab: the velocity is read from the velocity tables (VelArgs::tab_q /
+// tab_f), no velocity rows in shared memory
 template <int DIM, int P, typename T>
-__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms, bool fe = false) {
+__host__ __device__ inline size_t adv_smem_bytes(const int* tile, int n_terms, bool tab = false) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   const int bx = tile[0] + 2, by = DIM > 1 ? tile[1] + 2 : 1, bz = DIM > 2 ? tile[2] + 2 : 1;
   const int nt = tile[0] * tile[1] * (DIM > 2 ? tile[2] : 1);
   size_t box = (size_t)bx * by * bz * NM * sizeof(T);
-  size_t vt = fe ? 0 : (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
+  size_t vt = tab ? 0 : (size_t)n_terms * (tile[0] + tile[1] + (DIM > 2 ? tile[2] : 0)) * NPT * sizeof(T);
   size_t fl = (size_t)DIM * NF * nt * sizeof(T);
   return box + vt + fl;
 }
@@ -183,12 +183,14 @@ __device__ __forceinline__ void scatter_face(T* R, const T* Ls, const T* Fm, T c
 }
 
 // General velocity: a runtime sum of separable terms per component.  (A
-// velocity whose components are single terms takes adv_sep_kernel.)  FE:
-// the velocity of a coupled FE simulator, tabulated once per field update
-// (fe_tabulate_*): at every cell's quadrature points and, single-valued, at
-// every face's (advection.implement.h:891-905).
+// velocity whose components are single terms takes adv_sep_kernel.)  TAB:
+// the velocity's spatial part read from tables made once per field update
+// at every cell's quadrature points and, single-valued, at every face's
+// (vel_tabulate_* for a sum of terms, fe_tabulate_* for the velocity of a
+// coupled FE simulator, advection.implement.h:891-905), times the time
+// factor.
 // one tile of a stage (launch slot `slot`); a plain launch serves slot blockIdx.x
-template <int DIM, int P, typename T, bool FE = false>
+template <int DIM, int P, typename T, bool TAB = false>
 __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   constexpr int N1 = P + 1, NQ = P + 2, NM = ipow(N1, DIM), NPT = NQ + 2, NF = ipow(N1, DIM - 1);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -200,11 +202,11 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   const int nterm = a.v.n_terms;
   const int span = tx + ty + (DIM > 2 ? tz : 0);
   T* vt = box + (size_t)nboxc * NM;
-  T* fl = vt + (FE ? 0 : (size_t)max(nterm, 1) * span * NPT);   // [DIM][NF][nt]
+  T* fl = vt + (TAB ? 0 : (size_t)max(nterm, 1) * span * NPT);   // [DIM][NF][nt]
   const Tab1D<T>& tb = tab<T>(P);
   const TileCoord tc = tile_coord(m, DIM, slot);
 
-  if constexpr (!FE) {
+  if constexpr (!TAB) {
     // ---- stage velocity-table rows of this tile: vt[(k*span + li)*NPT + j]
     const int total = nterm * span * NPT;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
@@ -249,23 +251,23 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
     const int li = axis == 0 ? tc.lx : (axis == 1 ? tx + tc.ly : tx + ty + tc.lz);
     return vt + (size_t)(k * span + li) * NPT;
   };
-  // FE: the tables at this cell's quadrature points ([comp][point][cell],
+  // TAB: the tables at this cell's quadrature points ([comp][point][cell],
   // cell lexicographic) and at its faces ([E][point][face], face index
   // lexicographic over n + e_E faces)
-  const long long fe_cell = tc.gx + (long long)m.n[0] * (tc.gy + (long long)m.n[1] * tc.gz);
-  auto fe_point = [&](int qx, int qy, int qz, T* u) {
+  const long long tab_cell = tc.gx + (long long)m.n[0] * (tc.gy + (long long)m.n[1] * tc.gz);
+  auto tab_point = [&](int qx, int qy, int qz, T* u) {
     constexpr int NQD = ipow(NQ, DIM);
     const int q = qx + NQ * (qy + NQ * qz);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) u[d] = a.v.fe_q[((size_t)d * NQD + q) * m.ncell + fe_cell] * ct;
+    for (int d = 0; d < DIM; ++d) u[d] = a.v.tab_q[((size_t)d * NQD + q) * m.ncell + tab_cell] * ct;
   };
-  auto fe_face = [&](auto EC, int S, int q0, int q1) -> T {
+  auto tab_face = [&](auto EC, int S, int q0, int q1) -> T {
     constexpr int E = decltype(EC)::value;
     int f[3] = {tc.gx, tc.gy, tc.gz};
     f[E] += S;
     const long long nf0 = m.n[0] + (E == 0), nf1 = m.n[1] + (E == 1);
     const long long face = f[0] + nf0 * (f[1] + nf1 * f[2]);
-    return a.v.fe_f[a.v.fe_foff[E] + (size_t)(q0 + NQ * q1) * a.v.fe_nf[E] + face] * ct;
+    return a.v.tab_f[a.v.tab_foff[E] + (size_t)(q0 + NQ * q1) * a.v.tab_nf[E] + face] * ct;
   };
   // velocity component `comp` (times the time factor) at table columns
   auto vel = [&](int comp, int jx, int jy, int jz) -> T {
@@ -299,7 +301,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
 #pragma unroll
           for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
           T uq[2];
-          if constexpr (FE) fe_point(qx, qy, 0, uq);
+          if constexpr (TAB) tab_point(qx, qy, 0, uq);
           else { uq[0] = vel(0, qx, qy, 0); uq[1] = vel(1, qx, qy, 0); }
           const T u0 = uq[0], u1 = uq[1];
           const T w = tb.wq[qx] * tb.wq[qy] * phi;
@@ -356,7 +358,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
 #pragma unroll
             for (int aa = 0; aa < N1; ++aa) phi += Py[aa] * tb.Lq[aa][qx];
             T uq[3];
-            if constexpr (FE) fe_point(qx, qy, qz, uq);
+            if constexpr (TAB) tab_point(qx, qy, qz, uq);
             else { uq[0] = vel(0, qx, qy, qz); uq[1] = vel(1, qx, qy, qz); uq[2] = vel(2, qx, qy, qz); }
             const T u0 = uq[0], u1 = uq[1], u2 = uq[2];
             const T w = tb.wq[qx] * tb.wq[qy] * tb.wq[qz] * phi;
@@ -401,7 +403,7 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
       if (DIM > 2) j[t1] = q1;
       T w = tb.wq[q0];
       if constexpr (DIM > 2) w = w * tb.wq[q1];
-      if constexpr (FE) return fe_face(std::integral_constant<int, E>(), S, q0, q1) * w;
+      if constexpr (TAB) return tab_face(std::integral_constant<int, E>(), S, q0, q1) * w;
       else return vel(E, j[0], j[1], j[2]) * w;
     };
   };
@@ -480,9 +482,9 @@ __device__ __forceinline__ void adv_stage_tile(const AdvArgs<T>& a, int slot) {
   store_tile<DIM, NM>(m, stage_buf, a.out, tc.ox, tc.oy, tc.oz);
 }
 
-template <int DIM, int P, typename T, bool FE>
+template <int DIM, int P, typename T, bool TAB>
 __global__ void __launch_bounds__(256, 2) adv_stage_kernel(const AdvArgs<T> a) {
-  adv_stage_tile<DIM, P, T, FE>(a, (int)blockIdx.x);
+  adv_stage_tile<DIM, P, T, TAB>(a, (int)blockIdx.x);
 }
 
 }  // namespace flsp

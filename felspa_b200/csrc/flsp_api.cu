@@ -128,13 +128,16 @@ struct flsp_handle {
   flsp_velocity_desc vel;
   int nmax = 1, npt = 1;
   // velocity of a coupled FE simulator (fe_pv > 0): the nodal lattice (FP64)
-  // and its tables at the cells' and faces' quadrature points (state
-  // precision; layouts of VelArgs::fe_q / fe_f)
   int fe_pv = 0;
   double* fe_u64 = nullptr;
-  void* fe_q = nullptr;
-  void* fe_f = nullptr;
-  long long fe_foff[3] = {0, 0, 0}, fe_nf[3] = {0, 0, 0};
+  // velocity tables at the cells' and faces' quadrature points (state
+  // precision; layouts of VelArgs::tab_q / tab_f): the FE field, or a
+  // velocity of several terms per component (the point-wise stage kernel's
+  // input); tab_ok when they hold the current velocity
+  void* tab_q = nullptr;
+  void* tab_f = nullptr;
+  long long tab_foff[3] = {0, 0, 0}, tab_nf[3] = {0, 0, 0};
+  bool tab_ok = false;
   DevClock* clk = nullptr;
   DevClock* clk_host = nullptr;   // pinned mirror
   int64_t* perm = nullptr;
@@ -220,11 +223,15 @@ struct flsp_handle {
       v.sep1 = false;
       v.optab = nullptr;
       v.fe_pv = fe_pv;
-      v.fe_q = fe_q;
-      v.fe_f = fe_f;
+    }
+    // tables of a velocity the separable kernel does not take
+    if (tab_ok && !use_sep_kernel(v)) {
+      v.tab = true;
+      v.tab_q = tab_q;
+      v.tab_f = tab_f;
       for (int e = 0; e < 3; ++e) {
-        v.fe_foff[e] = fe_foff[e];
-        v.fe_nf[e] = fe_nf[e];
+        v.tab_foff[e] = tab_foff[e];
+        v.tab_nf[e] = tab_nf[e];
       }
     }
     return v;
@@ -679,15 +686,46 @@ double lagrange(int pv, const double* x, int a, double t) {
 }
 
 void free_fe_velocity(flsp_handle* h) {
-  if (h->fe_q) cudaFree(h->fe_q);
-  if (h->fe_f) cudaFree(h->fe_f);
   if (h->fe_u64) cudaFree(h->fe_u64);
-  h->fe_q = h->fe_f = nullptr;
   h->fe_u64 = nullptr;
   h->fe_pv = 0;
+  h->tab_ok = false;
 }
 
-int build_vtab(flsp_handle* h) {
+// the velocity tables (sizes fixed by the mesh and the degree)
+int ensure_vel_tables(flsp_handle* h) {
+  if (h->tab_q) return FLSP_OK;
+  const int nq = h->p + 2;
+  const long long nqd = h->dim > 2 ? (long long)nq * nq * nq : (long long)nq * nq;
+  const long long nqf = h->dim > 2 ? (long long)nq * nq : nq;
+  long long off = 0;
+  for (int e = 0; e < 3; ++e) {
+    long long nf = e < h->dim ? 1 : 0;
+    for (int d = 0; d < h->dim && e < h->dim; ++d) nf *= h->m.n[d] + (d == e);
+    h->tab_foff[e] = off;
+    h->tab_nf[e] = nf;
+    off += nqf * nf;
+  }
+  if (cudaMalloc(&h->tab_q, (size_t)(h->dim * nqd * h->m.ncell) * h->tsize) != cudaSuccess ||
+      cudaMalloc(&h->tab_f, (size_t)off * h->tsize) != cudaSuccess) {
+    if (h->tab_q) cudaFree(h->tab_q);
+    h->tab_q = nullptr;
+    return fail(FLSP_ERR_OOM, "velocity table allocation failed");
+  }
+  return FLSP_OK;
+}
+
+void free_vel_tables(flsp_handle* h) {
+  if (h->tab_q) cudaFree(h->tab_q);
+  if (h->tab_f) cudaFree(h->tab_f);
+  h->tab_q = h->tab_f = nullptr;
+  h->tab_ok = false;
+}
+
+// tables: tabulate a velocity of several terms per component (the
+// point-wise stage kernel reads the tables instead of summing the terms at
+// every point of every stage; batch members always)
+int build_vtab(flsp_handle* h, bool tables = true) {
   const int dim = h->dim;
   layout_velocity(h);
   const int nq = h->p + 2;
@@ -732,9 +770,16 @@ int build_vtab(flsp_handle* h) {
     CU(cudaMemcpy(h->vtab, tf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   }
   ST(build_optab(h, tabd));
-  // static CFL part: max over vertices of |u_spatial| / diam
   int comp[kMaxTerms];
   for (int k = 0; k < h->vel_dev.n_terms; ++k) comp[k] = h->vel_dev.terms[k].comp;
+  h->tab_ok = false;
+  if (tables && (h->batch_member || !use_sep_kernel(h->veldev()))) {
+    ST(ensure_vel_tables(h));
+    ST(launch_vel_tabulate(h->ctx(), h->vtab64, h->vel_dev.n_terms, comp, h->nmax, h->npt, h->tab_q, h->tab_f,
+                           h->tab_foff, h->tab_nf));
+    h->tab_ok = true;
+  }
+  // static CFL part: max over vertices of |u_spatial| / diam
   CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
   ST(launch_static_cfl(h->ctx(), h->vtab64, h->vel_dev.n_terms, comp, h->nmax, h->npt, h->clk));
   CU(cudaStreamSynchronize(h->stream));
@@ -1035,6 +1080,7 @@ void flsp_destroy(flsp_handle* h) {
   if (h->vtab) cudaFree(h->vtab);
   if (h->vtab64) cudaFree(h->vtab64);
   free_fe_velocity(h);
+  free_vel_tables(h);
   if (h->optab) cudaFree(h->optab);
   void* lrn[] = {h->lrn_flags, h->lrn_work, h->lrn_cells, h->lrn_count, h->lrn_tot, h->lrn_save, h->lrn_feat,
                  h->nb_flags, h->nb_lists, h->nb_counts};
@@ -1107,21 +1153,9 @@ int flsp_set_velocity_fe(flsp_handle* h, int degree, const double* values, int64
     free_fe_velocity(h);
     std::memset(&h->vel, 0, sizeof(h->vel));
     h->vel.time_kind = FLSP_T_ONE;
-    ST(build_vtab(h));
+    ST(build_vtab(h, false));
     CU(cudaMalloc(&h->fe_u64, (size_t)n * sizeof(double)));
-    const int nq = h->p + 2;
-    const long long nqd = h->dim > 2 ? (long long)nq * nq * nq : (long long)nq * nq;
-    const long long nqf = h->dim > 2 ? (long long)nq * nq : nq;
-    long long off = 0;
-    for (int e = 0; e < 3; ++e) {
-      long long nf = e < h->dim ? 1 : 0;
-      for (int d = 0; d < h->dim && e < h->dim; ++d) nf *= h->m.n[d] + (d == e);
-      h->fe_foff[e] = off;
-      h->fe_nf[e] = nf;
-      off += nqf * nf;
-    }
-    CU(cudaMalloc(&h->fe_q, (size_t)(h->dim * nqd * h->m.ncell) * h->tsize));
-    CU(cudaMalloc(&h->fe_f, (size_t)off * h->tsize));
+    ST(ensure_vel_tables(h));
     h->fe_pv = degree;
   }
   double gl[kMaxFeVel + 1], xq[8], wq[8], gb[kMaxFeVel + 1][kMaxNQ + 2];
@@ -1133,10 +1167,11 @@ int flsp_set_velocity_fe(flsp_handle* h, int degree, const double* values, int64
   // in place: ordered after the work already queued on the problem's stream
   CU(cudaMemcpyAsync(h->fe_u64, values, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   Ctx c = h->ctx();
-  ST(launch_fe_tabulate(c, h->fe_u64, degree, gb, h->fe_q, h->fe_f, h->fe_foff, h->fe_nf));
+  ST(launch_fe_tabulate(c, h->fe_u64, degree, gb, h->tab_q, h->tab_f, h->tab_foff, h->tab_nf));
   CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
   ST(launch_fe_static_cfl(c, h->fe_u64, degree, h->clk));
   CU(cudaStreamSynchronize(h->stream));
+  h->tab_ok = true;
   h->has_vel = true;
   if (same) return FLSP_OK;
   clear_graphs(h);
@@ -1991,6 +2026,13 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
     for (int k = 0; k < 3; ++k) q.buf[k] = h->buf[k];
     q.clk = h->clk;
     VelDev v = h->veldev();
+    if (!h->tab_ok) return fail(FLSP_ERR_BAD_ARG, "batched problem without velocity tables");
+    q.tab_q = h->tab_q;
+    q.tab_f = h->tab_f;
+    for (int e = 0; e < 3; ++e) {
+      q.tab_foff[e] = h->tab_foff[e];
+      q.tab_nf[e] = h->tab_nf[e];
+    }
     q.vtab = v.vtab;
     q.n_terms = v.n_terms;
     q.nmax = v.nmax;

@@ -210,13 +210,14 @@ struct VelArgs {
   int npt;
   int comp[kMaxTerms];
   int cstart[4];   // terms of component c: [cstart[c], cstart[c+1]) (terms sorted by component)
-  // velocity of a coupled FE simulator (no terms), tabulated: fe_q at the
-  // cells' quadrature points [comp][point][cell], fe_f at the faces'
-  // [E][point][face] (block E at fe_foff[E], fe_nf[E] faces normal to E)
-  const T* fe_q;
-  const T* fe_f;
-  long long fe_foff[3];
-  long long fe_nf[3];
+  // velocity tables (the point-wise kernel's TAB form): the spatial part
+  // at the cells' quadrature points, tab_q[comp][point][cell], and its
+  // normal component at the faces' points, tab_f[E][point][face] (block E
+  // at tab_foff[E], tab_nf[E] faces normal to E)
+  const T* tab_q;
+  const T* tab_f;
+  long long tab_foff[3];
+  long long tab_nf[3];
 };
 
 // first term of each component in a component-sorted term list

@@ -47,7 +47,7 @@ int adv_default_tile(const Ctx& c, const VelDev& v, int* tile) {
     const int(*cq)[3] = DIM == 2 ? c2 : c3;
     int i = 0;
     for (; i < 3; ++i)
-      if (adv_smem_bytes<DIM, P, T>(cq[i], std::max(v.n_terms, 1), v.fe_pv > 0) <= 200 * 1024) break;
+      if (adv_smem_bytes<DIM, P, T>(cq[i], std::max(v.n_terms, 1), v.tab) <= 200 * 1024) break;
     tile[0] = cq[i][0];
     tile[1] = cq[i][1];
     tile[2] = cq[i][2];
@@ -71,9 +71,9 @@ int adv_prepare(const Ctx& c, const VelDev& v, const int* tile) {
   return dispatch(c, [&](auto D, auto PP, auto tz) -> int {
     constexpr int DIM = decltype(D)::value, P = decltype(PP)::value;
     using T = decltype(tz);
-    const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1), v.fe_pv > 0);
+    const size_t smem = adv_smem_bytes<DIM, P, T>(tile, std::max(v.n_terms, 1), v.tab);
     if (smem > 227 * 1024) return set_error(FLSP_ERR_BAD_ARG, "advection tile too large for shared memory");
-    auto kern = v.fe_pv > 0 ? adv_stage_kernel<DIM, P, T, true> : adv_stage_kernel<DIM, P, T, false>;
+    auto kern = v.tab ? adv_stage_kernel<DIM, P, T, true> : adv_stage_kernel<DIM, P, T, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return set_error(FLSP_ERR_CUDA, std::string("adv attr: ") + cudaGetErrorString(e));
@@ -109,12 +109,12 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     a.v.npt = v.npt;
     for (int k = 0; k < v.n_terms; ++k) a.v.comp[k] = v.comp[k];
     term_ranges(a.v.comp, v.n_terms, a.v.cstart);
-    if (v.fe_pv > 0) {
-      a.v.fe_q = reinterpret_cast<const T*>(v.fe_q);
-      a.v.fe_f = reinterpret_cast<const T*>(v.fe_f);
+    if (v.tab) {
+      a.v.tab_q = reinterpret_cast<const T*>(v.tab_q);
+      a.v.tab_f = reinterpret_cast<const T*>(v.tab_f);
       for (int e = 0; e < 3; ++e) {
-        a.v.fe_foff[e] = v.fe_foff[e];
-        a.v.fe_nf[e] = v.fe_nf[e];
+        a.v.tab_foff[e] = v.tab_foff[e];
+        a.v.tab_nf[e] = v.tab_nf[e];
       }
     }
     a.phi_s = reinterpret_cast<const T*>(in);
@@ -124,8 +124,8 @@ int launch_adv_stage(const Ctx& c, const VelDev& v, const void* in, const void* 
     a.stage = stage;
     a.combine = combine;
     a.ct_explicit = ct_explicit;
-    const size_t smem = adv_smem_bytes<DIM, P, T>(a.m.tile, std::max(v.n_terms, 1), v.fe_pv > 0);
-    if (v.fe_pv > 0)
+    const size_t smem = adv_smem_bytes<DIM, P, T>(a.m.tile, std::max(v.n_terms, 1), v.tab);
+    if (v.tab)
       adv_stage_kernel<DIM, P, T, true><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);
     else
       adv_stage_kernel<DIM, P, T, false><<<(unsigned)nblocks(a.m), t[0] * t[1] * t[2], smem, c.stream>>>(a);

@@ -42,6 +42,13 @@ __device__ __forceinline__ void make_adv_args(const BatchProb& pr, int ix, int i
 #pragma unroll 1
   for (int k = 0; k < kMaxTerms; ++k) a.v.comp[k] = pr.comp[k];
   term_ranges(pr.comp, pr.n_terms, a.v.cstart);
+  a.v.tab_q = reinterpret_cast<const T*>(pr.tab_q);
+  a.v.tab_f = reinterpret_cast<const T*>(pr.tab_f);
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    a.v.tab_foff[e] = pr.tab_foff[e];
+    a.v.tab_nf[e] = pr.tab_nf[e];
+  }
   a.phi_s = reinterpret_cast<const T*>(pr.buf[ix]);
   a.phi_n = reinterpret_cast<const T*>(pr.buf[in_n]);
   a.out = reinterpret_cast<T*>(pr.buf[iout]);
@@ -63,7 +70,7 @@ __global__ void __launch_bounds__(256, 2)
     const int2 w = items[it];
     if (threadIdx.x == 0) make_adv_args<T>(probs[w.x], ix, in_n, iout, stage, combine, a);
     __syncthreads();
-    adv_stage_tile<2, P, T>(a, w.y);
+    adv_stage_tile<2, P, T, true>(a, w.y);   // velocity from the problem's tables
     __syncthreads();   // shared memory is reused by the next item
   }
 }
@@ -167,9 +174,9 @@ int batch_smem(int kind, int p, int prec, const int* tile, int n_terms, size_t* 
     using T = decltype(tz);
     if (kind == kBatchKindAdv) {
       switch (p) {
-        case 1: return adv_smem_bytes<2, 1, T>(tile, std::max(n_terms, 1));
-        case 2: return adv_smem_bytes<2, 2, T>(tile, std::max(n_terms, 1));
-        default: return adv_smem_bytes<2, 3, T>(tile, std::max(n_terms, 1));
+        case 1: return adv_smem_bytes<2, 1, T>(tile, std::max(n_terms, 1), true);
+        case 2: return adv_smem_bytes<2, 2, T>(tile, std::max(n_terms, 1), true);
+        default: return adv_smem_bytes<2, 3, T>(tile, std::max(n_terms, 1), true);
       }
     } else if (kind == kBatchKindHJ) {
       switch (p) {

@@ -106,8 +106,38 @@ int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk)
   return launch_status("fe_static_cfl_kernel");
 }
 
-int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* fe_q,
-                       void* fe_f, const long long* foff, const long long* nf) {
+int launch_vel_tabulate(const Ctx& c, const double* vtab64, int n_terms, const int* comp, int nmax, int npt,
+                        void* tab_q, void* tab_f, const long long* foff, const long long* nf) {
+  VelTerms vt;
+  term_ranges(comp, n_terms, vt.cstart);
+  const int nq = c.p + 2;
+  const int threads = 256;
+  auto grid = [&](long long n) { return (int)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 148LL * 32)); };
+  const long long nqd = c.dim > 2 ? (long long)nq * nq * nq : (long long)nq * nq;
+  const long long nqf = c.dim > 2 ? (long long)nq * nq : nq;
+  auto run = [&](auto tz) -> int {
+    using T = decltype(tz);
+    T* q = static_cast<T*>(tab_q);
+    T* f = static_cast<T*>(tab_f);
+    if (c.dim == 2)
+      vel_tabulate_cells<2, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, vtab64, nmax, npt, vt, nq, q);
+    else
+      vel_tabulate_cells<3, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, vtab64, nmax, npt, vt, nq, q);
+    for (int e = 0; e < c.dim; ++e) {
+      if (c.dim == 2)
+        vel_tabulate_faces<2, T><<<grid(nqf * nf[e]), threads, 0, c.stream>>>(c.m, vtab64, nmax, npt, vt, nq, e, nf[e],
+                                                                              f + foff[e]);
+      else
+        vel_tabulate_faces<3, T><<<grid(nqf * nf[e]), threads, 0, c.stream>>>(c.m, vtab64, nmax, npt, vt, nq, e, nf[e],
+                                                                              f + foff[e]);
+    }
+    return launch_status("vel_tabulate");
+  };
+  return c.prec == FLSP_FP64 ? run(double(0)) : run(float(0));
+}
+
+int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* tab_q,
+                       void* tab_f, const long long* foff, const long long* nf) {
   FeBasis fb;
   std::memcpy(fb.b, gb, sizeof(fb.b));
   const int nq = c.p + 2;
@@ -117,8 +147,8 @@ int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*g
   const long long nqf = c.dim > 2 ? (long long)nq * nq : nq;
   auto run = [&](auto tz) -> int {
     using T = decltype(tz);
-    T* q = static_cast<T*>(fe_q);
-    T* f = static_cast<T*>(fe_f);
+    T* q = static_cast<T*>(tab_q);
+    T* f = static_cast<T*>(tab_f);
     if (c.dim == 2) fe_tabulate_cells<2, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, q);
     else fe_tabulate_cells<3, T><<<grid(nqd * c.m.ncell), threads, 0, c.stream>>>(c.m, u64, pv, nq, fb, q);
     for (int e = 0; e < c.dim; ++e) {

@@ -55,6 +55,9 @@ struct BatchProb {
   const void* vtab;               // velocity table (state precision)
   int n_terms, nmax, npt;
   int comp[kMaxTerms];
+  const void* tab_q;              // velocity tables of the problem (VelArgs::tab_q / tab_f)
+  const void* tab_f;
+  long long tab_foff[3], tab_nf[3];
   int p;                          // degree 1..3
   AdvClockArgs ca;                // advection clock parameters
   double adv_scale;               // advection CFL scaling of the degree
@@ -138,11 +141,14 @@ struct VelDev {
   const void* optab;   // per-axis operator rows of a sep1 velocity (T precision), or null
   int opstride;        // operator rows per (component, axis) in optab
   int* err;            // device error word (DevClock::err)
-  // FE velocity field (fe_pv > 0): T-precision point and face tables
+  // velocity tables (tab): T-precision values at the cells' and faces'
+  // quadrature points (VelArgs::tab_q / tab_f), made from the terms or from
+  // the FE field of a coupled simulator (fe_pv > 0: its lattice degree)
+  bool tab;
   int fe_pv;
-  const void* fe_q;
-  const void* fe_f;
-  long long fe_foff[3], fe_nf[3];
+  const void* tab_q;
+  const void* tab_f;
+  long long tab_foff[3], tab_nf[3];
 };
 // stage kernel of this velocity: separable-operator kernel when optab is set
 inline bool use_sep_kernel(const VelDev& v) { return v.sep1 && v.optab != nullptr; }
@@ -185,11 +191,16 @@ int launch_static_cfl(const Ctx& c, const double* vtab64, int n_terms, const int
                       int npt, DevClock* clk);
 // static CFL part of an FE velocity lattice (FP64, degree pv), max-ed into clk->vd_static
 int launch_fe_static_cfl(const Ctx& c, const double* u64, int pv, DevClock* clk);
+// the spatial part of a sum of separable terms (FP64 term tables of
+// build_vtab, terms sorted by component) at every cell's QGauss(p+2) points
+// and every face's, in the state precision (layouts of VelArgs::tab_q / tab_f)
+int launch_vel_tabulate(const Ctx& c, const double* vtab64, int n_terms, const int* comp, int nmax, int npt,
+                        void* tab_q, void* tab_f, const long long* foff, const long long* nf);
 // the FE velocity lattice (FP64, degree pv) at every cell's QGauss(p+2)
 // points and every face's, in the state precision (layouts of VelArgs::
-// fe_q / fe_f); gb[a][q] = Lagrange basis a at Gauss point q
-int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* fe_q,
-                       void* fe_f, const long long* foff, const long long* nf);
+// tab_q / tab_f); gb[a][q] = Lagrange basis a at Gauss point q
+int launch_fe_tabulate(const Ctx& c, const double* u64, int pv, const double (*gb)[kMaxNQ + 2], void* tab_q,
+                       void* tab_f, const long long* foff, const long long* nf);
 // two-level FP64 reduction; partial holds 2 * reduce_blocks(c) doubles,
 // out_dev receives two doubles (sum pair, or max)
 int launch_reduce(const Ctx& c, int which, const void* phi, const void* ref,

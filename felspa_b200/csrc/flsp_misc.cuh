@@ -254,6 +254,72 @@ __global__ void fe_static_cfl_kernel(const MeshArgs m, const double* __restrict_
   }
 }
 
+// terms of each component in a component-sorted term list
+struct VelTerms {
+  int cstart[4];
+};
+
+// the spatial part of a sum of separable terms at every cell's quadrature
+// points: one thread per (point, cell), cell fastest; per term the product
+// ((coeff f0) f1) f2 of the term tables' entries, the component's terms in
+// order (the point-wise stage kernel's evaluation), in FP64, stored in T
+template <int DIM, typename T>
+__global__ void vel_tabulate_cells(const MeshArgs m, const double* __restrict__ vtab, int nmax, int npt,
+                                   const VelTerms vt, int nq, T* __restrict__ out) {
+  const int nqd = DIM > 2 ? nq * nq * nq : nq * nq;
+  const long long total = (long long)nqd * m.ncell;
+  auto row = [&](int k, int ax, int i) { return vtab + ((size_t)(k * 3 + ax) * nmax + i) * npt; };
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long cell = i % m.ncell;
+    const int q = (int)(i / m.ncell);
+    const int qx = q % nq, qy = (q / nq) % nq, qz = DIM > 2 ? q / (nq * nq) : 0;
+    const int gx = (int)(cell % m.n[0]), gy = (int)((cell / m.n[0]) % m.n[1]);
+    const int gz = DIM > 2 ? (int)(cell / ((long long)m.n[0] * m.n[1])) : 0;
+    for (int d = 0; d < DIM; ++d) {
+      double u = 0.0;
+      for (int k = vt.cstart[d]; k < vt.cstart[d + 1]; ++k) {
+        double v = row(k, 0, gx)[qx] * row(k, 1, gy)[qy];
+        if (DIM == 3) v = v * row(k, 2, gz)[qz];
+        u += v;
+      }
+      out[((size_t)d * nqd + q) * m.ncell + cell] = T(u);
+    }
+  }
+}
+
+// the normal component E at every face's points: from the lower cell's
+// upper-face entries (the first face: the upper cell's lower-face entries,
+// the same face coordinate bit for bit)
+template <int DIM, typename T>
+__global__ void vel_tabulate_faces(const MeshArgs m, const double* __restrict__ vtab, int nmax, int npt,
+                                   const VelTerms vt, int nq, int E, long long nface, T* __restrict__ out) {
+  const int nqf = DIM > 2 ? nq * nq : nq;
+  const int nf0 = m.n[0] + (E == 0), nf1 = m.n[1] + (E == 1);
+  const int t0 = E == 0 ? 1 : 0, t1 = E == 2 ? 1 : 2;
+  const long long total = (long long)nqf * nface;
+  auto row = [&](int k, int ax, int i) { return vtab + ((size_t)(k * 3 + ax) * nmax + i) * npt; };
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long face = i % nface;
+    const int q = (int)(i / nface);
+    const int q0 = q % nq, q1 = DIM > 2 ? q / nq : 0;
+    const int f[3] = {(int)(face % nf0), (int)((face / nf0) % nf1), DIM > 2 ? (int)(face / ((long long)nf0 * nf1)) : 0};
+    int cidx[3] = {f[0], f[1], f[2]}, j[3] = {0, 0, 0};
+    if (f[E] > 0) { cidx[E] = f[E] - 1; j[E] = nq + 1; }
+    else j[E] = nq;
+    j[t0] = q0;
+    if (DIM > 2) j[t1] = q1;
+    double u = 0.0;
+    for (int k = vt.cstart[E]; k < vt.cstart[E + 1]; ++k) {
+      double v = row(k, 0, cidx[0])[j[0]] * row(k, 1, cidx[1])[j[1]];
+      if (DIM == 3) v = v * row(k, 2, cidx[2])[j[2]];
+      u += v;
+    }
+    out[(size_t)q * nface + face] = T(u);
+  }
+}
+
 struct FeBasis {
   double b[kMaxFeVel + 1][kMaxNQ + 2];   // Lagrange basis a at Gauss point q
 };
