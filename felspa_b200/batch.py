@@ -105,8 +105,9 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
     stream) and the autotuner's report; for comparison, on `compare_problems`
     of the problems (all of them by default), the same problems issued one
     after the other, each in its own graph-replayed run on its own stream (so
-    that they overlap on the GPU), against the batched launches, both by wall
-    clock over `compare_steps` steps."""
+    that they overlap on the GPU), and as one group (one graph per period, a
+    branch per problem), against the batched launches, all by wall clock
+    over `compare_steps` steps."""
     import time
     import torch
     from .lib import check, load
@@ -148,6 +149,14 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
         pb.sync()
     t_single = time.perf_counter() - t0
     sub_dofs = sum(pb.n_dofs for pb in singles)
+    # the same problems as one group: one graph per period, a branch per problem
+    g = Group(singles)
+    g.run_periods(1, ctl)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.run_periods(compare_steps // reinit_every, ctl)
+    t_group = time.perf_counter() - t0
+    g.close()
     for pb in singles:
         pb.close()
     bs = make_batch(sub, precision=abi.FP32)
@@ -163,7 +172,10 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
             "streams_vs_batched": {"problems": compare_problems, "steps": compare_steps,
                                   "one_by_one_s": t_single, "batched_s": t_batch_sub,
                                   "one_by_one_dof_steps_per_s": sub_dofs * compare_steps / t_single,
-                                  "batched_dof_steps_per_s": sub_dofs * compare_steps / t_batch_sub}}
+                                  "batched_dof_steps_per_s": sub_dofs * compare_steps / t_batch_sub,
+                                  "group_s": t_group,
+                                  "group_dof_steps_per_s": sub_dofs * (compare_steps // reinit_every) * reinit_every
+                                  / t_group}}
 
 
 class Group:
