@@ -1973,6 +1973,7 @@ struct flsp_batch {
   // per kernel kind (adv, hj, weno) and degree 1..3: the items' range in the
   // kind's list (sorted by degree), shared memory, persistent grid
   int deg_off[3][4] = {}, deg_cnt[3][4] = {};
+  int prob_off[4] = {}, prob_cnt[4] = {};   // per degree: its range of the descriptors
   size_t deg_smem[3][4] = {};
   int deg_grid[3][4] = {};
   bool built = false;
@@ -2011,8 +2012,18 @@ int batch_build(flsp_batch* b, const int* adv_tile, const int* hj_tile) {
   std::vector<BatchProb> pr((size_t)n);
   std::vector<int2> ia, ih, iw;
   size_t sa[4] = {0, 0, 0, 0}, sh[4] = {0, 0, 0, 0}, sw[4] = {0, 0, 0, 0};
+  // descriptors sorted by degree (descending): each degree's problems are one
+  // range of the array (its chain's clocks), items refer to the sorted index
+  std::vector<int> order((size_t)n);
+  for (int i = 0; i < n; ++i) order[(size_t)i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->h[x]->p > b->h[y]->p; });
+  for (int p = 0; p < 4; ++p) b->prob_off[p] = b->prob_cnt[p] = 0;
   for (int i = 0; i < n; ++i) {
-    flsp_handle* h = b->h[i];
+    flsp_handle* h = b->h[(size_t)order[(size_t)i]];
+    if (h->p >= 1 && h->p <= 3) {
+      if (b->prob_cnt[h->p] == 0) b->prob_off[h->p] = i;
+      ++b->prob_cnt[h->p];
+    }
     BatchProb& q = pr[(size_t)i];
     std::memset(&q, 0, sizeof(q));
     q.m_adv = h->m;
@@ -2168,57 +2179,95 @@ int batch_hj_all(flsp_batch* b, int thr, int src, int phi0, int dst, int mode, i
   });
 }
 
-int batch_weno_all(flsp_batch* b, int in, int out) {
-  return batch_each_degree(b, kBatchKindWeno, [&](int p, cudaStream_t s) {
-    return launch_batch_weno(s, b->prec, p, b->probs, b->items_weno + b->deg_off[kBatchKindWeno][p],
-                             b->deg_cnt[kBatchKindWeno][p], b->deg_grid[kBatchKindWeno][p],
-                             kWenoTile[0] * kWenoTile[1], b->deg_smem[kBatchKindWeno][p], in, out,
-                             b->weno_list[p], b->weno_n + p, b->deg_cells[p]);
-  });
-}
-
-int batch_enqueue_step(flsp_batch* b) {
-  ST(launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvBegin, 0.0));
-  const int x = b->cur, y = (x + 1) % 3, z = (x + 2) % 3;
+// One degree's chain on stream s: `steps` substeps of the degree's problems
+// and, with ro, their reinitialisation; the buffer roles advance from *cur
+// (the same sequence for every degree).
+int batch_chain(flsp_batch* b, int p, cudaStream_t s, int steps, const flsp_reinit_opts* ro, bool limiter,
+                int* cur) {
+  const BatchProb* probs = b->probs + b->prob_off[p];
+  const int np = b->prob_cnt[p];
+  const int kA = kBatchKindAdv, kH = kBatchKindHJ, kW = kBatchKindWeno;
   const int thr = b->adv_tile[0] * b->adv_tile[1];
-  auto st = [&](int in, int pn, int out, int k, int comb) { return batch_adv_all(b, thr, in, pn, out, k, comb); };
-  if (b->rk == 1) {
-    ST(st(x, x, y, 0, kRK1));
-    b->cur = y;
-  } else if (b->rk == 2) {
-    ST(st(x, x, y, 0, kRK2a));
-    ST(st(y, x, z, 1, kRK2b));
-    b->cur = z;
-  } else {
-    ST(st(x, x, y, 0, kRK3a));
-    ST(st(y, x, z, 1, kRK3b));
-    ST(st(z, x, y, 2, kRK3c));
-    b->cur = y;
+  auto stage = [&](int in, int pn, int out, int k, int comb) {
+    return launch_batch_adv(s, b->prec, p, b->probs, b->items_adv + b->deg_off[kA][p], b->deg_cnt[kA][p],
+                            b->deg_grid[kA][p], thr, b->deg_smem[kA][p], in, pn, out, k, comb);
+  };
+  for (int k = 0; k < steps; ++k) {
+    ST(launch_batch_clock(s, probs, np, kBatchAdvBegin, 0.0));
+    const int x = *cur, y = (x + 1) % 3, z = (x + 2) % 3;
+    if (b->rk == 1) {
+      ST(stage(x, x, y, 0, kRK1));
+      *cur = y;
+    } else if (b->rk == 2) {
+      ST(stage(x, x, y, 0, kRK2a));
+      ST(stage(y, x, z, 1, kRK2b));
+      *cur = z;
+    } else {
+      ST(stage(x, x, y, 0, kRK3a));
+      ST(stage(y, x, z, 1, kRK3b));
+      ST(stage(z, x, y, 2, kRK3c));
+      *cur = y;
+    }
+    ST(launch_batch_clock(s, probs, np, kBatchAdvEnd, 0.0));
   }
-  return launch_batch_clock(b->stream, b->probs, (int)b->h.size(), kBatchAdvEnd, 0.0);
-}
-
-int batch_enqueue_reinit(flsp_batch* b, const flsp_reinit_opts* o, bool limiter) {
-  const int n = (int)b->h.size();
-  const int phi0 = b->cur;
-  const int thr = b->hj_tile[0] * b->hj_tile[1];
-  ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjReset, 0.0));
-  ST(batch_hj_all(b, thr, phi0, phi0, -1, kHJCflOnly, o->rk_order));
-  for (int k = 0; k < o->n_pseudo_steps; ++k) {
-    ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjBegin, o->cfl_max));
-    const int src = b->cur;
+  if (!ro) return FLSP_OK;
+  const int hthr = b->hj_tile[0] * b->hj_tile[1];
+  auto hj = [&](int src, int phi0, int dst, int mode) {
+    return launch_batch_hj(s, b->prec, p, b->probs, b->items_hj + b->deg_off[kH][p], b->deg_cnt[kH][p],
+                           b->deg_grid[kH][p], hthr, b->deg_smem[kH][p], src, phi0, dst, mode, ro->rk_order);
+  };
+  const int phi0 = *cur;
+  ST(launch_batch_clock(s, probs, np, kBatchHjReset, 0.0));
+  ST(hj(phi0, phi0, -1, kHJCflOnly));
+  for (int k = 0; k < ro->n_pseudo_steps; ++k) {
+    ST(launch_batch_clock(s, probs, np, kBatchHjBegin, ro->cfl_max));
+    const int src = *cur;
     const int dst = (src == phi0) ? (phi0 + 1) % 3 : other(src, phi0);
-    ST(batch_hj_all(b, thr, src, phi0, dst, kHJStep, o->rk_order));
+    ST(hj(src, phi0, dst, kHJStep));
     int res = dst;
     if (limiter) {
       const int lim = other(dst, phi0);
-      ST(batch_weno_all(b, dst, lim));
+      ST(launch_batch_weno(s, b->prec, p, b->probs, b->items_weno + b->deg_off[kW][p], b->deg_cnt[kW][p],
+                           b->deg_grid[kW][p], kWenoTile[0] * kWenoTile[1], b->deg_smem[kW][p], dst, lim,
+                           b->weno_list[p], b->weno_n + p, b->deg_cells[p]));
       res = lim;
     }
-    b->cur = res;
-    ST(launch_batch_clock(b->stream, b->probs, n, kBatchHjEnd, 0.0));
+    *cur = res;
+    ST(launch_batch_clock(s, probs, np, kBatchHjEnd, 0.0));
   }
   return FLSP_OK;
+}
+
+// `steps` substeps and, with ro, a reinitialisation of every problem: one
+// chain per degree, the chains side by side on their own streams, forked
+// from the batch stream once and joined back once (a degree waits only for
+// its own problems between stages)
+int batch_enqueue_chains(flsp_batch* b, int steps, const flsp_reinit_opts* ro, bool limiter) {
+  int n = 0;
+  for (int p = 1; p <= 3; ++p) n += b->prob_cnt[p] > 0;
+  const int cur0 = b->cur;
+  int cur_end = cur0;
+  if (n <= 1) {
+    for (int p = 3; p >= 1; --p)
+      if (b->prob_cnt[p] > 0) ST(batch_chain(b, p, b->stream, steps, ro, limiter, &cur_end));
+    b->cur = cur_end;
+    return FLSP_OK;
+  }
+  CU(cudaEventRecord(b->ev_fork, b->stream));
+  int st = FLSP_OK;
+  for (int p = 3; p >= 1; --p) {
+    if (b->prob_cnt[p] == 0) continue;
+    cudaStream_t s = b->side[p - 1];
+    CU(cudaStreamWaitEvent(s, b->ev_fork, 0));
+    int cur = cur0;
+    if (st == FLSP_OK) st = batch_chain(b, p, s, steps, ro, limiter, &cur);
+    cur_end = cur;
+    // join even after a failed launch, so that a capture stays joined
+    CU(cudaEventRecord(b->ev_join[p - 1], s));
+    CU(cudaStreamWaitEvent(b->stream, b->ev_join[p - 1], 0));
+  }
+  if (st == FLSP_OK) b->cur = cur_end;
+  return st;
 }
 
 }  // namespace
@@ -2411,8 +2460,7 @@ int flsp_batch_run_steps(flsp_batch* b, const flsp_ls_opts* o, int n_steps) {
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int st = FLSP_OK;
-        for (int s2 = 0; s2 < to_reinit && st == FLSP_OK; ++s2) st = batch_enqueue_step(b);
-        if (st == FLSP_OK) st = batch_enqueue_reinit(b, &ro, limiter);
+        st = batch_enqueue_chains(b, to_reinit, &ro, limiter);
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (st != FLSP_OK) { if (g) cudaGraphDestroy(g); b->cur = cur0; return st; }
         if (ce != cudaSuccess) return fail(FLSP_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
@@ -2429,7 +2477,7 @@ int flsp_batch_run_steps(flsp_batch* b, const flsp_ls_opts* o, int n_steps) {
       done += to_reinit;
     } else {
       const int k = std::min(to_reinit, n_steps - done);
-      for (int s2 = 0; s2 < k; ++s2) ST(batch_enqueue_step(b));
+      ST(batch_enqueue_chains(b, k, nullptr, false));
       b->n_since_reinit += k;
       done += k;
     }
