@@ -212,3 +212,33 @@ def test_noalloc_argument_checks_without_gpu(flsp):
             reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, abi.RED_MASS_ERROR, fake, ic=BadIC(**kw))
     with pytest.raises(flsp.FlspError, match="null argument"):
         reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, 0, abi.RED_MASS, fake)
+
+
+def test_noalloc_argument_checks_without_gpu(flsp):
+    """flsp_reduce_noalloc refuses missing inputs and bad kinds before it
+    touches a device (fake non-null addresses: nothing is read)"""
+    from felspa_b200.level_set import Mesh, reduce_noalloc
+    from felspa_b200.lib import FlspError
+    from felspa_b200 import fields as F
+    mesh = Mesh(2, (8, 8))
+    fake = 0x1000
+    with pytest.raises(FlspError, match="needs an IC"):
+        reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, abi.RED_MASS_ERROR, fake)
+    with pytest.raises(FlspError, match="needs ref_state"):
+        reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, abi.RED_L1_INTERFACE, fake)
+    with pytest.raises(FlspError, match="bad reduction kind"):
+        reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, 99, fake)
+    with pytest.raises(FlspError, match="bad basis"):
+        reduce_noalloc(mesh, 1, 7, abi.FP64, fake, abi.RED_MASS, fake)
+    with pytest.raises(FlspError, match="null argument"):
+        reduce_noalloc(mesh, 1, abi.BASIS_Q, abi.FP64, fake, abi.RED_MASS, 0)
+    bad_ic = F.sphere((0.5, 0.5), 0.2)
+    d = bad_ic.desc()
+    d.root = 99
+    import ctypes as C
+    L = flsp.load()
+    md = mesh.desc()
+    st = L.flsp_reduce_noalloc(C.byref(md), 1, abi.BASIS_Q, abi.FP64, C.c_void_p(fake), None,
+                               abi.RED_L2_ERROR_IC, C.byref(d), C.c_void_p(fake), None)
+    assert st == abi.FLSP_ERR_BAD_ARG
+    assert b"bad IC" in L.flsp_last_error()
