@@ -246,6 +246,14 @@ int flsp_n_dofs(const flsp_handle* h, int64_t* n_dofs);
 int flsp_dofs_per_cell(const flsp_handle* h, int* n);
 
 /* state -------------------------------------------------------------- */
+/* A velocity whose components are single terms runs the separable stage
+   kernel.  Any other (several terms for a component; every member of a
+   batch) is tabulated once here: its spatial part at every cell's
+   QGauss(p+2) points and its normal component at every face's, in the
+   state precision, read by the stage kernel times the time factor.  The
+   tables take dim (p+2)^dim values per cell plus (p+2)^(dim-1) per face
+   (3D Q2 FP32: ~1 KB per cell), allocated on the first such velocity and
+   kept until flsp_destroy.                                              */
 int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v);
 /* Velocity from a coupled finite-element simulator (the advection
    assembler's simulator branch, advection.implement.h:472-477,891-905;
