@@ -774,10 +774,16 @@ int build_vtab(flsp_handle* h, bool tables = true) {
   for (int k = 0; k < h->vel_dev.n_terms; ++k) comp[k] = h->vel_dev.terms[k].comp;
   h->tab_ok = false;
   if (tables && (h->batch_member || !use_sep_kernel(h->veldev()))) {
-    ST(ensure_vel_tables(h));
-    ST(launch_vel_tabulate(h->ctx(), h->vtab64, h->vel_dev.n_terms, comp, h->nmax, h->npt, h->tab_q, h->tab_f,
-                           h->tab_foff, h->tab_nf));
-    h->tab_ok = true;
+    const int st = ensure_vel_tables(h);
+    if (st == FLSP_OK) {
+      ST(launch_vel_tabulate(h->ctx(), h->vtab64, h->vel_dev.n_terms, comp, h->nmax, h->npt, h->tab_q, h->tab_f,
+                             h->tab_foff, h->tab_nf));
+      h->tab_ok = true;
+    } else if (h->batch_member) {
+      return st;   // the batched stage kernel reads tables only
+    } else {
+      cudaGetLastError();   // no room for the tables: the stage kernel sums the terms at every point
+    }
   }
   // static CFL part: max over vertices of |u_spatial| / diam
   CU(cudaMemsetAsync(&h->clk->vd_static, 0, sizeof(double), h->stream));
