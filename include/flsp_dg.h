@@ -253,7 +253,9 @@ int flsp_dofs_per_cell(const flsp_handle* h, int* n);
    state precision, read by the stage kernel times the time factor.  The
    tables take dim (p+2)^dim values per cell plus (p+2)^(dim-1) per face
    (3D Q2 FP32: ~1 KB per cell), allocated on the first such velocity and
-   kept until flsp_destroy.                                              */
+   kept until flsp_destroy; where they do not fit in device memory the
+   stage kernel sums the terms at every point instead (batch members
+   fail with FLSP_ERR_OOM).                                              */
 int flsp_set_velocity(flsp_handle* h, const flsp_velocity_desc* v);
 /* Velocity from a coupled finite-element simulator (the advection
    assembler's simulator branch, advection.implement.h:472-477,891-905;
