@@ -130,7 +130,26 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
     b.sync()
     finite = all(np.all(np.isfinite(p.get_state())) for p in b.problems[:16])
     n_dofs = b.n_dofs
+    # the FP32 run against the same batch in FP64 after the same steps: per
+    # problem the L1 interface difference and the relative area difference
+    # (FP64 device reductions of the FP64 problem)
+    s32 = [p.get_state() for p in b.problems]
     b.close()
+    b64 = make_batch(inst, precision=abi.FP64)
+    b64.run_steps(reinit_every + steps, ctl)
+    l1, darea = [], []
+    for pb, st in zip(b64.problems, s32):
+        s64 = pb.get_state()
+        a64 = pb.reduce(abi.RED_MASS)
+        pb.set_state(st)
+        a32 = pb.reduce(abi.RED_MASS)
+        pb.snapshot()
+        pb.set_state(s64)
+        l1.append(pb.reduce(abi.RED_L1_INTERFACE))
+        darea.append(abs(a32 - a64) / abs(a64))
+    b64.close()
+    fp32_vs_fp64 = {"steps": reinit_every + steps, "l1_interface_max": float(max(l1)),
+                    "l1_interface_mean": float(np.mean(l1)), "area_rel_max": float(max(darea))}
     # the same problems one by one, each its own graph-replayed run on its own stream
     sub = inst[:compare_problems]
     singles = []
@@ -168,7 +187,7 @@ def uneven_batch_benchmark(n_problems=256, steps=500, reinit_every=10, n_pseudo=
     bs.close()
     return {"problems": n_problems, "n_dofs": n_dofs, "steps": steps, "reinit_every": reinit_every,
             "pseudo_steps": n_pseudo, "device_ms": ms, "dof_steps_per_s": n_dofs * steps / (ms * 1e-3),
-            "autotune": tune, "autotune_s": t_tune, "finite": bool(finite),
+            "autotune": tune, "autotune_s": t_tune, "finite": bool(finite), "fp32_vs_fp64": fp32_vs_fp64,
             "streams_vs_batched": {"problems": compare_problems, "steps": compare_steps,
                                   "one_by_one_s": t_single, "batched_s": t_batch_sub,
                                   "one_by_one_dof_steps_per_s": sub_dofs * compare_steps / t_single,
