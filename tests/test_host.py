@@ -116,3 +116,22 @@ def test_bench_clock_parser(tmp_path):
     s.proc = P()
     r = s.stop()
     assert r["sm_mhz"] == 1882.5 and r["reasons"] == ["sw_power_cap"] and r["sm_max_mhz"] == 1965.0
+
+
+def test_fe_lattice_layout():
+    """the FE velocity lattice: Gauss-Lobatto nodes per cell, shared faces,
+    components then z, y, x with x fastest"""
+    import math
+    import numpy as np
+    from felspa_b200 import fields as F
+    x3 = F.gauss_lobatto01(3)
+    assert np.allclose(x3, [0.0, 0.5 - 0.5 / math.sqrt(5.0), 0.5 + 0.5 / math.sqrt(5.0), 1.0])
+    cs = F.fe_lattice_coords((3, 2), 2, lo=(0.0, 1.0), hi=(3.0, 2.0))
+    assert np.allclose(cs[0], [0, 0.5, 1, 1.5, 2, 2.5, 3])
+    assert np.allclose(cs[1], [1.0, 1.25, 1.5, 1.75, 2.0])
+    u = F.fe_lattice(lambda x: np.stack([x[..., 0], 10.0 * x[..., 1]], axis=-1), (3, 2), 2,
+                     lo=(0.0, 1.0), hi=(3.0, 2.0))
+    assert u.shape == (2, 5, 7)
+    assert np.allclose(u[0][0], cs[0]) and np.allclose(u[1][:, 0], 10.0 * cs[1])
+    r = F.random_fe_lattice((4, 3, 2), 3, seed=1)
+    assert r.shape == (3, 7, 10, 13)
